@@ -1,0 +1,236 @@
+/*
+ * ne2b.h — C ABI of the B200 simulation core for neuro_edit v2 networks.
+ *
+ * This is the drop-in boundary for the reference's `sim::Backend` trait
+ * (sim/src/lib.rs:119-184).  A Rust `impl Backend for B200Sim` binds these
+ * entry points one-to-one (the binding is written out in INTEGRATION.md);
+ * every other caller (the Python mirror in neuro_edit_v2_b200, the batch
+ * runner, the serving loop) uses the same symbols.
+ *
+ * Conventions
+ *   - Every entry point returns an ne2b_status (0 = NE2B_OK).  On failure
+ *     ne2b_last_error() returns a thread-local message.  Nothing panics or
+ *     throws across this boundary.
+ *   - The caller owns every buffer it passes in; the library copies what it
+ *     keeps.  Output buffers are caller-allocated with the documented size.
+ *   - One handle is used from one host thread at a time.  Stepping calls are
+ *     asynchronous on the handle's CUDA stream (like the reference CUDA
+ *     backend, sim/src/cuda.rs:584-604); every read synchronises first.
+ *   - Plain pointers and sizes only; no CUDA, torch or C++ types.
+ */
+#ifndef NE2B_H
+#define NE2B_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NE2B_OK = 0,
+    NE2B_EINVAL = 1,      /* bad argument, index out of range, malformed net */
+    NE2B_ENOMEM = 2,      /* device or host allocation failed */
+    NE2B_ECUDA = 3,       /* CUDA runtime error (message names the call) */
+    NE2B_EWINDOW = 4,     /* spike_counts window between record depth and t */
+    NE2B_UNSUPPORTED = 5, /* feature not provided by this backend */
+    NE2B_EFULL = 6,       /* admission refused: footprint exceeds free capacity */
+    NE2B_ENODATA = 7      /* nothing to return (e.g. spike_row outside the window) */
+} ne2b_status;
+
+/* Neuron model registry ids, sim/src/model/mod.rs:117 (MODELS order). */
+enum { NE2B_MODEL_IZH = 0, NE2B_MODEL_ADEX = 1 };
+
+/* A network in the flat layout the reference builds before a sim:
+ * NeuronParams::from_network (sim/src/state.rs:98-153), SynCsr from
+ * Network::synapse_csr (net-format/src/network.rs:654-692) and StimMap
+ * (sim/src/stim.rs:26-48). */
+typedef struct {
+    uint32_t n;                  /* neurons */
+    const uint8_t *model;        /* [n] registry id per neuron */
+    const float *params;         /* [n * param_stride] param rows (izh: a,b,c,d; AdEx: 10) */
+    uint32_t param_stride;       /* row width, >= the widest model's param count */
+    const float *x0;             /* [n * 2] initial state rows, or NULL = model init */
+    uint64_t n_syn;
+    const uint32_t *src_ptr;     /* [n + 1] source-major CSR row pointers */
+    const uint32_t *tgt;         /* [n_syn] target neuron */
+    const float *w;              /* [n_syn] weight, Dale's-law signed */
+    const uint16_t *delay_steps; /* [n_syn] delay in steps, >= 1 */
+    const float *tau_ms;         /* [n_syn] per-synapse tau or NULL (0 = merged path) */
+    uint32_t n_inputs;           /* stimulus inputs (Network::inputs) */
+    const uint32_t *stim_ptr;    /* [n + 1] neuron-major (input, weight) rows, or NULL */
+    const uint32_t *stim_input;  /* [stim_ptr[n]] */
+    const float *stim_w;         /* [stim_ptr[n]] */
+} ne2b_net_desc;
+
+/* SimConfig (sim/src/state.rs:8-49) plus the project's additions. */
+typedef struct {
+    float dt_ms;
+    float synapse_tau_ms;
+    float readout_tau_ms;
+    float noise_rate_hz;         /* Poisson kicks (state.rs:15-22) */
+    float noise_kick_mv;
+    uint64_t seed;
+    int32_t record_spikes;
+    uint32_t spike_record_steps;
+    int32_t int_weights;         /* fixed-point ring, scale 4096 (kernels.rs:57-66) */
+    float gauss_sd;              /* Gaussian current noise sd, 0 = off (new) */
+    uint32_t window_steps;       /* on-device per-neuron spike counts per window, 0 = off (new) */
+    uint32_t max_windows;        /* windows kept on device when window_steps > 0 */
+} ne2b_config;
+
+/* sim/src/state.rs:35-49 defaults (dt 0.1, tau 2/2, kick 20 mV, seed 1, ...). */
+void ne2b_config_default(ne2b_config *cfg);
+
+const char *ne2b_last_error(void);
+const char *ne2b_version(void);
+
+/* ------------------------------------------------------------------ sim */
+/* One network on one GPU: the B200 counterpart of CpuSim / CudaSim. */
+typedef struct ne2b_sim ne2b_sim;
+
+/* Sim::with_params (sim/src/lib.rs:217-233), CudaSim::with_params
+ * (sim/src/cuda.rs:130-239).  device = CUDA ordinal. */
+ne2b_status ne2b_create(const ne2b_net_desc *net, const ne2b_config *cfg, int device, ne2b_sim **out);
+ne2b_status ne2b_destroy(ne2b_sim *sim);
+
+ne2b_status ne2b_n(const ne2b_sim *sim, uint32_t *n);                 /* Backend::n */
+ne2b_status ne2b_step_count(const ne2b_sim *sim, uint64_t *t);        /* Backend::step_count */
+ne2b_status ne2b_time_ms(const ne2b_sim *sim, double *ms);            /* Backend::time_ms */
+ne2b_status ne2b_ring_depth(const ne2b_sim *sim, uint32_t *d);        /* state.rs:221 ring_depth */
+/* Backend::run_steps / run_ms (lib.rs:126-127; cuda.rs:584-609): asynchronous */
+ne2b_status ne2b_run_steps(ne2b_sim *sim, uint64_t steps);
+ne2b_status ne2b_run_ms(ne2b_sim *sim, float ms);
+ne2b_status ne2b_reset_state(ne2b_sim *sim);                          /* Backend::reset_state */
+ne2b_status ne2b_synchronize(ne2b_sim *sim);                          /* Backend::synchronize */
+ne2b_status ne2b_dev_mem_bytes(const ne2b_sim *sim, uint64_t *bytes); /* Backend::dev_mem_bytes */
+
+/* Readbacks (lib.rs:136-151).  Buffers hold n values unless noted. */
+ne2b_status ne2b_read_trace(ne2b_sim *sim, float *out);                    /* Backend::trace */
+ne2b_status ne2b_read_state(ne2b_sim *sim, uint32_t slot, float *out);     /* Backend::state */
+ne2b_status ne2b_read_syn_current(ne2b_sim *sim, float *out);              /* merged s[i] (cpu.rs:31) */
+/* Backend::last_spikes: ascending ids; *count = spikes, at most cap written */
+ne2b_status ne2b_last_spikes(ne2b_sim *sim, uint32_t *out, uint32_t cap, uint32_t *count);
+/* Backend::spike_counts (lib.rs:143-146): NE2B_EWINDOW between depth and t */
+ne2b_status ne2b_spike_counts(ne2b_sim *sim, uint64_t rows, uint32_t *out);
+/* Backend::spike_row: out holds ceil(n/64) words; NE2B_ENODATA outside the window */
+ne2b_status ne2b_spike_row(ne2b_sim *sim, uint32_t back, uint64_t *out);
+ne2b_status ne2b_spikes_total(ne2b_sim *sim, uint64_t *total);             /* Backend::spikes_total */
+ne2b_status ne2b_mean_rate_hz(ne2b_sim *sim, double *hz);                  /* Backend::mean_rate_hz */
+/* On-device window counts (new): window w, n values */
+ne2b_status ne2b_window_counts(ne2b_sim *sim, uint32_t window, uint16_t *out);
+ne2b_status ne2b_windows_done(ne2b_sim *sim, uint32_t *count);
+
+/* Drive (lib.rs:152-183; stim.rs:60-127) */
+ne2b_status ne2b_set_input_constant(ne2b_sim *sim, uint32_t input, float value);
+ne2b_status ne2b_input_values(ne2b_sim *sim, float *out);                  /* [n_inputs] */
+ne2b_status ne2b_play_input(ne2b_sim *sim, uint32_t input, const float *series, uint64_t len);
+ne2b_status ne2b_loop_input(ne2b_sim *sim, uint32_t input, const float *series, uint64_t len);
+ne2b_status ne2b_set_external(ne2b_sim *sim, uint32_t neuron, float amps);
+ne2b_status ne2b_set_external_all(ne2b_sim *sim, const float *ext, uint32_t len);
+ne2b_status ne2b_external(ne2b_sim *sim, float *out);
+ne2b_status ne2b_set_noise(ne2b_sim *sim, float rate_hz, float kick_mv);
+ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd);                 /* new */
+
+/* Editor observability (lib.rs:164-176): not provided by this backend. */
+ne2b_status ne2b_set_v_watch(ne2b_sim *sim, const uint32_t *ids, uint32_t count);
+ne2b_status ne2b_set_grid_watches(ne2b_sim *sim, const uint32_t *members, const uint32_t *group_ptr,
+                                  uint32_t groups);
+
+/* ---------------------------------------------------------------- batch */
+/* Many independent networks of uneven size stepped together: one
+ * persistent kernel per step over every net's tiles, the multi-step loop
+ * replayed from a CUDA graph.  Results per net are those of the net run
+ * alone (bit-identical in fixed-point mode). */
+typedef struct ne2b_batch ne2b_batch;
+ne2b_status ne2b_batch_create(const ne2b_net_desc *nets, const ne2b_config *cfgs, uint32_t count,
+                              int device, ne2b_batch **out);
+ne2b_status ne2b_batch_destroy(ne2b_batch *b);
+ne2b_status ne2b_batch_play_input(ne2b_batch *b, uint32_t net, uint32_t input, const float *series,
+                                  uint64_t len);
+ne2b_status ne2b_batch_run_steps(ne2b_batch *b, uint64_t steps);
+ne2b_status ne2b_batch_reset_state(ne2b_batch *b);
+ne2b_status ne2b_batch_synchronize(ne2b_batch *b);
+ne2b_status ne2b_batch_window_counts(ne2b_batch *b, uint32_t net, uint32_t window, uint16_t *out);
+ne2b_status ne2b_batch_spikes_total(ne2b_batch *b, uint32_t net, uint64_t *total);
+ne2b_status ne2b_batch_read_state(ne2b_batch *b, uint32_t net, uint32_t slot, float *out);
+/* Time candidate tile shapes on a snapshot of the batch and keep the
+ * fastest (state is restored afterwards). */
+ne2b_status ne2b_batch_autotune(ne2b_batch *b, uint32_t steps_per_trial);
+ne2b_status ne2b_batch_tile_shape(ne2b_batch *b, uint32_t *block, uint32_t *neurons_per_thread,
+                                  uint32_t *blocks_per_sm);
+ne2b_status ne2b_batch_set_tile_shape(ne2b_batch *b, uint32_t block, uint32_t neurons_per_thread,
+                                      uint32_t blocks_per_sm);
+ne2b_status ne2b_batch_dev_mem_bytes(ne2b_batch *b, uint64_t *bytes);
+ne2b_status ne2b_batch_last_step_ms(ne2b_batch *b, float *ms);
+
+/* -------------------------------------------------------------- serving */
+/* Continuous batching of trial requests: requests are admitted into free
+ * device capacity between steps, stepped together, and retired when their
+ * duration is reached; all state stays on the device. */
+typedef struct ne2b_server ne2b_server;
+typedef struct {
+    uint64_t neuron_capacity;    /* padded neurons resident at once */
+    uint64_t synapse_capacity;   /* synapses resident at once */
+    uint64_t ring_capacity;      /* ring words (depth x padded neurons) resident at once */
+    uint32_t max_requests;       /* concurrent request slots */
+    uint32_t steps_per_launch;   /* steps per graph replay between admissions */
+    int32_t int_weights;
+} ne2b_server_config;
+ne2b_status ne2b_server_create(const ne2b_server_config *cfg, int device, ne2b_server **out);
+ne2b_status ne2b_server_destroy(ne2b_server *s);
+/* Footprint of a request in the three capacities, for admission control. */
+ne2b_status ne2b_request_footprint(const ne2b_net_desc *net, const ne2b_config *cfg, uint64_t *neurons,
+                                   uint64_t *synapses, uint64_t *ring_words);
+/* Admit a request: net + cfg + a [steps x n_inputs] input matrix.  cfg
+ * must set window_steps; steps is the trial duration.  NE2B_EFULL when it
+ * does not fit now (retry after ne2b_server_step retires requests). */
+ne2b_status ne2b_server_submit(ne2b_server *s, const ne2b_net_desc *net, const ne2b_config *cfg,
+                               const float *inputs, uint64_t steps, uint64_t *request_id);
+/* Run one launch of steps_per_launch steps over every admitted request and
+ * retire the finished ones; *finished = number of requests finished. */
+ne2b_status ne2b_server_step(ne2b_server *s, uint32_t *active, uint32_t *finished);
+/* Pop one finished request: its id, neuron count and windows; counts is
+ * [windows x n] u16 (caller sizes it via ne2b_server_result_shape). */
+ne2b_status ne2b_server_result_shape(ne2b_server *s, uint64_t request_id, uint32_t *n, uint32_t *windows);
+ne2b_status ne2b_server_take_result(ne2b_server *s, uint64_t request_id, uint16_t *counts,
+                                    uint64_t *spikes_total);
+ne2b_status ne2b_server_finished_ids(ne2b_server *s, uint64_t *ids, uint32_t cap, uint32_t *count);
+ne2b_status ne2b_server_stats(ne2b_server *s, uint64_t *admitted, uint64_t *retired, uint32_t *active,
+                              uint64_t *neurons_used, uint64_t *synapses_used);
+
+/* ----------------------------------------------------------- net building */
+/* A host-side network owned by the library, in the ne2b_net_desc layout. */
+typedef struct ne2b_net ne2b_net;
+/* Network::synapse_csr (net-format/src/network.rs:654-692): stable sort by
+ * source, Dale's-law sign from the source kind (kind[i]: 0 exc, 1 inh,
+ * 2 regular), steps = max(1, round(delay/dt)), overflow of u16 is
+ * NE2B_EINVAL. Inputs are synapse lists in insertion order. */
+ne2b_status ne2b_net_from_synapses(uint32_t n, const uint8_t *model, const float *params,
+                                   uint32_t param_stride, const uint8_t *kind, uint64_t n_syn,
+                                   const uint32_t *src, const uint32_t *tgt, const float *w,
+                                   const float *delay_ms, const float *tau_ms, float dt_ms,
+                                   ne2b_net **out);
+/* Random K-out workload net (10k/100k/1M configurations). */
+ne2b_status ne2b_gen_random_kout(uint32_t n, uint32_t k, uint64_t seed, float w_scale, float exc_hi,
+                                 float inh_hi, float delay_cap_ms, float dt_ms, ne2b_net **out);
+/* Local 3-D liquid workload net (batched / served configurations). */
+ne2b_status ne2b_gen_liquid(uint32_t side, uint64_t seed, double lambda_units, int32_t radius_units,
+                            float w_rec, uint32_t n_inputs, uint32_t targets_per_input, float w_in,
+                            int32_t model, float dt_ms, ne2b_net **out);
+/* Convert every neuron of a net to a model with the given param rows
+ * (exc_row for kind 0/2, inh_row for kind 1). */
+ne2b_status ne2b_net_set_model_all(ne2b_net *net, int32_t model, const float *exc_row,
+                                   const float *inh_row, uint32_t row_len);
+ne2b_status ne2b_net_desc_of(const ne2b_net *net, ne2b_net_desc *out);
+ne2b_status ne2b_net_kinds(const ne2b_net *net, uint8_t *kind);
+ne2b_status ne2b_net_free(ne2b_net *net);
+
+/* Deterministic exp used by the AdEx step (host copy of the device code). */
+float ne2b_expf(float x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NE2B_H */

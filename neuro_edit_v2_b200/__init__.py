@@ -1,0 +1,24 @@
+"""neuro_edit_v2_b200 — B200-native simulation core for neuro_edit v2 networks.
+
+The step loop of the reference `sim` crate (Izhikevich/AdEx update, spike
+compaction, delivery into the per-delay synaptic ring in fp32 or int32 fixed
+point, current decay, noise, stimulus and spike-count readout) as
+ahead-of-time sm_100a CUDA kernels behind the C ABI of include/ne2b.h.  This
+package is the Python mirror of that ABI; importing it loads the library and
+fails loudly if it is missing.
+"""
+from . import _abi
+from ._abi import MODEL_ADEX, MODEL_IZH, Config, Ne2bError, default_config
+from .net import FlatNet, NativeNet, from_synapses, liquid, random_kout, to_adex
+from .sim import B200Sim, Batch, Server, SpikeWindowError, footprint
+
+__all__ = [
+    "B200Sim", "Batch", "Server", "SpikeWindowError", "footprint", "FlatNet", "NativeNet", "from_synapses",
+    "liquid", "random_kout", "to_adex", "Config", "default_config", "Ne2bError", "MODEL_IZH", "MODEL_ADEX",
+    "expf",
+]
+
+
+def expf(x: float) -> float:
+    """The deterministic exp of the AdEx step (host copy of the device code)."""
+    return float(_abi.lib.ne2b_expf(float(x)))

@@ -1,0 +1,590 @@
+// ne2b_capi.cu — the extern "C" entry points declared in include/ne2b.h.
+// Each entry point validates its handle and arguments, calls the Engine and
+// returns a status; no exception or abort crosses the boundary.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "ne2b_engine.h"
+
+using ne2b::Engine;
+using ne2b::NetHost;
+using ne2b::set_error;
+
+namespace ne2b {
+const char *last_error_str();
+}
+
+struct ne2b_sim {
+    Engine eng;
+    uint32_t slot = 0;
+};
+
+struct ne2b_batch {
+    Engine eng;
+    std::vector<uint32_t> slots;
+};
+
+struct ne2b_server {
+    struct Req {
+        uint32_t slot = 0, n = 0, windows = 0;
+        uint64_t steps = 0, fp_neurons = 0, fp_syn = 0, fp_ring = 0;
+        bool done = false;
+        std::vector<uint16_t> counts;
+        uint64_t spikes = 0;
+    };
+    Engine eng;
+    ne2b_server_config cfg{};
+    std::map<uint64_t, Req> reqs;
+    std::vector<uint64_t> finished;
+    uint64_t used_neurons = 0, used_syn = 0, used_ring = 0;
+    uint64_t next_id = 1, admitted = 0, retired = 0;
+};
+
+#define GUARD(expr)                                                            \
+    do {                                                                       \
+        try {                                                                  \
+            return (expr);                                                     \
+        } catch (const std::bad_alloc &) {                                     \
+            return set_error(NE2B_ENOMEM, "host allocation failed");           \
+        } catch (...) {                                                        \
+            return set_error(NE2B_ECUDA, "unexpected internal exception");     \
+        }                                                                      \
+    } while (0)
+
+#define CHECK_SIM(sim)                                                         \
+    if (!(sim)) return set_error(NE2B_EINVAL, "null sim handle");              \
+    NetHost *h = (sim)->eng.net((sim)->slot);                                  \
+    if (!h) return set_error(NE2B_EINVAL, "sim has no network");
+
+extern "C" {
+
+void ne2b_config_default(ne2b_config *c) {
+    if (!c) return;
+    memset(c, 0, sizeof *c);
+    c->dt_ms = 0.1f;            // net-format/src/lib.rs:39
+    c->synapse_tau_ms = 2.0f;   // lib.rs:26
+    c->readout_tau_ms = 2.0f;   // lib.rs:29
+    c->noise_rate_hz = 0.0f;    // state.rs:41
+    c->noise_kick_mv = 20.0f;   // state.rs:42
+    c->seed = 1;
+    c->record_spikes = 0;
+    c->spike_record_steps = 512;
+    c->int_weights = 0;
+    c->gauss_sd = 0.0f;
+    c->window_steps = 0;
+    c->max_windows = 0;
+}
+
+const char *ne2b_last_error(void) { return ne2b::last_error_str(); }
+const char *ne2b_version(void) { return "ne2b 0.1 sm_100a"; }
+
+// ------------------------------------------------------------------- sim
+ne2b_status ne2b_create(const ne2b_net_desc *net, const ne2b_config *cfg, int device, ne2b_sim **out) {
+    if (!out || !net || !cfg) return set_error(NE2B_EINVAL, "ne2b_create: null argument");
+    *out = nullptr;
+    GUARD(([&]() -> ne2b_status {
+        ne2b_sim *s = new ne2b_sim();
+        ne2b_status st = s->eng.init(device, cfg->int_weights != 0, 1);
+        if (st == NE2B_OK) st = s->eng.add_net(net, cfg, nullptr, 0, &s->slot);
+        if (st != NE2B_OK) {
+            delete s;
+            return st;
+        }
+        *out = s;
+        return NE2B_OK;
+    })());
+}
+
+ne2b_status ne2b_destroy(ne2b_sim *sim) {
+    delete sim;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_n(const ne2b_sim *sim, uint32_t *n) {
+    CHECK_SIM(const_cast<ne2b_sim *>(sim));
+    *n = h->n;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_step_count(const ne2b_sim *sim, uint64_t *t) {
+    CHECK_SIM(const_cast<ne2b_sim *>(sim));
+    *t = h->t;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_time_ms(const ne2b_sim *sim, double *ms) {
+    CHECK_SIM(const_cast<ne2b_sim *>(sim));
+    *ms = (double)h->t * (double)h->cfg.dt_ms;  // cpu.rs:385-387
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_ring_depth(const ne2b_sim *sim, uint32_t *d) {
+    CHECK_SIM(const_cast<ne2b_sim *>(sim));
+    *d = h->D;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_run_steps(ne2b_sim *sim, uint64_t steps) {
+    CHECK_SIM(sim);
+    GUARD(sim->eng.run_steps(steps));
+}
+
+ne2b_status ne2b_run_ms(ne2b_sim *sim, float ms) {
+    CHECK_SIM(sim);
+    // cpu.rs:379-382: (ms / dt).round() as usize (saturating at 0)
+    float st = roundf(ms / h->cfg.dt_ms);
+    uint64_t steps = (st > 0.0f && st == st) ? (uint64_t)st : 0;
+    GUARD(sim->eng.run_steps(steps));
+}
+
+ne2b_status ne2b_reset_state(ne2b_sim *sim) {
+    CHECK_SIM(sim);
+    GUARD(sim->eng.reset_net(sim->slot));
+}
+
+ne2b_status ne2b_synchronize(ne2b_sim *sim) {
+    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
+    return sim->eng.sync();
+}
+
+ne2b_status ne2b_dev_mem_bytes(const ne2b_sim *sim, uint64_t *bytes) {
+    if (!sim || !bytes) return set_error(NE2B_EINVAL, "null argument");
+    *bytes = sim->eng.dev_bytes();
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_read_trace(ne2b_sim *sim, float *out) {
+    CHECK_SIM(sim);
+    return sim->eng.read_f32(h->dev.trace, h->n, out);
+}
+
+ne2b_status ne2b_read_state(ne2b_sim *sim, uint32_t slot, float *out) {
+    CHECK_SIM(sim);
+    if (slot >= 2) return set_error(NE2B_EINVAL, "state slot %u >= 2", slot);
+    return sim->eng.read_f32(slot == 0 ? h->dev.v : h->dev.u, h->n, out);
+}
+
+ne2b_status ne2b_read_syn_current(ne2b_sim *sim, float *out) {
+    CHECK_SIM(sim);
+    return sim->eng.read_f32(h->dev.s, h->n, out);
+}
+
+ne2b_status ne2b_last_spikes(ne2b_sim *sim, uint32_t *out, uint32_t cap, uint32_t *count) {
+    CHECK_SIM(sim);
+    if (!count) return set_error(NE2B_EINVAL, "null count");
+    *count = 0;
+    std::vector<uint64_t> row((h->n + 63) / 64);
+    ne2b_status st = sim->eng.spike_row(*h, 0, row.data());
+    if (st == NE2B_ENODATA) return NE2B_OK;  // cpu.rs:546-548: empty
+    if (st != NE2B_OK) return st;
+    uint32_t c = 0;
+    for (size_t wi = 0; wi < row.size(); ++wi) {
+        uint64_t w = row[wi];
+        while (w) {
+            const uint32_t i = (uint32_t)(wi * 64 + __builtin_ctzll(w));
+            w &= w - 1;
+            if (i < h->n) {
+                if (c < cap && out) out[c] = i;
+                ++c;
+            }
+        }
+    }
+    *count = c;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_spike_counts(ne2b_sim *sim, uint64_t rows, uint32_t *out) {
+    CHECK_SIM(sim);
+    if (!out && h->n) return set_error(NE2B_EINVAL, "null out");
+    GUARD(sim->eng.spike_counts(*h, rows, out));
+}
+
+ne2b_status ne2b_spike_row(ne2b_sim *sim, uint32_t back, uint64_t *out) {
+    CHECK_SIM(sim);
+    return sim->eng.spike_row(*h, back, out);
+}
+
+ne2b_status ne2b_spikes_total(ne2b_sim *sim, uint64_t *total) {
+    CHECK_SIM(sim);
+    return sim->eng.spikes_total(*h, total);
+}
+
+ne2b_status ne2b_mean_rate_hz(ne2b_sim *sim, double *hz) {
+    CHECK_SIM(sim);
+    if (h->t == 0) {  // cpu.rs:389-396
+        *hz = 0.0;
+        return NE2B_OK;
+    }
+    uint64_t tot = 0;
+    ne2b_status st = sim->eng.spikes_total(*h, &tot);
+    if (st != NE2B_OK) return st;
+    const double n = h->n ? (double)h->n : 1.0;
+    *hz = (double)tot / n / ((double)h->t * (double)h->cfg.dt_ms / 1000.0);
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_window_counts(ne2b_sim *sim, uint32_t window, uint16_t *out) {
+    CHECK_SIM(sim);
+    return sim->eng.window_counts(*h, window, out);
+}
+
+ne2b_status ne2b_windows_done(ne2b_sim *sim, uint32_t *count) {
+    CHECK_SIM(sim);
+    *count = h->cfg.window_steps ? (uint32_t)std::min<uint64_t>(h->t / h->cfg.window_steps, h->dev.max_windows) : 0;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_set_input_constant(ne2b_sim *sim, uint32_t input, float value) {
+    CHECK_SIM(sim);
+    if (input >= h->n_inputs) return set_error(NE2B_EINVAL, "input %u out of range (%u inputs)", input, h->n_inputs);
+    h->stim.constants[input] = value;
+    h->dev.stim_len = 0;  // repack at the next run
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_input_values(ne2b_sim *sim, float *out) {
+    CHECK_SIM(sim);
+    for (uint32_t k = 0; k < h->n_inputs; ++k) out[k] = h->stim.constants[k];
+    return NE2B_OK;
+}
+
+static ne2b_status play(ne2b_sim *sim, uint32_t input, const float *series, uint64_t len, bool loop) {
+    CHECK_SIM(sim);
+    if (input >= h->n_inputs) return set_error(NE2B_EINVAL, "input %u out of range (%u inputs)", input, h->n_inputs);
+    if (len && !series) return set_error(NE2B_EINVAL, "null series");
+    GUARD(([&]() -> ne2b_status {
+        h->stim.play(input, h->t, series, len, loop);
+        h->dev.stim_len = 0;
+        return NE2B_OK;
+    })());
+}
+
+ne2b_status ne2b_play_input(ne2b_sim *sim, uint32_t input, const float *series, uint64_t len) {
+    return play(sim, input, series, len, false);
+}
+
+ne2b_status ne2b_loop_input(ne2b_sim *sim, uint32_t input, const float *series, uint64_t len) {
+    return play(sim, input, series, len, true);
+}
+
+ne2b_status ne2b_set_external(ne2b_sim *sim, uint32_t neuron, float amps) {
+    CHECK_SIM(sim);
+    if (neuron >= h->n) return NE2B_OK;  // cpu.rs:588-592: out of range is a no-op
+    std::vector<float> ext = h->ext_host;
+    ext[neuron] = amps;
+    return sim->eng.set_ext(*h, ext.data(), (uint32_t)ext.size());
+}
+
+ne2b_status ne2b_set_external_all(ne2b_sim *sim, const float *ext, uint32_t len) {
+    CHECK_SIM(sim);
+    if (len && !ext) return set_error(NE2B_EINVAL, "null ext");
+    return sim->eng.set_ext(*h, ext, len);
+}
+
+ne2b_status ne2b_external(ne2b_sim *sim, float *out) {
+    CHECK_SIM(sim);
+    for (uint32_t i = 0; i < h->n; ++i) out[i] = h->ext_host[i];
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_set_noise(ne2b_sim *sim, float rate_hz, float kick_mv) {
+    CHECK_SIM(sim);
+    h->cfg.noise_rate_hz = rate_hz;  // cuda.rs:807-810
+    h->cfg.noise_kick_mv = kick_mv;
+    return sim->eng.refresh_noise(*h);
+}
+
+ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd) {
+    CHECK_SIM(sim);
+    h->cfg.gauss_sd = sd;
+    return sim->eng.refresh_noise(*h);
+}
+
+ne2b_status ne2b_set_v_watch(ne2b_sim *sim, const uint32_t *ids, uint32_t count) {
+    (void)sim; (void)ids; (void)count;
+    return set_error(NE2B_UNSUPPORTED, "v-watch recording is not provided by the B200 backend");
+}
+
+ne2b_status ne2b_set_grid_watches(ne2b_sim *sim, const uint32_t *members, const uint32_t *group_ptr,
+                                  uint32_t groups) {
+    (void)sim; (void)members; (void)group_ptr; (void)groups;
+    return set_error(NE2B_UNSUPPORTED, "grid traces are not provided by the B200 backend");
+}
+
+// ----------------------------------------------------------------- batch
+ne2b_status ne2b_batch_create(const ne2b_net_desc *nets, const ne2b_config *cfgs, uint32_t count, int device,
+                              ne2b_batch **out) {
+    if (!out || (!nets && count) || (!cfgs && count)) return set_error(NE2B_EINVAL, "ne2b_batch_create: null argument");
+    *out = nullptr;
+    if (count == 0) return set_error(NE2B_EINVAL, "empty batch");
+    for (uint32_t k = 1; k < count; ++k)
+        if ((cfgs[k].int_weights != 0) != (cfgs[0].int_weights != 0))
+            return set_error(NE2B_EINVAL, "all nets of a batch share one ring mode");
+    GUARD(([&]() -> ne2b_status {
+        ne2b_batch *b = new ne2b_batch();
+        ne2b_status st = b->eng.init(device, cfgs[0].int_weights != 0, count);
+        for (uint32_t k = 0; k < count && st == NE2B_OK; ++k) {
+            uint32_t slot = 0;
+            st = b->eng.add_net(&nets[k], &cfgs[k], nullptr, 0, &slot);
+            b->slots.push_back(slot);
+        }
+        if (st != NE2B_OK) {
+            delete b;
+            return st;
+        }
+        *out = b;
+        return NE2B_OK;
+    })());
+}
+
+ne2b_status ne2b_batch_destroy(ne2b_batch *b) {
+    delete b;
+    return NE2B_OK;
+}
+
+#define CHECK_BATCH_NET(b, k)                                                        \
+    if (!(b)) return set_error(NE2B_EINVAL, "null batch handle");                    \
+    if ((k) >= (b)->slots.size()) return set_error(NE2B_EINVAL, "net %u out of range", (k)); \
+    NetHost *h = (b)->eng.net((b)->slots[(k)]);                                      \
+    if (!h) return set_error(NE2B_EINVAL, "batch net %u missing", (k));
+
+ne2b_status ne2b_batch_play_input(ne2b_batch *b, uint32_t net, uint32_t input, const float *series, uint64_t len) {
+    CHECK_BATCH_NET(b, net);
+    if (input >= h->n_inputs) return set_error(NE2B_EINVAL, "input %u out of range (%u inputs)", input, h->n_inputs);
+    GUARD(([&]() -> ne2b_status {
+        h->stim.play(input, h->t, series, len, false);
+        h->dev.stim_len = 0;
+        return NE2B_OK;
+    })());
+}
+
+ne2b_status ne2b_batch_run_steps(ne2b_batch *b, uint64_t steps) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    GUARD(b->eng.run_steps(steps));
+}
+
+ne2b_status ne2b_batch_reset_state(ne2b_batch *b) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    for (uint32_t s : b->slots) {
+        ne2b_status st = b->eng.reset_net(s);
+        if (st != NE2B_OK) return st;
+    }
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_batch_synchronize(ne2b_batch *b) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    return b->eng.sync();
+}
+
+ne2b_status ne2b_batch_window_counts(ne2b_batch *b, uint32_t net, uint32_t window, uint16_t *out) {
+    CHECK_BATCH_NET(b, net);
+    return b->eng.window_counts(*h, window, out);
+}
+
+ne2b_status ne2b_batch_spikes_total(ne2b_batch *b, uint32_t net, uint64_t *total) {
+    CHECK_BATCH_NET(b, net);
+    return b->eng.spikes_total(*h, total);
+}
+
+ne2b_status ne2b_batch_read_state(ne2b_batch *b, uint32_t net, uint32_t slot, float *out) {
+    CHECK_BATCH_NET(b, net);
+    if (slot >= 2) return set_error(NE2B_EINVAL, "state slot %u >= 2", slot);
+    return b->eng.read_f32(slot == 0 ? h->dev.v : h->dev.u, h->n, out);
+}
+
+ne2b_status ne2b_batch_autotune(ne2b_batch *b, uint32_t steps_per_trial) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    GUARD(b->eng.autotune(steps_per_trial));
+}
+
+ne2b_status ne2b_batch_tile_shape(ne2b_batch *b, uint32_t *block, uint32_t *npt, uint32_t *bps) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    *block = b->eng.shape().block;
+    *npt = b->eng.shape().npt;
+    *bps = b->eng.shape().blocks_per_sm;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_batch_set_tile_shape(ne2b_batch *b, uint32_t block, uint32_t npt, uint32_t bps) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    ne2b::TileShape s;
+    s.block = block;
+    s.npt = npt;
+    s.blocks_per_sm = bps;
+    GUARD(b->eng.set_shape(s));
+}
+
+ne2b_status ne2b_batch_dev_mem_bytes(ne2b_batch *b, uint64_t *bytes) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    *bytes = b->eng.dev_bytes();
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_batch_last_step_ms(ne2b_batch *b, float *ms) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    *ms = b->eng.last_ms();
+    return NE2B_OK;
+}
+
+// --------------------------------------------------------------- serving
+ne2b_status ne2b_request_footprint(const ne2b_net_desc *net, const ne2b_config *cfg, uint64_t *neurons,
+                                   uint64_t *synapses, uint64_t *ring_words) {
+    if (!net || !cfg) return set_error(NE2B_EINVAL, "null argument");
+    const uint64_t np = (net->n + ne2b::kNeuronAlign - 1) / ne2b::kNeuronAlign * ne2b::kNeuronAlign;
+    uint32_t maxd = 1;
+    for (uint64_t j = 0; j < net->n_syn; ++j) maxd = std::max<uint32_t>(maxd, net->delay_steps[j]);
+    const uint64_t D = std::max<uint32_t>(2, maxd + 1);
+    if (neurons) *neurons = np;
+    if (synapses) *synapses = net->n_syn;
+    if (ring_words) *ring_words = D * np;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_server_create(const ne2b_server_config *cfg, int device, ne2b_server **out) {
+    if (!cfg || !out) return set_error(NE2B_EINVAL, "null argument");
+    *out = nullptr;
+    if (cfg->max_requests == 0) return set_error(NE2B_EINVAL, "max_requests must be > 0");
+    GUARD(([&]() -> ne2b_status {
+        ne2b_server *s = new ne2b_server();
+        s->cfg = *cfg;
+        if (s->cfg.steps_per_launch == 0) s->cfg.steps_per_launch = 64;
+        ne2b_status st = s->eng.init(device, cfg->int_weights != 0, cfg->max_requests);
+        if (st != NE2B_OK) {
+            delete s;
+            return st;
+        }
+        s->eng.graph_steps = s->cfg.steps_per_launch;
+        *out = s;
+        return NE2B_OK;
+    })());
+}
+
+ne2b_status ne2b_server_destroy(ne2b_server *s) {
+    delete s;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_server_submit(ne2b_server *s, const ne2b_net_desc *net, const ne2b_config *cfg_in,
+                               const float *inputs, uint64_t steps, uint64_t *request_id) {
+    if (!s || !net || !cfg_in || !request_id) return set_error(NE2B_EINVAL, "null argument");
+    if (steps == 0) return set_error(NE2B_EINVAL, "a request needs steps > 0");
+    if (cfg_in->window_steps == 0) return set_error(NE2B_EINVAL, "a request needs window_steps > 0");
+    if ((cfg_in->int_weights != 0) != (s->cfg.int_weights != 0))
+        return set_error(NE2B_EINVAL, "request ring mode differs from the server's");
+    uint64_t fn = 0, fs = 0, fr = 0;
+    ne2b_status st = ne2b_request_footprint(net, cfg_in, &fn, &fs, &fr);
+    if (st != NE2B_OK) return st;
+    if (fn > s->cfg.neuron_capacity || fs > s->cfg.synapse_capacity || fr > s->cfg.ring_capacity)
+        return set_error(NE2B_EINVAL, "request footprint exceeds the server's total capacity");
+    uint32_t active = 0;
+    for (auto &kv : s->reqs) active += !kv.second.done;
+    if (active >= s->cfg.max_requests || s->used_neurons + fn > s->cfg.neuron_capacity ||
+        s->used_syn + fs > s->cfg.synapse_capacity || s->used_ring + fr > s->cfg.ring_capacity)
+        return set_error(NE2B_EFULL, "no capacity for this request now");
+    GUARD(([&]() -> ne2b_status {
+        ne2b_config cfg = *cfg_in;
+        cfg.max_windows = (uint32_t)((steps + cfg.window_steps - 1) / cfg.window_steps);
+        ne2b_server::Req r;
+        ne2b_status st2 = s->eng.add_net(net, &cfg, inputs, steps, &r.slot);
+        if (st2 != NE2B_OK) return st2;
+        r.n = net->n;
+        r.windows = (uint32_t)(steps / cfg.window_steps);
+        r.steps = steps;
+        r.fp_neurons = fn;
+        r.fp_syn = fs;
+        r.fp_ring = fr;
+        s->used_neurons += fn;
+        s->used_syn += fs;
+        s->used_ring += fr;
+        const uint64_t id = s->next_id++;
+        s->reqs.emplace(id, std::move(r));
+        s->admitted++;
+        *request_id = id;
+        return NE2B_OK;
+    })());
+}
+
+ne2b_status ne2b_server_step(ne2b_server *s, uint32_t *active_out, uint32_t *finished_out) {
+    if (!s) return set_error(NE2B_EINVAL, "null server handle");
+    GUARD(([&]() -> ne2b_status {
+        ne2b_status st = s->eng.run_steps(s->cfg.steps_per_launch);
+        if (st != NE2B_OK) return st;
+        uint32_t fin = 0, act = 0;
+        for (auto &kv : s->reqs) {
+            ne2b_server::Req &r = kv.second;
+            if (r.done) continue;
+            NetHost *h = s->eng.net(r.slot);
+            if (h && h->t >= h->t_end) {
+                r.counts.resize((size_t)r.windows * r.n);
+                for (uint32_t w = 0; w < r.windows && st == NE2B_OK; ++w)
+                    st = s->eng.window_counts(*h, w, r.counts.data() + (size_t)w * r.n);
+                if (st == NE2B_OK) st = s->eng.spikes_total(*h, &r.spikes);
+                if (st == NE2B_OK) st = s->eng.remove_net(r.slot);
+                if (st != NE2B_OK) return st;
+                r.done = true;
+                s->used_neurons -= r.fp_neurons;
+                s->used_syn -= r.fp_syn;
+                s->used_ring -= r.fp_ring;
+                s->retired++;
+                s->finished.push_back(kv.first);
+                ++fin;
+            } else {
+                ++act;
+            }
+        }
+        if (active_out) *active_out = act;
+        if (finished_out) *finished_out = fin;
+        return NE2B_OK;
+    })());
+}
+
+ne2b_status ne2b_server_result_shape(ne2b_server *s, uint64_t id, uint32_t *n, uint32_t *windows) {
+    if (!s) return set_error(NE2B_EINVAL, "null server handle");
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return set_error(NE2B_EINVAL, "unknown request %llu", (unsigned long long)id);
+    *n = it->second.n;
+    *windows = it->second.windows;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_server_take_result(ne2b_server *s, uint64_t id, uint16_t *counts, uint64_t *spikes_total) {
+    if (!s) return set_error(NE2B_EINVAL, "null server handle");
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return set_error(NE2B_EINVAL, "unknown request %llu", (unsigned long long)id);
+    if (!it->second.done) return set_error(NE2B_ENODATA, "request %llu is still running", (unsigned long long)id);
+    if (counts && !it->second.counts.empty())
+        memcpy(counts, it->second.counts.data(), sizeof(uint16_t) * it->second.counts.size());
+    if (spikes_total) *spikes_total = it->second.spikes;
+    s->reqs.erase(it);
+    s->finished.erase(std::remove(s->finished.begin(), s->finished.end(), id), s->finished.end());
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_server_finished_ids(ne2b_server *s, uint64_t *ids, uint32_t cap, uint32_t *count) {
+    if (!s || !count) return set_error(NE2B_EINVAL, "null argument");
+    const uint32_t c = (uint32_t)s->finished.size();
+    for (uint32_t k = 0; k < c && k < cap && ids; ++k) ids[k] = s->finished[k];
+    *count = c;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_server_stats(ne2b_server *s, uint64_t *admitted, uint64_t *retired, uint32_t *active,
+                              uint64_t *neurons_used, uint64_t *synapses_used) {
+    if (!s) return set_error(NE2B_EINVAL, "null server handle");
+    uint32_t act = 0;
+    for (auto &kv : s->reqs) act += !kv.second.done;
+    if (admitted) *admitted = s->admitted;
+    if (retired) *retired = s->retired;
+    if (active) *active = act;
+    if (neurons_used) *neurons_used = s->used_neurons;
+    if (synapses_used) *synapses_used = s->used_syn;
+    return NE2B_OK;
+}
+
+}  // extern "C"

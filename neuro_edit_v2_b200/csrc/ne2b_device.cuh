@@ -1,0 +1,114 @@
+// ne2b_device.cuh — per-neuron arithmetic of the B200 step kernel.
+//
+// Every float operation that the reference performs in f32 is written with an
+// explicit round-to-nearest intrinsic (__fadd_rn, __fmul_rn, __fdiv_rn), so the
+// compiler cannot contract it into an FMA or reorder it: the kernel computes
+// exactly the IEEE-754 sequence of the reference CPU step (sim/src/cpu.rs:
+// 216-261, sim/src/model/izh.rs:184-192, sim/src/model/adex.rs:163-176).
+#pragma once
+#include <stdint.h>
+
+namespace ne2b {
+
+// Counter-hash base of (neuron, step, seed): sim/src/state.rs:285-288.
+__device__ __forceinline__ uint64_t noise_base(uint32_t i, uint64_t t, uint64_t seed) {
+    return (uint64_t)i * 0x9E3779B97F4A7C15ull + t * 0xBF58476D1CE4E5B9ull + seed * 0x94D049BB133111EBull;
+}
+
+// splitmix64 finaliser: sim/src/state.rs:289-293.
+__device__ __forceinline__ uint64_t mix64(uint64_t h) {
+    h ^= h >> 30;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 27;
+    h *= 0x94D049BB133111EBull;
+    h ^= h >> 31;
+    return h;
+}
+
+// Poisson kick flag: state.rs:299-301, kernels.rs:128-130.
+__device__ __forceinline__ bool noise_fires(uint64_t base, float p) {
+    uint32_t h = (uint32_t)(mix64(base) >> 32);
+    return __fmul_rn(__uint2float_rn(h), 2.3283064e-10f) < p;
+}
+
+// Gaussian current numerator: the four 16-bit fields of one splitmix64 hash
+// of base + G (G = 0xD1B54A32D192ED03) summed (Irwin-Hall, 4 terms) minus the
+// mean 131070.  Multiplied by sd*sqrt(3)/65536 it has mean 0 and variance
+// 1 - 2^-32.  Integer-exact, so CPU and GPU agree bit-for-bit.
+__device__ __forceinline__ int32_t gauss_numer(uint64_t base) {
+    uint64_t h = mix64(base + 0xD1B54A32D192ED03ull);
+    uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
+    int32_t s = (int32_t)((lo & 0xffffu) + (lo >> 16) + (hi & 0xffffu) + (hi >> 16));
+    return s - 131070;
+}
+
+// Deterministic exp(x) for the AdEx step: Cody-Waite reduction x = k*ln2 + r
+// with ln2 split into a 32-significant-bit head and a double tail, the
+// degree-13 Taylor polynomial of e^r (coefficients 1/i! rounded to double)
+// evaluated by Horner with fused multiply-adds, scaled by 2^k, rounded once to
+// float.  Only IEEE double operations, so the host copy (ne2b_expf) and the
+// parity oracle reproduce it bit-for-bit.
+__device__ __forceinline__ float det_expf(float x) {
+    if (x != x) return x;
+    if (x > 88.8f) return __int_as_float(0x7f800000);
+    if (x < -104.0f) return 0.0f;
+    const double xd = (double)x;
+    const double k = rint(__dmul_rn(xd, 0x1.71547652b82fep+0));
+    double r = __fma_rn(-k, 0x1.62e42fee00000p-1, xd);
+    r = __fma_rn(-k, 0x1.a39ef35793c76p-33, r);
+    double p = 0x1.6124613a86d09p-33;
+    p = __fma_rn(p, r, 0x1.1eed8eff8d898p-29);
+    p = __fma_rn(p, r, 0x1.ae64567f544e4p-26);
+    p = __fma_rn(p, r, 0x1.27e4fb7789f5cp-22);
+    p = __fma_rn(p, r, 0x1.71de3a556c734p-19);
+    p = __fma_rn(p, r, 0x1.a01a01a01a01ap-16);
+    p = __fma_rn(p, r, 0x1.a01a01a01a01ap-13);
+    p = __fma_rn(p, r, 0x1.6c16c16c16c17p-10);
+    p = __fma_rn(p, r, 0x1.1111111111111p-7);
+    p = __fma_rn(p, r, 0x1.5555555555555p-5);
+    p = __fma_rn(p, r, 0x1.5555555555555p-3);
+    p = __fma_rn(p, r, 0x1.0000000000000p-1);
+    p = __fma_rn(p, r, 1.0);
+    p = __fma_rn(p, r, 1.0);
+    const long long ki = (long long)k;
+    const double scale = __longlong_as_double((ki + 1023ll) << 52);
+    return __double2float_rn(__dmul_rn(p, scale));
+}
+
+// Izhikevich step, sim/src/model/izh.rs:184-192 (CUDA text izh.rs:194-199):
+// reset for last step's crossing, v with the old u, u with the new v.
+__device__ __forceinline__ bool izh_step(const float *p, float &v, float &u, float I, float dt) {
+    if (v >= 30.0f) {
+        v = p[2];
+        u = __fadd_rn(u, p[3]);
+    }
+    float a = __fmul_rn(__fmul_rn(0.04f, v), v);
+    float b = __fmul_rn(5.0f, v);
+    float sum = __fadd_rn(__fsub_rn(__fadd_rn(__fadd_rn(a, b), 140.0f), u), I);
+    v = __fadd_rn(v, __fmul_rn(dt, sum));
+    u = __fadd_rn(u, __fmul_rn(__fmul_rn(dt, p[0]), __fsub_rn(__fmul_rn(p[1], v), u)));
+    return v >= 30.0f;
+}
+
+// AdEx step, sim/src/model/adex.rs:163-176 (CUDA text adex.rs:178-185):
+// p = [C, gL, EL, VT, dT, a, tau_w, b, Vr, Vpeak].
+__device__ __forceinline__ bool adex_step(const float *p, float &v, float &w, float I, float dt) {
+    if (v >= p[9]) {
+        v = p[8];
+        w = __fadd_rn(w, p[7]);
+    }
+    const float arg = fminf(__fdiv_rn(__fsub_rn(v, p[3]), p[4]), 10.0f);
+    const float ex = det_expf(arg);
+    // -p1*(v-p2) + p1*p4*ex - w + I
+    float acc = __fmul_rn(-p[1], __fsub_rn(v, p[2]));
+    acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(p[1], p[4]), ex));
+    acc = __fadd_rn(__fsub_rn(acc, w), I);
+    v = __fadd_rn(v, __fdiv_rn(__fmul_rn(dt, acc), p[0]));
+    float accw = __fsub_rn(__fmul_rn(p[5], __fsub_rn(v, p[2])), w);
+    w = __fadd_rn(w, __fdiv_rn(__fmul_rn(dt, accw), p[6]));
+    const bool spiked = v >= p[9];
+    if (v > p[9]) v = p[9];
+    return spiked;
+}
+
+}  // namespace ne2b

@@ -1,0 +1,766 @@
+// ne2b_engine.cu — host runtime: per-net device allocations, the param
+// dictionary, tiles, CUDA-graph replay of launch groups, stimulus packing,
+// readbacks, snapshots for the tile-shape autotuner.
+#include "ne2b_engine.h"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "ne2b_kernels.h"
+
+namespace ne2b {
+
+static thread_local std::string g_err;
+
+ne2b_status set_error(ne2b_status st, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return st;
+}
+
+ne2b_status cuda_error(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return NE2B_OK;
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(NE2B_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+    return set_error(NE2B_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+const char *last_error_str() { return g_err.c_str(); }
+
+#define NE2B_CUDA(call)                                                  \
+    do {                                                                 \
+        cudaError_t _e = (call);                                         \
+        if (_e != cudaSuccess) return cuda_error(_e, #call);             \
+    } while (0)
+#define NE2B_TRY(call)                                                   \
+    do {                                                                 \
+        ne2b_status _s = (call);                                         \
+        if (_s != NE2B_OK) return _s;                                    \
+    } while (0)
+
+// ------------------------------------------------------------ Stimulus
+// stim.rs:102-115
+float Stimulus::value(uint32_t k, uint64_t t) const {
+    if (k < series.size() && !series[k].empty()) {
+        const std::vector<float> &s = series[k];
+        const uint64_t start = k < play_start.size() ? play_start[k] : 0;
+        if (k < looped.size() && looped[k]) {
+            const int64_t m = (int64_t)s.size();
+            int64_t d = ((int64_t)t - (int64_t)start) % m;
+            if (d < 0) d += m;
+            return s[(size_t)d];
+        }
+        const uint64_t idx = t - start;  // wrapping_sub
+        return idx < s.size() ? s[(size_t)idx] : 0.0f;
+    }
+    return k < constants.size() ? constants[k] : 0.0f;
+}
+
+// stim.rs:71-96
+void Stimulus::play(uint32_t k, uint64_t t, const float *v, uint64_t len, bool loop) {
+    if (k >= series.size()) series.resize(k + 1);
+    if (k >= play_start.size()) play_start.resize(k + 1, 0);
+    if (k >= looped.size()) looped.resize(k + 1, 0);
+    series[k].assign(v, v + len);
+    play_start[k] = t;
+    looped[k] = loop ? 1 : 0;
+}
+
+// -------------------------------------------------------------- Engine
+Engine::~Engine() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    clear_graphs();
+    for (NetHost *h : nets_) {
+        if (!h) continue;
+        for (void *p : h->allocs) cudaFreeAsync(p, stream_);
+        delete h;
+    }
+    if (stream_) cudaStreamSynchronize(stream_);
+    cudaFree(d_nets_);
+    cudaFree(d_counters_);
+    cudaFree(d_ptab_);
+    cudaFree(d_tiles_);
+    cudaFree(d_eng_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::clear_graphs() {
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+}
+
+ne2b_status Engine::init(int device, bool int_ring, uint32_t max_nets) {
+    device_ = device;
+    int_ring_ = int_ring;
+    NE2B_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    NE2B_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return set_error(NE2B_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                         prop.major, prop.minor);
+    sm_count_ = prop.multiProcessorCount;
+    NE2B_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t thr = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    nets_cap_ = max_nets ? max_nets : 1;
+    NE2B_CUDA(cudaMalloc(&d_nets_, sizeof(NetDev) * nets_cap_));
+    NE2B_CUDA(cudaMemset(d_nets_, 0, sizeof(NetDev) * nets_cap_));
+    NE2B_CUDA(cudaMalloc(&d_counters_, sizeof(NetCounters) * nets_cap_));
+    NE2B_CUDA(cudaMemset(d_counters_, 0, sizeof(NetCounters) * nets_cap_));
+    NE2B_CUDA(cudaMalloc(&d_eng_, sizeof(EngineDev)));
+    ptab_cap_ = 64;
+    NE2B_CUDA(cudaMalloc(&d_ptab_, sizeof(ParamRow) * ptab_cap_));
+    tiles_cap_ = 1024;
+    NE2B_CUDA(cudaMalloc(&d_tiles_, sizeof(Tile) * tiles_cap_));
+    NE2B_CUDA(cudaEventCreate(&ev0_));
+    NE2B_CUDA(cudaEventCreate(&ev1_));
+    nets_.assign(nets_cap_, nullptr);
+    return upload_eng();
+}
+
+ne2b_status Engine::upload_eng() {
+    EngineDev e;
+    e.tiles = d_tiles_;
+    e.n_tiles = n_tiles_;
+    e.n_nets = nets_cap_;
+    e.nets = d_nets_;
+    e.ptab = d_ptab_;
+    e.counters = d_counters_;
+    NE2B_CUDA(cudaMemcpyAsync(d_eng_, &e, sizeof e, cudaMemcpyHostToDevice, stream_));
+    // the source lives on this stack frame: wait for the copy
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::param_index(uint32_t model, const float *p, uint32_t np, uint16_t *idx) {
+    std::vector<uint32_t> key(kMaxParams + 1, 0u);
+    key[0] = model;
+    for (uint32_t k = 0; k < np && k < kMaxParams; ++k) memcpy(&key[k + 1], &p[k], 4);
+    auto it = ptab_index_.find(key);
+    if (it != ptab_index_.end()) {
+        *idx = it->second;
+        return NE2B_OK;
+    }
+    if (h_ptab_.size() >= 65536)
+        return set_error(NE2B_UNSUPPORTED, "more than 65536 distinct parameter rows in one engine");
+    ParamRow r;
+    memset(&r, 0, sizeof r);
+    for (uint32_t k = 0; k < np && k < kMaxParams; ++k) r.p[k] = p[k];
+    r.model = model;
+    *idx = (uint16_t)h_ptab_.size();
+    h_ptab_.push_back(r);
+    ptab_index_[key] = *idx;
+    ptab_dirty_ = true;
+    return NE2B_OK;
+}
+
+ne2b_status Engine::upload_ptab() {
+    if (!ptab_dirty_) return NE2B_OK;
+    if (h_ptab_.size() > ptab_cap_) {
+        uint32_t cap = ptab_cap_;
+        while (cap < h_ptab_.size()) cap *= 2;
+        NE2B_CUDA(cudaStreamSynchronize(stream_));
+        NE2B_CUDA(cudaFree(d_ptab_));
+        d_ptab_ = nullptr;
+        NE2B_CUDA(cudaMalloc(&d_ptab_, sizeof(ParamRow) * cap));
+        ptab_cap_ = cap;
+        NE2B_TRY(upload_eng());
+    }
+    NE2B_CUDA(cudaMemcpyAsync(d_ptab_, h_ptab_.data(), sizeof(ParamRow) * h_ptab_.size(), cudaMemcpyHostToDevice,
+                              stream_));
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    ptab_dirty_ = false;
+    return NE2B_OK;
+}
+
+static float host_decay(float dt, float tau) {
+    // cpu.rs:203-204: (-dt / tau.max(1e-6)).exp() in f32 (libm expf)
+    const float t = tau > 1e-6f ? tau : 1e-6f;
+    return expf(-dt / t);
+}
+
+static void fill_noise(NetDev &d, const ne2b_config &c) {
+    d.pkick = c.noise_rate_hz * c.dt_ms / 1000.0f;                 // cpu.rs:197
+    d.kick = c.noise_kick_mv != 0.0f ? c.noise_kick_mv / c.dt_ms : 0.0f;  // cpu.rs:198-202
+    d.gauss_k = c.gauss_sd != 0.0f ? (float)((double)c.gauss_sd * 1.7320508075688772 / 65536.0) : 0.0f;
+}
+
+ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
+                            uint32_t *slot_out) {
+    if (!net || !cfg) return set_error(NE2B_EINVAL, "add_net: null net or config");
+    const uint32_t n = net->n;
+    if (!(cfg->dt_ms >= 0.001f && cfg->dt_ms <= 100.0f))  // lib.rs:35-39 valid_dt_ms
+        return set_error(NE2B_EINVAL, "dt_ms %g outside [0.001, 100]", (double)cfg->dt_ms);
+    if (n > 0 && (!net->model || !net->params || !net->src_ptr))
+        return set_error(NE2B_EINVAL, "net: model, params and src_ptr are required");
+    if (net->param_stride < 4 && n > 0) return set_error(NE2B_EINVAL, "param_stride %u < 4", net->param_stride);
+    if (n > 0 && net->src_ptr[n] != net->n_syn)
+        return set_error(NE2B_EINVAL, "src_ptr[n] = %u but n_syn = %llu", net->src_ptr[n],
+                         (unsigned long long)net->n_syn);
+    if (net->n_syn > 0xffffffffull) return set_error(NE2B_UNSUPPORTED, "more than 2^32-1 synapses in one net");
+    uint32_t maxd = 1;
+    for (uint32_t i = 0; i < n; ++i)
+        if (net->src_ptr[i] > net->src_ptr[i + 1]) return set_error(NE2B_EINVAL, "src_ptr not monotone at %u", i);
+    for (uint64_t j = 0; j < net->n_syn; ++j) {
+        if (net->tgt[j] >= n) return set_error(NE2B_EINVAL, "synapse %llu targets %u >= n %u", (unsigned long long)j, net->tgt[j], n);
+        const uint32_t d = net->delay_steps[j];
+        if (d < 1) return set_error(NE2B_EINVAL, "synapse %llu has delay 0 steps", (unsigned long long)j);
+        if (d > maxd) maxd = d;
+        if (net->tau_ms && net->tau_ms[j] > 0.0f)
+            return set_error(NE2B_UNSUPPORTED, "per-synapse tau (synapse %llu) is not supported by this backend",
+                             (unsigned long long)j);
+    }
+    for (uint32_t i = 0; i < n; ++i)
+        if (net->model[i] > 1) return set_error(NE2B_EINVAL, "neuron %u: unknown model id %u", i, net->model[i]);
+    if (n > 0 && net->n_inputs > 0 && net->stim_ptr) {
+        if (net->stim_ptr[0] != 0) return set_error(NE2B_EINVAL, "stim_ptr[0] != 0");
+        for (uint32_t i = 0; i < n; ++i)
+            if (net->stim_ptr[i] > net->stim_ptr[i + 1]) return set_error(NE2B_EINVAL, "stim_ptr not monotone");
+        for (uint32_t j = 0; j < net->stim_ptr[n]; ++j)
+            if (net->stim_input[j] >= net->n_inputs) return set_error(NE2B_EINVAL, "stim entry %u names input %u", j, net->stim_input[j]);
+    }
+    if (cfg->window_steps > 0 && cfg->window_steps > 131070u)
+        return set_error(NE2B_EINVAL, "window_steps %u would overflow the u16 window counts", cfg->window_steps);
+    if (inputs && net->n_inputs == 0) inputs = nullptr;
+
+    uint32_t slot = nets_cap_;
+    for (uint32_t j = 0; j < nets_cap_; ++j)
+        if (!nets_[j]) { slot = j; break; }
+    if (slot == nets_cap_) return set_error(NE2B_EFULL, "all %u net slots are in use", nets_cap_);
+
+    NetHost *h = new NetHost();
+    h->cfg = *cfg;
+    h->slot = slot;
+    h->n = n;
+    h->n_pad = (n + kNeuronAlign - 1) / kNeuronAlign * kNeuronAlign;
+    h->D = maxd + 1 < 2 ? 2 : maxd + 1;  // state.rs:221-224
+    h->e = net->n_syn;
+    h->n_inputs = net->n_inputs;
+    h->t_end = inputs ? steps : ~0ull;
+    h->fixed_stim = inputs != nullptr;
+    h->stim.constants.assign(net->n_inputs, 0.0f);
+    h->stim.series.assign(net->n_inputs, {});
+    h->stim.play_start.assign(net->n_inputs, 0);
+    h->stim.looped.assign(net->n_inputs, 0);
+    h->ext_host.assign(n, 0.0f);
+
+    auto alloc = [&](void **p, size_t bytes) -> ne2b_status {
+        *p = nullptr;
+        if (bytes == 0) return NE2B_OK;
+        cudaError_t e = cudaMallocAsync(p, bytes, stream_);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync (net arrays)");
+        h->allocs.push_back(*p);
+        h->dev_bytes += bytes;
+        return NE2B_OK;
+    };
+    auto fail = [&](ne2b_status st) {
+        for (void *p : h->allocs) cudaFreeAsync(p, stream_);
+        cudaStreamSynchronize(stream_);
+        delete h;
+        return st;
+    };
+    auto up = [&](void *dst, const void *src, size_t bytes) -> ne2b_status {
+        if (!bytes) return NE2B_OK;
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_);
+        return e == cudaSuccess ? NE2B_OK : cuda_error(e, "cudaMemcpyAsync (net upload)");
+    };
+#define NET_TRY(x)                          \
+    do {                                    \
+        ne2b_status _s = (x);               \
+        if (_s != NE2B_OK) return fail(_s); \
+    } while (0)
+
+    const uint32_t np = h->n_pad;
+    NetDev &d = h->dev;
+    memset(&d, 0, sizeof d);
+    void *p = nullptr;
+    NET_TRY(alloc(&p, sizeof(float) * np)); d.v = (float *)p;
+    NET_TRY(alloc(&p, sizeof(float) * np)); d.u = (float *)p;
+    NET_TRY(alloc(&p, sizeof(float) * np)); d.s = (float *)p;
+    NET_TRY(alloc(&p, sizeof(float) * np)); d.trace = (float *)p;
+    NET_TRY(alloc(&p, sizeof(float) * np)); d.ext = (float *)p;
+    NET_TRY(alloc(&p, sizeof(float) * np)); d.v0 = (const float *)p;
+    NET_TRY(alloc(&p, sizeof(float) * np)); d.u0 = (const float *)p;
+    NET_TRY(alloc(&p, sizeof(uint16_t) * np)); d.pidx = (const uint16_t *)p;
+    NET_TRY(alloc(&p, sizeof(unsigned long long) * np)); d.pn_total = (unsigned long long *)p;
+    NET_TRY(alloc(&p, sizeof(uint32_t) * (size_t)h->D * np)); d.ring = p;
+    NET_TRY(alloc(&p, sizeof(uint32_t) * ((size_t)n + 1))); d.rowptr = (const uint32_t *)p;
+    NET_TRY(alloc(&p, sizeof(uint32_t) * h->e)); d.tgt = (const uint32_t *)p;
+    NET_TRY(alloc(&p, sizeof(uint32_t) * h->e)); d.w = p;
+    const bool d16 = h->D > 256;
+    NET_TRY(alloc(&p, (d16 ? 2 : 1) * h->e)); d.delay = p;
+
+    // host-side rows: params -> dictionary, x0
+    std::vector<uint16_t> pidx(np, 0);
+    std::vector<float> v0(np, 0.0f), u0(np, 0.0f);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *row = net->params + (size_t)i * net->param_stride;
+        const uint32_t m = net->model[i];
+        const uint32_t width = std::min<uint32_t>(net->param_stride, 10);
+        NET_TRY(param_index(m, row, width, &pidx[i]));
+        if (net->x0) {
+            v0[i] = net->x0[2 * (size_t)i];
+            u0[i] = net->x0[2 * (size_t)i + 1];
+        } else if (m == NE2B_MODEL_ADEX) {  // adex.rs:149-152
+            v0[i] = row[2];
+            u0[i] = 0.0f;
+        } else {  // izh.rs:175-178
+            v0[i] = -65.0f;
+            u0[i] = row[1] * v0[i];
+        }
+    }
+    if (n > 0) pidx[n - 1] = pidx[n - 1];
+    NET_TRY(upload_ptab());
+    NET_TRY(up((void *)d.pidx, pidx.data(), sizeof(uint16_t) * np));
+    NET_TRY(up((void *)d.v0, v0.data(), sizeof(float) * np));
+    NET_TRY(up((void *)d.u0, u0.data(), sizeof(float) * np));
+    NET_TRY(cuda_error(cudaMemsetAsync(d.ext, 0, sizeof(float) * np, stream_), "memset ext"));
+    NET_TRY(up((void *)d.rowptr, net->src_ptr, sizeof(uint32_t) * ((size_t)n + 1)));
+    NET_TRY(up((void *)d.tgt, net->tgt, sizeof(uint32_t) * h->e));
+    if (int_ring_) {
+        std::vector<int32_t> wq(h->e);
+        for (uint64_t j = 0; j < h->e; ++j) wq[j] = (int32_t)lrintf(net->w[j] * 4096.0f);  // kernels.rs:61 rt_put
+        NET_TRY(up((void *)d.w, wq.data(), 4 * h->e));
+    } else {
+        NET_TRY(up((void *)d.w, net->w, 4 * h->e));
+    }
+    if (d16) {
+        NET_TRY(up((void *)d.delay, net->delay_steps, 2 * h->e));
+    } else {
+        std::vector<uint8_t> d8(h->e);
+        for (uint64_t j = 0; j < h->e; ++j) d8[j] = (uint8_t)net->delay_steps[j];
+        NET_TRY(up((void *)d.delay, d8.data(), h->e));
+    }
+    // stimulus routing
+    const bool has_stim = n > 0 && net->n_inputs > 0 && net->stim_ptr && net->stim_ptr[n] > 0;
+    if (has_stim) {
+        const uint32_t ne = net->stim_ptr[n];
+        NET_TRY(alloc(&p, sizeof(uint32_t) * ((size_t)n + 1))); d.stim_ptr = (const uint32_t *)p;
+        NET_TRY(alloc(&p, sizeof(uint32_t) * ne)); d.stim_in = (const uint32_t *)p;
+        NET_TRY(alloc(&p, sizeof(float) * ne)); d.stim_w = (const float *)p;
+        NET_TRY(up((void *)d.stim_ptr, net->stim_ptr, sizeof(uint32_t) * ((size_t)n + 1)));
+        NET_TRY(up((void *)d.stim_in, net->stim_input, sizeof(uint32_t) * ne));
+        NET_TRY(up((void *)d.stim_w, net->stim_w, sizeof(float) * ne));
+        h->stim_ptr_host.assign(net->stim_ptr, net->stim_ptr + n + 1);
+        if (inputs) {
+            NET_TRY(alloc(&p, sizeof(float) * (size_t)steps * net->n_inputs)); d.stim_buf = (const float *)p;
+            NET_TRY(up((void *)d.stim_buf, inputs, sizeof(float) * (size_t)steps * net->n_inputs));
+            d.stim_t0 = 0;
+            d.stim_len = (uint32_t)std::min<uint64_t>(steps, 0xffffffffull);
+        } else {
+            h->stim_cap = (uint32_t)stim_chunk;
+            NET_TRY(alloc(&p, sizeof(float) * (size_t)h->stim_cap * net->n_inputs)); d.stim_buf = (const float *)p;
+            d.stim_t0 = 0;
+            d.stim_len = 0;  // packed before the first launch
+        }
+    }
+    // spike record + windows
+    uint32_t rec_rows = 0;
+    if (cfg->record_spikes) rec_rows = cfg->spike_record_steps < 2 ? 2 : cfg->spike_record_steps;  // cpu.rs:112-116
+    if (rec_rows) {
+        NET_TRY(alloc(&p, sizeof(uint32_t) * (size_t)rec_rows * (np / 32))); d.rec_bits = (uint32_t *)p;
+    }
+    if (cfg->window_steps > 0) {
+        NET_TRY(alloc(&p, sizeof(uint32_t) * np)); d.wcount = (uint32_t *)p;
+        const uint32_t mw = cfg->max_windows ? cfg->max_windows : 1;
+        NET_TRY(alloc(&p, sizeof(uint16_t) * (size_t)mw * np)); d.win_out = (uint16_t *)p;
+        d.win_steps = cfg->window_steps;
+        d.max_windows = mw;
+    }
+    d.n = n;
+    d.n_pad = np;
+    d.D = h->D;
+    d.t = 0;
+    d.tmod = 0;
+    d.t_end = h->t_end;
+    d.seed = cfg->seed;
+    d.n_inputs = net->n_inputs;
+    d.rec_rows = rec_rows;
+    d.dt = cfg->dt_ms;
+    d.decay_s = host_decay(cfg->dt_ms, cfg->synapse_tau_ms);
+    d.decay_t = host_decay(cfg->dt_ms, cfg->readout_tau_ms);
+    fill_noise(d, *cfg);
+    d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
+              (cfg->window_steps ? kNetWindows : 0u);
+    nets_[slot] = h;
+    NET_TRY(reset_net(slot));
+    NET_TRY(rebuild_tiles());
+#undef NET_TRY
+    *slot_out = slot;
+    return NE2B_OK;
+}
+
+ne2b_status Engine::remove_net(uint32_t slot) {
+    NetHost *h = net(slot);
+    if (!h) return set_error(NE2B_EINVAL, "no net in slot %u", slot);
+    NetDev z;
+    memset(&z, 0, sizeof z);
+    NE2B_CUDA(cudaMemcpyAsync(d_nets_ + slot, &z, sizeof z, cudaMemcpyHostToDevice, stream_));
+    for (void *p : h->allocs) NE2B_CUDA(cudaFreeAsync(p, stream_));
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    nets_[slot] = nullptr;
+    delete h;
+    return rebuild_tiles();
+}
+
+ne2b_status Engine::upload_net(NetHost &h) {
+    NE2B_CUDA(cudaMemcpyAsync(d_nets_ + h.slot, &h.dev, sizeof(NetDev), cudaMemcpyHostToDevice, stream_));
+    // h.dev may change right after this returns: wait for the copy
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return NE2B_OK;
+}
+
+uint32_t Engine::active_nets() const {
+    uint32_t c = 0;
+    for (NetHost *h : nets_) c += h != nullptr;
+    return c;
+}
+
+uint64_t Engine::dev_bytes() const {
+    uint64_t b = 0;
+    for (NetHost *h : nets_)
+        if (h) b += h->dev_bytes;
+    return b;
+}
+
+uint32_t Engine::grid() const {
+    uint32_t bps = shape_.blocks_per_sm;
+    const int occ = step_occupancy(int_ring_, shape_.block, shape_.npt);
+    if (bps == 0 || (int)bps > occ) bps = (uint32_t)(occ > 0 ? occ : 1);
+    uint32_t g = (uint32_t)sm_count_ * bps;
+    // never more blocks than tiles: idle blocks still cost launch time
+    const uint32_t nt = n_tiles_ ? n_tiles_ : 1;
+    return g < nt ? g : nt;
+}
+
+ne2b_status Engine::rebuild_tiles() {
+    const uint32_t tile = shape_.block * shape_.npt;
+    std::vector<Tile> tiles;
+    for (NetHost *h : nets_) {
+        if (!h) continue;
+        for (uint32_t start = 0; start < h->n_pad; start += tile) {
+            Tile t;
+            t.net = h->slot;
+            t.start = start;
+            t.count = std::min(tile, h->n_pad - start);
+            t.flags = 0;
+            if (!h->stim_ptr_host.empty()) {
+                const uint32_t lo = std::min(start, h->n), hi = std::min(start + t.count, h->n);
+                if (h->stim_ptr_host[hi] > h->stim_ptr_host[lo]) t.flags |= kTileHasStim;
+            }
+            tiles.push_back(t);
+        }
+    }
+    const uint32_t old_grid = grid();
+    if (tiles.size() > tiles_cap_) {
+        uint32_t cap = tiles_cap_;
+        while (cap < tiles.size()) cap *= 2;
+        NE2B_CUDA(cudaStreamSynchronize(stream_));
+        NE2B_CUDA(cudaFree(d_tiles_));
+        d_tiles_ = nullptr;
+        NE2B_CUDA(cudaMalloc(&d_tiles_, sizeof(Tile) * cap));
+        tiles_cap_ = cap;
+    }
+    if (!tiles.empty())
+        NE2B_CUDA(cudaMemcpyAsync(d_tiles_, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, stream_));
+    n_tiles_ = (uint32_t)tiles.size();
+    NE2B_TRY(upload_eng());
+    if (grid() != old_grid) clear_graphs();
+    return NE2B_OK;
+}
+
+ne2b_status Engine::set_shape(const TileShape &s) {
+    if (!shape_supported(s.block, s.npt))
+        return set_error(NE2B_EINVAL, "tile shape block=%u npt=%u is not compiled in", s.block, s.npt);
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    shape_ = s;
+    clear_graphs();
+    return rebuild_tiles();
+}
+
+ne2b_status Engine::reset_net(uint32_t slot) {
+    NetHost *hp = net(slot);
+    if (!hp) return set_error(NE2B_EINVAL, "no net in slot %u", slot);
+    NetHost &h = *hp;
+    NetDev &d = h.dev;
+    NE2B_CUDA(launch_reset_neurons(d, stream_));
+    NE2B_CUDA(cudaMemsetAsync(d.ring, 0, sizeof(uint32_t) * (size_t)h.D * h.n_pad, stream_));
+    if (d.rec_bits) NE2B_CUDA(cudaMemsetAsync(d.rec_bits, 0, sizeof(uint32_t) * (size_t)d.rec_rows * (h.n_pad / 32), stream_));
+    if (d.win_out) NE2B_CUDA(cudaMemsetAsync(d.win_out, 0, sizeof(uint16_t) * (size_t)d.max_windows * h.n_pad, stream_));
+    NE2B_CUDA(cudaMemsetAsync(d_counters_ + slot, 0, sizeof(NetCounters), stream_));
+    h.t = 0;
+    d.t = 0;
+    d.tmod = 0;
+    if (!h.fixed_stim) d.stim_len = 0;  // repack from t = 0
+    return upload_net(h);
+}
+
+ne2b_status Engine::sync() {
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::pack_stim(NetHost &h, uint64_t steps) {
+    const uint32_t ni = h.n_inputs;
+    h.pack_buf.resize((size_t)steps * ni);
+    for (uint64_t s = 0; s < steps; ++s)
+        for (uint32_t k = 0; k < ni; ++k) h.pack_buf[(size_t)s * ni + k] = h.stim.value(k, h.t + s);  // stim.rs:118-127
+    NE2B_CUDA(cudaMemcpyAsync((void *)h.dev.stim_buf, h.pack_buf.data(), sizeof(float) * h.pack_buf.size(),
+                              cudaMemcpyHostToDevice, stream_));
+    h.dev.stim_t0 = (long long)h.t;
+    h.dev.stim_len = (uint32_t)steps;
+    return upload_net(h);
+}
+
+ne2b_status Engine::launch_group(uint32_t steps) {
+    if (n_tiles_ == 0 || steps == 0) return NE2B_OK;
+    const uint32_t g = grid();
+    if (steps == graph_steps) {
+        auto it = graphs_.find(steps);
+        if (it == graphs_.end()) {
+            cudaGraph_t gr;
+            NE2B_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            cudaError_t err = cudaSuccess;
+            for (uint32_t k = 0; k < steps && err == cudaSuccess; ++k)
+                err = launch_step(int_ring_, shape_.block, shape_.npt, d_eng_, k, g, stream_);
+            if (err == cudaSuccess) err = launch_advance(d_nets_, nets_cap_, steps, stream_);
+            cudaError_t e2 = cudaStreamEndCapture(stream_, &gr);
+            if (err != cudaSuccess) return cuda_error(err, "step launch during capture");
+            NE2B_CUDA(e2);
+            cudaGraphExec_t ex;
+            cudaError_t e3 = cudaGraphInstantiate(&ex, gr, 0);
+            cudaGraphDestroy(gr);
+            NE2B_CUDA(e3);
+            it = graphs_.emplace(steps, ex).first;
+        }
+        NE2B_CUDA(cudaGraphLaunch(it->second, stream_));
+        return NE2B_OK;
+    }
+    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, shape_.block, shape_.npt, d_eng_, k, g, stream_));
+    NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::run_steps(uint64_t steps) {
+    NE2B_CUDA(cudaSetDevice(device_));
+    while (steps > 0) {
+        uint64_t chunk = steps;
+        for (NetHost *h : nets_)
+            if (h && h->stim_cap && !h->fixed_stim) chunk = std::min<uint64_t>(chunk, h->stim_cap);
+        for (NetHost *h : nets_) {
+            if (!h || !h->stim_cap || h->fixed_stim) continue;
+            const uint64_t lo = (uint64_t)h->dev.stim_t0, hi = lo + h->dev.stim_len;
+            if (!(h->dev.stim_len > 0 && h->t >= lo && h->t + chunk <= hi)) NE2B_TRY(pack_stim(*h, h->stim_cap));
+        }
+        uint64_t left = chunk;
+        while (left > 0) {
+            const uint32_t g = (uint32_t)std::min<uint64_t>(left, graph_steps);
+            NE2B_TRY(launch_group(g));
+            left -= g;
+        }
+        for (NetHost *h : nets_)
+            if (h) {
+                h->t = std::min<uint64_t>(h->t + chunk, h->t_end);
+                h->dev.t = h->t;
+                h->dev.tmod = (uint32_t)(h->t % h->D);
+            }
+        steps -= chunk;
+    }
+    return NE2B_OK;
+}
+
+ne2b_status Engine::read_f32(const float *dev, uint32_t n, float *out) {
+    if (n == 0) return NE2B_OK;
+    NE2B_CUDA(cudaMemcpyAsync(out, dev, sizeof(float) * n, cudaMemcpyDeviceToHost, stream_));
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::spike_counts(NetHost &h, uint64_t rows, uint32_t *out) {
+    const uint32_t n = h.n;
+    if (!h.dev.rec_rows || h.t == 0) {  // cpu.rs:425-428
+        memset(out, 0, sizeof(uint32_t) * n);
+        return NE2B_OK;
+    }
+    if (rows < h.t && rows > h.dev.rec_rows)
+        return set_error(NE2B_EWINDOW, "spike_counts window %llu exceeds the recorded %u steps",
+                         (unsigned long long)rows, h.dev.rec_rows);
+    if (n == 0) return NE2B_OK;
+    uint32_t *tmp = nullptr;
+    NE2B_CUDA(cudaMallocAsync((void **)&tmp, sizeof(uint32_t) * n, stream_));
+    cudaError_t e;
+    if (rows >= h.t) e = launch_pn_total(h.dev.pn_total, n, tmp, stream_);
+    else e = launch_window_count(h.dev.rec_bits, h.dev.rec_rows, h.n_pad, n, h.t, (uint32_t)rows, tmp, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, stream_);
+    cudaFreeAsync(tmp, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    return cuda_error(e, "spike_counts");
+}
+
+ne2b_status Engine::spike_row(NetHost &h, uint32_t back, uint64_t *out) {
+    const uint32_t rr = h.dev.rec_rows;
+    if (!rr || h.t == 0 || back >= h.t || back >= rr)  // cpu.rs:399-406
+        return set_error(NE2B_ENODATA, "spike_row %u is outside the recorded window", back);
+    const uint64_t t = h.t - 1 - back;
+    const uint32_t row = (uint32_t)(t % rr);
+    const uint32_t words = (h.n + 63) / 64;
+    NE2B_CUDA(cudaMemcpyAsync(out, h.dev.rec_bits + (size_t)row * (h.n_pad / 32), sizeof(uint64_t) * words,
+                              cudaMemcpyDeviceToHost, stream_));
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::spikes_total(NetHost &h, uint64_t *out) {
+    NE2B_CUDA(cudaMemcpyAsync(out, &d_counters_[h.slot].spikes_total, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream_));
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::window_counts(NetHost &h, uint32_t window, uint16_t *out) {
+    if (!h.dev.win_out) return set_error(NE2B_EINVAL, "window counts are off (window_steps = 0)");
+    if (window >= h.dev.max_windows) return set_error(NE2B_EINVAL, "window %u >= max_windows %u", window, h.dev.max_windows);
+    if (h.n == 0) return NE2B_OK;
+    NE2B_CUDA(cudaMemcpyAsync(out, h.dev.win_out + (size_t)window * h.n_pad, sizeof(uint16_t) * h.n,
+                              cudaMemcpyDeviceToHost, stream_));
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::set_ext(NetHost &h, const float *ext, uint32_t len) {
+    const uint32_t m = std::min(len, h.n);
+    for (uint32_t i = 0; i < m; ++i) h.ext_host[i] = ext[i];
+    bool any = false;
+    for (float x : h.ext_host) {
+        uint32_t b;
+        memcpy(&b, &x, 4);
+        if (b) { any = true; break; }
+    }
+    if (h.n) NE2B_CUDA(cudaMemcpyAsync(h.dev.ext, h.ext_host.data(), sizeof(float) * h.n, cudaMemcpyHostToDevice, stream_));
+    h.dev.flags = any ? (h.dev.flags | kNetHasExt) : (h.dev.flags & ~kNetHasExt);
+    return upload_net(h);
+}
+
+ne2b_status Engine::refresh_noise(NetHost &h) {
+    fill_noise(h.dev, h.cfg);
+    return upload_net(h);
+}
+
+// Snapshot of every mutable device array (state, ring, record, windows,
+// descriptors, counters) for the autotuner's trial runs.
+ne2b_status Engine::snapshot(std::vector<std::vector<uint8_t>> &snap) {
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    snap.clear();
+    auto grab = [&](const void *p, size_t bytes) -> ne2b_status {
+        std::vector<uint8_t> b(bytes);
+        if (bytes) NE2B_CUDA(cudaMemcpy(b.data(), p, bytes, cudaMemcpyDeviceToHost));
+        snap.push_back(std::move(b));
+        return NE2B_OK;
+    };
+    NE2B_TRY(grab(d_nets_, sizeof(NetDev) * nets_cap_));
+    NE2B_TRY(grab(d_counters_, sizeof(NetCounters) * nets_cap_));
+    for (NetHost *h : nets_) {
+        if (!h) continue;
+        const NetDev &d = h->dev;
+        const size_t np = h->n_pad;
+        NE2B_TRY(grab(d.v, 4 * np));
+        NE2B_TRY(grab(d.u, 4 * np));
+        NE2B_TRY(grab(d.s, 4 * np));
+        NE2B_TRY(grab(d.trace, 4 * np));
+        NE2B_TRY(grab(d.pn_total, 8 * np));
+        NE2B_TRY(grab(d.ring, 4 * (size_t)h->D * np));
+        NE2B_TRY(grab(d.rec_bits, d.rec_bits ? 4 * (size_t)d.rec_rows * (np / 32) : 0));
+        NE2B_TRY(grab(d.wcount, d.wcount ? 4 * np : 0));
+        NE2B_TRY(grab(d.win_out, d.win_out ? 2 * (size_t)d.max_windows * np : 0));
+    }
+    return NE2B_OK;
+}
+
+ne2b_status Engine::restore(const std::vector<std::vector<uint8_t>> &snap) {
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    size_t k = 0;
+    auto put = [&](void *p) -> ne2b_status {
+        const std::vector<uint8_t> &b = snap[k++];
+        if (!b.empty()) NE2B_CUDA(cudaMemcpy(p, b.data(), b.size(), cudaMemcpyHostToDevice));
+        return NE2B_OK;
+    };
+    NE2B_TRY(put(d_nets_));
+    NE2B_TRY(put(d_counters_));
+    for (NetHost *h : nets_) {
+        if (!h) continue;
+        NetDev &d = h->dev;
+        NE2B_TRY(put(d.v));
+        NE2B_TRY(put(d.u));
+        NE2B_TRY(put(d.s));
+        NE2B_TRY(put(d.trace));
+        NE2B_TRY(put(d.pn_total));
+        NE2B_TRY(put(d.ring));
+        NE2B_TRY(put(d.rec_bits));
+        NE2B_TRY(put(d.wcount));
+        NE2B_TRY(put(d.win_out));
+        // host mirrors follow the restored descriptor
+        const NetDev *dd = reinterpret_cast<const NetDev *>(snap[0].data()) + h->slot;
+        h->t = dd->t;
+        h->dev.t = dd->t;
+        h->dev.tmod = dd->tmod;
+        h->dev.stim_t0 = dd->stim_t0;
+        h->dev.stim_len = dd->stim_len;
+    }
+    return NE2B_OK;
+}
+
+// Time each compiled tile shape (and half occupancy) on the live nets for
+// `steps_per_trial` steps, restoring the state after every trial; keep the
+// fastest.
+ne2b_status Engine::autotune(uint32_t steps_per_trial) {
+    if (steps_per_trial == 0) steps_per_trial = graph_steps;
+    std::vector<std::vector<uint8_t>> snap;
+    NE2B_TRY(snapshot(snap));
+    uint32_t blocks[32], npts[32], count = 0;
+    shape_list(blocks, npts, &count);
+    TileShape best = shape_;
+    float best_ms = 1e30f;
+    for (uint32_t c = 0; c < count; ++c) {
+        const int occ = step_occupancy(int_ring_, blocks[c], npts[c]);
+        for (int half = 0; half < 2; ++half) {
+            TileShape s;
+            s.block = blocks[c];
+            s.npt = npts[c];
+            s.blocks_per_sm = half ? (uint32_t)std::max(1, occ / 2) : 0;
+            if (half && occ < 2) continue;
+            NE2B_TRY(set_shape(s));
+            NE2B_TRY(restore(snap));
+            NE2B_TRY(run_steps(graph_steps));  // capture + warm
+            NE2B_CUDA(cudaEventRecord(ev0_, stream_));
+            NE2B_TRY(run_steps(steps_per_trial));
+            NE2B_CUDA(cudaEventRecord(ev1_, stream_));
+            NE2B_CUDA(cudaEventSynchronize(ev1_));
+            float ms = 0.0f;
+            NE2B_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = s;
+            }
+        }
+    }
+    NE2B_TRY(set_shape(best));
+    NE2B_TRY(restore(snap));
+    last_ms_ = best_ms;
+    return NE2B_OK;
+}
+
+}  // namespace ne2b

@@ -1,0 +1,129 @@
+// ne2b_engine.h — host runtime of the B200 simulation core.
+//
+// An Engine owns one CUDA stream and a set of independent networks that are
+// stepped together: one persistent step kernel per dt step covers every
+// active net's tiles, and launch groups of `graph_steps` steps are replayed
+// from a captured CUDA graph.  A single sim (ne2b_sim) is an Engine with one
+// net; the batch runner and the serving loop are Engines with many.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/ne2b.h"
+#include "ne2b_layout.h"
+
+namespace ne2b {
+
+ne2b_status set_error(ne2b_status st, const char *fmt, ...);
+ne2b_status cuda_error(cudaError_t e, const char *what);
+
+// Host mirror of one network's stimulus program (sim/src/stim.rs:9-127).
+struct Stimulus {
+    std::vector<float> constants;
+    std::vector<std::vector<float>> series;
+    std::vector<uint64_t> play_start;
+    std::vector<uint8_t> looped;
+    float value(uint32_t k, uint64_t t) const;
+    void play(uint32_t k, uint64_t t, const float *v, uint64_t len, bool loop);
+};
+
+struct NetHost {
+    ne2b_config cfg{};
+    NetDev dev{};             // host mirror of the device descriptor
+    uint32_t slot = 0;        // index in the engine's net array
+    uint32_t n = 0, n_pad = 0, D = 0, n_inputs = 0;
+    uint64_t e = 0;
+    uint64_t t = 0;           // host mirror of dev.t
+    uint64_t t_end = ~0ull;
+    uint64_t dev_bytes = 0;
+    bool fixed_stim = false;  // serving: the input matrix is uploaded once
+    uint32_t stim_cap = 0;    // rows of stim_buf
+    Stimulus stim;
+    std::vector<float> ext_host;
+    std::vector<uint32_t> stim_ptr_host;  // for tile flags
+    std::vector<void *> allocs;
+    std::vector<float> pack_buf;
+};
+
+struct TileShape {
+    uint32_t block = 256;
+    uint32_t npt = 2;
+    uint32_t blocks_per_sm = 0;  // 0 = occupancy limit
+};
+
+class Engine {
+  public:
+    Engine() = default;
+    ~Engine();
+    ne2b_status init(int device, bool int_ring, uint32_t max_nets);
+
+    // Adds a net (slot returned).  inputs/steps: a fixed [steps x n_inputs]
+    // input matrix (serving); NULL = host-packed stimulus program.
+    ne2b_status add_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
+                        uint32_t *slot);
+    ne2b_status remove_net(uint32_t slot);
+    ne2b_status run_steps(uint64_t steps);
+    ne2b_status reset_net(uint32_t slot);
+    ne2b_status sync();
+    ne2b_status set_shape(const TileShape &s);
+    ne2b_status autotune(uint32_t steps_per_trial);
+    ne2b_status rebuild_tiles();
+    ne2b_status upload_net(NetHost &h);
+
+    ne2b_status read_f32(const float *dev, uint32_t n, float *out);
+    ne2b_status spike_counts(NetHost &h, uint64_t rows, uint32_t *out);
+    ne2b_status spike_row(NetHost &h, uint32_t back, uint64_t *out);
+    ne2b_status spikes_total(NetHost &h, uint64_t *out);
+    ne2b_status window_counts(NetHost &h, uint32_t window, uint16_t *out);
+    ne2b_status set_ext(NetHost &h, const float *ext, uint32_t len);
+    ne2b_status refresh_noise(NetHost &h);
+    ne2b_status snapshot(std::vector<std::vector<uint8_t>> &snap);
+    ne2b_status restore(const std::vector<std::vector<uint8_t>> &snap);
+
+    NetHost *net(uint32_t slot) { return slot < nets_.size() ? nets_[slot] : nullptr; }
+    uint32_t active_nets() const;
+    uint64_t dev_bytes() const;
+    float last_ms() const { return last_ms_; }
+    const TileShape &shape() const { return shape_; }
+    cudaStream_t stream() const { return stream_; }
+    bool int_ring() const { return int_ring_; }
+    uint32_t graph_steps = 64;
+    uint64_t stim_chunk = 2048;
+
+  private:
+    ne2b_status launch_group(uint32_t steps);
+    ne2b_status pack_stim(NetHost &h, uint64_t steps);
+    ne2b_status param_index(uint32_t model, const float *p, uint32_t np, uint16_t *idx);
+    ne2b_status upload_ptab();
+    ne2b_status upload_eng();
+    uint32_t grid() const;
+    void clear_graphs();
+
+    int device_ = 0;
+    int sm_count_ = 148;
+    bool int_ring_ = true;
+    cudaStream_t stream_ = nullptr;
+    std::vector<NetHost *> nets_;
+    NetDev *d_nets_ = nullptr;
+    NetCounters *d_counters_ = nullptr;
+    uint32_t nets_cap_ = 0;
+    std::vector<ParamRow> h_ptab_;
+    std::map<std::vector<uint32_t>, uint16_t> ptab_index_;
+    ParamRow *d_ptab_ = nullptr;
+    uint32_t ptab_cap_ = 0;
+    bool ptab_dirty_ = false;
+    Tile *d_tiles_ = nullptr;
+    uint32_t tiles_cap_ = 0;
+    uint32_t n_tiles_ = 0;
+    EngineDev *d_eng_ = nullptr;
+    TileShape shape_;
+    std::map<uint32_t, cudaGraphExec_t> graphs_;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    float last_ms_ = 0.0f;
+};
+
+}  // namespace ne2b

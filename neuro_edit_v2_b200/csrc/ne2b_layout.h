@@ -1,0 +1,102 @@
+// ne2b_layout.h — device-resident layout shared by the step kernel and the
+// host engine.
+//
+// HBM layout per network (every array is the net's own allocation, so nets
+// can be admitted and retired independently):
+//   neuron state, structure-of-arrays, n_pad = round_up(n, 64) entries:
+//     v, u (model state slots 0/1), s (merged synaptic current), trace,
+//     ext, v0/u0 (reset rows), pidx (u16 index into the param table),
+//     pn_total (u64 lifetime spike counts), wcount (u32 current-window counts)
+//   delay ring: D x n_pad words (int32 fixed point or f32), slot-major, so the
+//     neuron pass reads one contiguous slot row per step
+//   CSR by source: rowptr[n+1] (u32, local), tgt[E] (u32, local), w[E]
+//     (int32 = lrintf(w*4096) or f32), delay[E] (u8 when D <= 256, else u16)
+//   stimulus: neuron-major (input, weight) rows and a [steps x n_inputs] f32
+//     value buffer; spike record: rows x n_pad/32 u32 words; window counts:
+//     max_windows x n_pad u16.
+#pragma once
+#include <stdint.h>
+
+namespace ne2b {
+
+constexpr uint32_t kNeuronAlign = 64;  // n_pad multiple: one u64 record word never spans nets
+constexpr uint32_t kMaxParams = 12;
+
+enum NetFlags : uint32_t {
+    kNetHasExt = 1u << 0,
+    kNetDelay16 = 1u << 1,
+    kNetRecord = 1u << 2,
+    kNetWindows = 1u << 3,
+    kNetActive = 1u << 4,
+};
+
+enum TileFlags : uint32_t {
+    kTileHasStim = 1u << 0,
+};
+
+struct alignas(16) ParamRow {
+    float p[kMaxParams];
+    uint32_t model;  // registry id: 0 izh, 1 AdEx
+    uint32_t pad[3];
+};
+
+struct alignas(16) Tile {
+    uint32_t net;
+    uint32_t start;  // first local neuron
+    uint32_t count;  // neurons in this tile (<= tile size)
+    uint32_t flags;
+};
+
+// Per-network descriptor.  Device copy read by the kernels; the host keeps a
+// mirror and rewrites the fields it changes.
+struct alignas(16) NetDev {
+    // neuron arrays
+    float *v, *u, *s, *trace, *ext;
+    const float *v0, *u0;
+    const uint16_t *pidx;
+    unsigned long long *pn_total;
+    uint32_t *wcount;
+    // ring (int32 or f32 words)
+    void *ring;
+    // csr
+    const uint32_t *rowptr;
+    const uint32_t *tgt;
+    const void *w;          // int32 or f32
+    const void *delay;      // u8 or u16
+    // stimulus
+    const uint32_t *stim_ptr;
+    const uint32_t *stim_in;
+    const float *stim_w;
+    const float *stim_buf;  // [stim_len x n_inputs]
+    // spike record + windows
+    uint32_t *rec_bits;     // [rec_rows x n_pad/32]
+    uint16_t *win_out;      // [max_windows x n_pad]
+    // scalars
+    unsigned long long t;       // step index of the next launch group's k = 0
+    unsigned long long t_end;   // steps at or beyond this are skipped (serving)
+    long long stim_t0;          // step of stim_buf row 0
+    unsigned long long seed;
+    uint32_t n, n_pad, D, tmod;  // tmod = t % D
+    uint32_t n_inputs, stim_len;
+    uint32_t rec_rows, win_steps, max_windows, flags;
+    float dt, pkick, kick, decay_s, decay_t, gauss_k;
+    uint32_t pad[2];
+};
+
+// Mutable per-net counters, kept apart from the read-mostly descriptor.
+struct NetCounters {
+    unsigned long long spikes_total;
+};
+
+// Everything a step launch needs, in device memory so that a captured CUDA
+// graph stays valid when nets are admitted or retired.
+struct EngineDev {
+    const Tile *tiles;
+    uint32_t n_tiles;
+    uint32_t n_nets;
+    NetDev *nets;
+    const ParamRow *ptab;
+    NetCounters *counters;
+};
+
+}  // namespace ne2b

@@ -1,0 +1,328 @@
+"""Python mirror of the reference `sim::Backend` trait (sim/src/lib.rs:119-184)
+over the B200 C ABI.
+
+`B200Sim` exposes the same methods, argument meanings and error behaviour as
+`CpuSim` / `CudaSim` (sim/src/cpu.rs, sim/src/cuda.rs): stepping is
+asynchronous, every read synchronises, `spike_counts` raises on a window that
+the record ring can no longer answer, and editor-only calls (`set_v_watch`,
+`set_grid_watches`) are reported as unsupported.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import Ne2bError, check, lib, ptr
+
+
+class SpikeWindowError(Ne2bError):
+    """`spike_counts` window between the record depth and t (cpu.rs:437-442)."""
+
+
+def _cfg(cfg: _abi.Config | None, **kw) -> _abi.Config:
+    if cfg is None:
+        return _abi.default_config(**kw)
+    for k, v in kw.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+class B200Sim:
+    """One network on one B200: `Backend` with kind B200."""
+
+    def __init__(self, net, cfg: _abi.Config | None = None, device: int = 0, **cfg_kw):
+        self._net = net  # keeps the arrays behind the descriptor alive during create
+        self.cfg = _cfg(cfg, **cfg_kw)
+        h = C.c_void_p()
+        check(lib.ne2b_create(C.byref(net.desc()), C.byref(self.cfg), device, C.byref(h)))
+        self._h = h
+        n = C.c_uint32()
+        check(lib.ne2b_n(self._h, C.byref(n)))
+        self._n = int(n.value)
+        self.n_inputs = int(net.n_inputs)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.ne2b_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- Backend (sim/src/lib.rs:119-184) -------------------------------
+    def kind(self) -> str:
+        return "B200"
+
+    def n(self) -> int:
+        return self._n
+
+    def step_count(self) -> int:
+        t = C.c_uint64()
+        check(lib.ne2b_step_count(self._h, C.byref(t)))
+        return int(t.value)
+
+    def time_ms(self) -> float:
+        v = C.c_double()
+        check(lib.ne2b_time_ms(self._h, C.byref(v)))
+        return float(v.value)
+
+    def ring_depth(self) -> int:
+        d = C.c_uint32()
+        check(lib.ne2b_ring_depth(self._h, C.byref(d)))
+        return int(d.value)
+
+    def run_steps(self, n: int) -> None:
+        check(lib.ne2b_run_steps(self._h, int(n)))
+
+    def run_ms(self, ms: float) -> None:
+        check(lib.ne2b_run_ms(self._h, float(ms)))
+
+    def reset_state(self) -> None:
+        check(lib.ne2b_reset_state(self._h))
+
+    def synchronize(self) -> None:
+        check(lib.ne2b_synchronize(self._h))
+
+    def dev_mem_bytes(self) -> int:
+        b = C.c_uint64()
+        check(lib.ne2b_dev_mem_bytes(self._h, C.byref(b)))
+        return int(b.value)
+
+    def trace(self) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.float32)
+        check(lib.ne2b_read_trace(self._h, ptr(out)))
+        return out
+
+    def state(self, slot: int) -> np.ndarray:
+        if slot >= 2:
+            return np.zeros(0, dtype=np.float32)  # cpu.rs:346-349: empty for unknown slots
+        out = np.empty(self._n, dtype=np.float32)
+        check(lib.ne2b_read_state(self._h, slot, ptr(out)))
+        return out
+
+    def v(self) -> np.ndarray:
+        return self.state(0)
+
+    def syn_current(self) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.float32)
+        check(lib.ne2b_read_syn_current(self._h, ptr(out)))
+        return out
+
+    def last_spikes(self) -> np.ndarray:
+        cnt = C.c_uint32()
+        check(lib.ne2b_last_spikes(self._h, None, 0, C.byref(cnt)))
+        out = np.empty(max(cnt.value, 1), dtype=np.uint32)
+        check(lib.ne2b_last_spikes(self._h, ptr(out), cnt.value, C.byref(cnt)))
+        return out[: cnt.value]
+
+    def spike_counts(self, rows: int) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.uint32)
+        st = lib.ne2b_spike_counts(self._h, min(int(rows), 2**64 - 1), ptr(out))
+        if st == _abi.NE2B_EWINDOW:
+            raise SpikeWindowError(st, lib.ne2b_last_error().decode())
+        check(st)
+        return out
+
+    def spike_row(self, back: int) -> np.ndarray | None:
+        out = np.empty((self._n + 63) // 64, dtype=np.uint64)
+        st = lib.ne2b_spike_row(self._h, int(back), ptr(out))
+        if st == _abi.NE2B_ENODATA:
+            return None
+        check(st)
+        return out
+
+    def spikes_total(self) -> int:
+        v = C.c_uint64()
+        check(lib.ne2b_spikes_total(self._h, C.byref(v)))
+        return int(v.value)
+
+    def mean_rate_hz(self) -> float:
+        v = C.c_double()
+        check(lib.ne2b_mean_rate_hz(self._h, C.byref(v)))
+        return float(v.value)
+
+    def set_input_constant(self, input: int, value: float) -> None:
+        check(lib.ne2b_set_input_constant(self._h, input, value))
+
+    def input_values(self) -> np.ndarray:
+        out = np.empty(max(self.n_inputs, 1), dtype=np.float32)
+        check(lib.ne2b_input_values(self._h, ptr(out)))
+        return out[: self.n_inputs]
+
+    def play_input(self, input: int, series) -> None:
+        s = np.ascontiguousarray(series, dtype=np.float32)
+        check(lib.ne2b_play_input(self._h, input, ptr(s), len(s)))
+
+    def loop_input(self, input: int, series) -> None:
+        s = np.ascontiguousarray(series, dtype=np.float32)
+        check(lib.ne2b_loop_input(self._h, input, ptr(s), len(s)))
+
+    def external(self) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.float32)
+        check(lib.ne2b_external(self._h, ptr(out)))
+        return out
+
+    def set_external(self, neuron: int, amps: float) -> None:
+        check(lib.ne2b_set_external(self._h, neuron, amps))
+
+    def set_external_all(self, ext) -> None:
+        e = np.ascontiguousarray(ext, dtype=np.float32)
+        check(lib.ne2b_set_external_all(self._h, ptr(e), len(e)))
+
+    def set_noise(self, rate_hz: float, kick_mv: float) -> None:
+        check(lib.ne2b_set_noise(self._h, rate_hz, kick_mv))
+
+    def set_gauss_noise(self, sd: float) -> None:
+        check(lib.ne2b_set_gauss_noise(self._h, sd))
+
+    def set_v_watch(self, ids) -> None:
+        a = np.ascontiguousarray(ids, dtype=np.uint32)
+        check(lib.ne2b_set_v_watch(self._h, ptr(a), len(a)))
+
+    # --- on-device window counts (new) ---------------------------------
+    def windows_done(self) -> int:
+        c = C.c_uint32()
+        check(lib.ne2b_windows_done(self._h, C.byref(c)))
+        return int(c.value)
+
+    def window_counts(self, window: int) -> np.ndarray:
+        out = np.empty(self._n, dtype=np.uint16)
+        check(lib.ne2b_window_counts(self._h, window, ptr(out)))
+        return out
+
+
+class Batch:
+    """Many independent networks stepped together in one kernel per step."""
+
+    def __init__(self, nets, cfgs, device: int = 0):
+        self._nets = list(nets)
+        descs = (_abi.NetDesc * len(self._nets))(*[n.desc() for n in self._nets])
+        cfg_arr = (_abi.Config * len(cfgs))(*cfgs)
+        h = C.c_void_p()
+        check(lib.ne2b_batch_create(descs, cfg_arr, len(self._nets), device, C.byref(h)))
+        self._h = h
+        self.sizes = [int(n.n) for n in self._nets]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.ne2b_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def play_input(self, net: int, input: int, series) -> None:
+        s = np.ascontiguousarray(series, dtype=np.float32)
+        check(lib.ne2b_batch_play_input(self._h, net, input, ptr(s), len(s)))
+
+    def run_steps(self, n: int) -> None:
+        check(lib.ne2b_batch_run_steps(self._h, int(n)))
+
+    def reset_state(self) -> None:
+        check(lib.ne2b_batch_reset_state(self._h))
+
+    def synchronize(self) -> None:
+        check(lib.ne2b_batch_synchronize(self._h))
+
+    def window_counts(self, net: int, window: int) -> np.ndarray:
+        out = np.empty(self.sizes[net], dtype=np.uint16)
+        check(lib.ne2b_batch_window_counts(self._h, net, window, ptr(out)))
+        return out
+
+    def spikes_total(self, net: int) -> int:
+        v = C.c_uint64()
+        check(lib.ne2b_batch_spikes_total(self._h, net, C.byref(v)))
+        return int(v.value)
+
+    def state(self, net: int, slot: int) -> np.ndarray:
+        out = np.empty(self.sizes[net], dtype=np.float32)
+        check(lib.ne2b_batch_read_state(self._h, net, slot, ptr(out)))
+        return out
+
+    def autotune(self, steps_per_trial: int = 128) -> tuple[int, int, int]:
+        check(lib.ne2b_batch_autotune(self._h, steps_per_trial))
+        return self.tile_shape()
+
+    def tile_shape(self) -> tuple[int, int, int]:
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib.ne2b_batch_tile_shape(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return int(a.value), int(b.value), int(c.value)
+
+    def set_tile_shape(self, block: int, npt: int, blocks_per_sm: int = 0) -> None:
+        check(lib.ne2b_batch_set_tile_shape(self._h, block, npt, blocks_per_sm))
+
+    def dev_mem_bytes(self) -> int:
+        b = C.c_uint64()
+        check(lib.ne2b_batch_dev_mem_bytes(self._h, C.byref(b)))
+        return int(b.value)
+
+
+class Server:
+    """Continuous-batching trial server (admission by device footprint)."""
+
+    def __init__(self, neuron_capacity: int, synapse_capacity: int, ring_capacity: int, max_requests: int = 256,
+                 steps_per_launch: int = 100, int_weights: bool = True, device: int = 0):
+        c = _abi.ServerConfig(neuron_capacity, synapse_capacity, ring_capacity, max_requests, steps_per_launch,
+                              1 if int_weights else 0)
+        h = C.c_void_p()
+        check(lib.ne2b_server_create(C.byref(c), device, C.byref(h)))
+        self._h = h
+        self.int_weights = int_weights
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.ne2b_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, net, cfg: _abi.Config, inputs: np.ndarray, steps: int) -> int | None:
+        """Admit a request; None when it does not fit right now."""
+        x = np.ascontiguousarray(inputs, dtype=np.float32)
+        rid = C.c_uint64()
+        st = lib.ne2b_server_submit(self._h, C.byref(net.desc()), C.byref(cfg), ptr(x), int(steps), C.byref(rid))
+        if st == _abi.NE2B_EFULL:
+            return None
+        check(st)
+        return int(rid.value)
+
+    def step(self) -> tuple[int, int]:
+        a, f = C.c_uint32(), C.c_uint32()
+        check(lib.ne2b_server_step(self._h, C.byref(a), C.byref(f)))
+        return int(a.value), int(f.value)
+
+    def finished(self) -> list[int]:
+        cnt = C.c_uint32()
+        check(lib.ne2b_server_finished_ids(self._h, None, 0, C.byref(cnt)))
+        ids = np.zeros(max(cnt.value, 1), dtype=np.uint64)
+        check(lib.ne2b_server_finished_ids(self._h, ptr(ids), cnt.value, C.byref(cnt)))
+        return [int(x) for x in ids[: cnt.value]]
+
+    def take(self, rid: int) -> tuple[np.ndarray, int]:
+        n, w = C.c_uint32(), C.c_uint32()
+        check(lib.ne2b_server_result_shape(self._h, rid, C.byref(n), C.byref(w)))
+        out = np.zeros((w.value, n.value), dtype=np.uint16)
+        tot = C.c_uint64()
+        check(lib.ne2b_server_take_result(self._h, rid, ptr(out), C.byref(tot)))
+        return out, int(tot.value)
+
+    def stats(self) -> dict:
+        a, r, act, nu, su = C.c_uint64(), C.c_uint64(), C.c_uint32(), C.c_uint64(), C.c_uint64()
+        check(lib.ne2b_server_stats(self._h, C.byref(a), C.byref(r), C.byref(act), C.byref(nu), C.byref(su)))
+        return {"admitted": a.value, "retired": r.value, "active": act.value, "neurons_used": nu.value,
+                "synapses_used": su.value}
+
+
+def footprint(net, cfg: _abi.Config) -> tuple[int, int, int]:
+    a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    check(lib.ne2b_request_footprint(C.byref(net.desc()), C.byref(cfg), C.byref(a), C.byref(b), C.byref(c)))
+    return int(a.value), int(b.value), int(c.value)

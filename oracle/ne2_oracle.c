@@ -493,19 +493,20 @@ int ne2o_noise_fires(uint32_t i, uint64_t t, uint64_t seed, float p) {
     return (float)ne2o_noise_hash(i, t, seed) * 2.3283064e-10f < p;
 }
 /* Gaussian current noise (project definition, not in the reference): the
- * same (i, t, seed) base offset by 1*G and 2*G (G = 0xD1B54A32D192ED03)
- * through the splitmix64 finaliser gives four u32 uniforms; their sum S is
- * Irwin-Hall(4) with mean 2^33 and variance 2^64/3, so (S - 2^33) *
- * sqrt(3)/2^32 has mean 0 and variance 1.  Integer-exact on CPU and GPU. */
+ * (i, t, seed) base of noise_hash offset by G = 0xD1B54A32D192ED03 goes
+ * through the splitmix64 finaliser once; its four 16-bit fields are
+ * uniforms on [0, 65535] and their sum S is Irwin-Hall(4) with mean 131070
+ * and variance 4*(65536^2-1)/12, so (S - 131070) * sqrt(3)/65536 has mean 0
+ * and variance 1 - 2^-32.  Integer-exact on CPU and GPU; tails end at
+ * +-2*sqrt(3) sd. */
 int64_t ne2o_gauss_numer(uint32_t i, uint64_t t, uint64_t seed) {
-    uint64_t b = noise_base(i, t, seed);
-    uint64_t h0 = mix64(b + 0xD1B54A32D192ED03ull);
-    uint64_t h1 = mix64(b + 2ull * 0xD1B54A32D192ED03ull);
-    uint64_t s = (h0 & 0xffffffffull) + (h0 >> 32) + (h1 & 0xffffffffull) + (h1 >> 32);
-    return (int64_t)s - (int64_t)(1ull << 33);
+    uint64_t h = mix64(noise_base(i, t, seed) + 0xD1B54A32D192ED03ull);
+    int64_t s = (int64_t)(h & 0xffff) + (int64_t)((h >> 16) & 0xffff) + (int64_t)((h >> 32) & 0xffff) +
+                (int64_t)(h >> 48);
+    return s - 131070;
 }
 float ne2o_gauss_scale(float sd) {
-    return (float)((double)sd * 1.7320508075688772 / 4294967296.0);
+    return (float)((double)sd * 1.7320508075688772 / 65536.0);
 }
 
 /* ===================================================== deterministic exp */

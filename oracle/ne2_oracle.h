@@ -116,7 +116,8 @@ void ne2o_csr_free(ne2o_csr *c);
 uint32_t ne2o_noise_hash(uint32_t i, uint64_t t, uint64_t seed);
 int      ne2o_noise_fires(uint32_t i, uint64_t t, uint64_t seed, float p);
 /* Gaussian current noise (project definition): Irwin-Hall sum of four
- * counter-hashed u32 uniforms; returns the integer numerator S - 2^33. */
+ * 16-bit fields of one counter hash; returns the integer numerator
+ * S - 131070 (multiply by ne2o_gauss_scale(sd) for the current). */
 int64_t  ne2o_gauss_numer(uint32_t i, uint64_t t, uint64_t seed);
 float    ne2o_gauss_scale(float sd);
 

@@ -1,0 +1,83 @@
+"""Shared helpers of the GPU parity tests: run the B200 backend and the C
+oracle on the same flat network and compare rasters and state."""
+from __future__ import annotations
+
+import numpy as np
+
+import pyoracle as O
+import neuro_edit_v2_b200 as nb
+
+# int ring: rasters and every state bit must match the oracle exactly.
+# fp32 ring: the device sums ring arrivals with float atomics in arbitrary
+# order (kernels.rs:200 does the same), so rasters must match up to a first
+# divergence step and spike totals within FP32_COUNT_RTOL afterwards
+# (sim/tests/gpu_vs_cpu.rs:82-112 allows 25%).
+FP32_COUNT_RTOL = 0.25
+
+
+def configs(int_weights: bool, chunk: int, exp_mode: int = 1, **kw):
+    g = nb.default_config(record_spikes=1, spike_record_steps=chunk, int_weights=1 if int_weights else 0)
+    o = O.cfg(record_spikes=1, spike_record_steps=chunk, int_weights=1 if int_weights else 0, exp_mode=exp_mode)
+    for k, v in kw.items():
+        setattr(g, k, v)
+        setattr(o, k, v)
+    return g, o
+
+
+def rows_equal(g: nb.B200Sim, o: O.OSim, rows: int) -> int:
+    """Index (back) of the first differing record row, or -1."""
+    for back in range(rows - 1, -1, -1):
+        a = g.spike_row(back)
+        b = o.spike_row(back)
+        if (a is None) != (b is None) or (a is not None and not np.array_equal(a, b)):
+            return back
+    return -1
+
+
+def lockstep(onet: O.ONet, steps: int, int_weights: bool = True, chunk: int = 64, exp_mode: int = 1,
+             drive=None, flat=None, **cfg_kw):
+    """Run both backends `steps` steps in chunks; return (gpu, oracle,
+    first_divergent_step or -1)."""
+    flat = flat if flat is not None else onet.flat(cfg_kw.get("dt_ms", 0.1))
+    gc, oc = configs(int_weights, chunk, exp_mode, **cfg_kw)
+    g = nb.B200Sim(flat, gc)
+    o = O.OSim(onet, oc)
+    if drive:
+        drive(g)
+        drive(o)
+    first = -1
+    done = 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        g.run_steps(k)
+        o.run_steps(k)
+        bad = rows_equal(g, o, k)
+        if bad >= 0 and first < 0:
+            first = done + (k - 1 - bad)
+            if int_weights:
+                break
+        done += k
+    return g, o, first
+
+
+def set_ext(sim, n: int, idx, amps) -> None:
+    """Constant external current on the neurons `idx` of either backend."""
+    if isinstance(sim, nb.B200Sim):
+        ext = sim.external()
+        ext[np.asarray(idx)] = amps
+        sim.set_external_all(ext)
+    else:
+        for i in idx:
+            sim.set_external(int(i), float(amps))
+
+
+def assert_state_bits_equal(g: nb.B200Sim, o: O.OSim):
+    for slot in (0, 1):
+        a, b = g.state(slot), o.state(slot)
+        bad = np.flatnonzero(a.view(np.uint32) != b.view(np.uint32))
+        assert bad.size == 0, f"state {slot}: {bad.size} neurons differ, first {bad[:5]} {a[bad[:5]]} vs {b[bad[:5]]}"
+    for name, a, b in (("s", g.syn_current(), o.syn_current()), ("trace", g.trace(), o.trace())):
+        bad = np.flatnonzero(a.view(np.uint32) != b.view(np.uint32))
+        assert bad.size == 0, f"{name}: {bad.size} neurons differ, first {bad[:5]}"
+    assert g.spikes_total() == o.spikes_total()
+    assert np.array_equal(g.spike_counts(2**63), o.spike_counts(2**63))

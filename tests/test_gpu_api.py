@@ -1,0 +1,166 @@
+"""`Backend` semantics of the B200 sim through the C ABI, each against the
+reference test it mirrors (and the oracle where a value is compared)."""
+import numpy as np
+import pytest
+
+import pyoracle as O
+import neuro_edit_v2_b200 as nb
+from helpers import configs, set_ext
+
+pytestmark = pytest.mark.gpu
+
+
+def one_neuron(depth=64, **kw):
+    net = O.ONet()
+    net.add_neuron(0, 0, 0, O.EXC)
+    g, o = configs(True, depth, **kw)
+    return net, nb.B200Sim(net.flat(), g), O.OSim(net, o)
+
+
+def test_single_neuron_hand_computed_on_gpu():
+    """sim/tests/cpu_ref.rs:16-46"""
+    net, g, o = one_neuron()
+    g.set_external(0, 10.0)
+    g.run_steps(1)
+    assert abs(g.state(0)[0] - (-64.3)) < 1e-4
+    assert abs(g.state(1)[0] - (-12.99972)) < 1e-4
+
+
+def test_spike_bits_cleared_on_ring_wrap():
+    """sim/tests/spike_ring.rs:61-76"""
+    net, g, _ = one_neuron(64)
+    g.set_external(0, 40.0)
+    g.run_steps(64 * 20)
+    g.set_external(0, 0.0)
+    g.run_steps(200)
+    before = g.spikes_total()
+    g.run_steps(64)
+    assert g.spike_counts(64)[0] == g.spikes_total() - before
+
+
+def test_spike_counts_window_semantics():
+    """sim/tests/spike_ring.rs:78-91"""
+    net, g, o = one_neuron(64)
+    for s in (g, o):
+        s.set_external(0, 40.0)
+        s.run_steps(300)
+    direct = g.spike_counts(5000)[0]
+    assert direct > 0 and direct == g.spikes_total()
+    with pytest.raises(nb.SpikeWindowError):
+        g.spike_counts(200)
+    for rows in (1, 17, 64, 300, 10**9):
+        assert np.array_equal(g.spike_counts(rows), o.spike_counts(rows))
+
+
+def test_spike_row_and_last_spikes_outside_window():
+    net, g, o = one_neuron(8)
+    assert g.spike_row(0) is None and len(g.last_spikes()) == 0
+    g.set_external(0, 40.0)
+    o.set_external(0, 40.0)
+    for _ in range(30):
+        g.run_steps(1)
+        o.run_steps(1)
+        assert np.array_equal(g.last_spikes(), o.last_step_spikes())
+    assert g.spike_row(8) is None
+    assert g.spike_row(7) is not None
+
+
+def test_reset_clears_state_keeps_drive():
+    """sim/tests/cpu_ref.rs:322-334; reset keeps ext and stimulus (cpu.rs:155-157)"""
+    net = O.ONet()
+    for i in range(4):
+        net.add_neuron(i * 50.0, 0, 0, O.EXC)
+    net.connect(0, 1, 5.0)
+    g = nb.B200Sim(net.flat(), record_spikes=1, int_weights=1)
+    g.set_external(0, 30.0)
+    g.run_steps(50)
+    assert g.spikes_total() > 0
+    g.reset_state()
+    assert g.step_count() == 0 and g.spikes_total() == 0
+    assert np.all(g.state(0) == -65.0)
+    assert np.all(g.syn_current() == 0.0)
+    assert g.external()[0] == 30.0
+    g2 = nb.B200Sim(net.flat(), record_spikes=1, int_weights=1)
+    g2.set_external(0, 30.0)
+    g.run_steps(50)
+    g2.run_steps(50)
+    assert np.array_equal(g.v().view(np.uint32), g2.v().view(np.uint32))
+
+
+def test_stimulus_play_loop_and_constants_match_oracle():
+    """stim.rs play/loop/constant semantics through run_steps chunks."""
+    net = O.ONet()
+    for i in range(3):
+        net.add_neuron(i * 50.0, 0, 0, O.EXC)
+    net.add_input([(0, 1.0), (2, 2.0)])
+    net.add_input([(1, 3.0)])
+    gc, oc = configs(True, 64)
+    g = nb.B200Sim(net.flat(), gc)
+    o = O.OSim(net, oc)
+    ramp = np.linspace(0, 20, 37).astype(np.float32)
+    for s in (g, o):
+        s.set_input_constant(0, 5.0)
+        s.loop_input(1, [4.0, 0.0, 9.0])
+    for k in (7, 1, 100, 2500):
+        g.run_steps(k)
+        o.run_steps(k)
+    for s in (g, o):
+        s.play_input(0, ramp)
+    g.run_steps(3000)
+    o.run_steps(3000)
+    assert np.array_equal(g.v().view(np.uint32), o.state(0).view(np.uint32))
+    assert g.spikes_total() == o.spikes_total() > 0
+
+
+def test_set_noise_on_live_sim():
+    """lib.rs:183 set_noise; kernel args follow cfg (cuda.rs:807-810)."""
+    onet = O.ONet.random_kout(2000, 20, 3)
+    gc, oc = configs(True, 64)
+    g = nb.B200Sim(onet.flat(), gc)
+    o = O.OSim(onet, oc)
+    g.run_steps(100)
+    o.run_steps(100)
+    g.set_noise(800.0, 20.0)
+    o.set_noise(800.0, 20.0)
+    g.run_steps(500)
+    o.run_steps(500)
+    assert g.spikes_total() == o.spikes_total() > 0
+    assert np.array_equal(g.v().view(np.uint32), o.state(0).view(np.uint32))
+
+
+def test_empty_net_advances_clock():
+    """sim/tests/bounds.rs: an empty net runs (cuda.rs:585-590)."""
+    flat = nb.FlatNet(model=np.zeros(0, np.uint8), params=np.zeros((0, 4), np.float32),
+                      src_ptr=np.zeros(1, np.uint32), tgt=np.zeros(0, np.uint32), w=np.zeros(0, np.float32),
+                      delay_steps=np.zeros(0, np.uint16))
+    g = nb.B200Sim(flat, record_spikes=1)
+    g.run_steps(10)
+    assert g.step_count() == 10 and g.spikes_total() == 0
+    assert len(g.spike_counts(5)) == 0
+
+
+def test_unsupported_and_invalid_calls_are_errors():
+    net, g, _ = one_neuron()
+    with pytest.raises(nb.Ne2bError, match="UNSUPPORTED"):
+        g.set_v_watch([0])
+    with pytest.raises(nb.Ne2bError, match="EINVAL"):
+        g.set_input_constant(3, 1.0)
+    bad = net.flat()
+    bad.tgt = np.array([5], np.uint32)
+    bad.src_ptr = np.array([0, 1], np.uint32)
+    bad.w = np.array([1.0], np.float32)
+    bad.delay_steps = np.array([1], np.uint16)
+    with pytest.raises(nb.Ne2bError, match="EINVAL"):
+        nb.B200Sim(bad)
+
+
+def test_window_counts_equal_sliding_spike_counts():
+    """On-device per-window counts equal spike_counts(window) at each window end."""
+    onet = O.ONet.bench_net(3000, 50, 2, 0.7, 5.0)
+    g = nb.B200Sim(onet.flat(), record_spikes=1, spike_record_steps=250, int_weights=1, noise_rate_hz=500.0,
+                   window_steps=250, max_windows=8)
+    for w in range(6):
+        g.run_steps(250)
+        ref = g.spike_counts(250)
+        assert np.array_equal(g.window_counts(w).astype(np.uint32), ref)
+    assert g.windows_done() == 6

@@ -1,0 +1,371 @@
+"""The oracle against the reference's own known-answer tests.
+
+Each test restates one test of the reference (cited file:line) against the C
+restatement in oracle/.  Passing them pins the oracle to the Rust CPU path:
+above all the FNV fingerprint 0x9d792bd233132f5d of sim/tests/cpu_ref.rs:
+208-244 covers Rng, create_2d_grid, create_connections, synapse_csr, Poisson
+noise and the Izhikevich step bit-for-bit.
+"""
+import math
+import struct
+
+import numpy as np
+import pytest
+
+import pyoracle as O
+
+
+def net_with(n):
+    """cpu_ref.rs:8-14"""
+    net = O.ONet()
+    for i in range(n):
+        net.add_neuron(i * 50.0, 0.0, 0.0, O.EXC)
+    return net
+
+
+def f32(x):
+    return struct.unpack("f", struct.pack("f", x))[0]
+
+
+def test_default_tau_fingerprint():
+    """cpu_ref.rs:208-244 — the pinned bit-exact fingerprint."""
+    net = O.ONet()
+    r = O.rng(3)
+    m = net.create_2d_grid(8, 8, 30.0)
+    net.create_connections(m, 0.35, 80.0, 6.0, r)
+    sim = O.OSim(net, O.cfg(record_spikes=1, spike_record_steps=512, noise_rate_hz=20.0, noise_kick_mv=0.8, seed=7))
+    sim.run_steps(400)
+    assert sim.fingerprint(400) == 0x9D792BD233132F5D
+
+
+def test_single_neuron_step_matches_hand_computed():
+    """cpu_ref.rs:16-46"""
+    net = net_with(1)
+    sim = O.OSim(net, O.cfg())
+    sim.set_external(0, 10.0)
+    sim.run_steps(1)
+    assert abs(sim.state(0)[0] - (-64.3)) < 1e-4
+    assert abs(sim.state(1)[0] - (-12.99972)) < 1e-4
+    sim.run_steps(1)
+    v2 = -64.3 + 0.1 * (0.04 * 64.3 * 64.3 - 5.0 * 64.3 + 140.0 + 12.99972 + 10.0)
+    assert abs(sim.state(0)[0] - v2) < 1e-3
+
+
+def test_spike_resets_next_step():
+    """cpu_ref.rs:48-69"""
+    sim = O.OSim(net_with(1), O.cfg())
+    sim.set_external(0, 30.0)
+    for _ in range(200):
+        sim.run_steps(1)
+        if sim.trace()[0] > 0.9:
+            break
+    else:
+        pytest.fail("neuron should spike")
+    tr = sim.trace()[0]
+    sim.run_steps(1)
+    assert sim.state(0)[0] < -60.0
+    assert sim.trace()[0] < tr
+
+
+def _fire_once(sim, amps=25.0):
+    sim.set_external(0, amps)
+    for _ in range(500):
+        before = sim.spikes_total()
+        sim.run_steps(1)
+        if sim.spikes_total() > before:
+            return sim.t - 1
+    pytest.fail("no spike")
+
+
+def test_synapse_arrives_after_delay_and_decays():
+    """cpu_ref.rs:71-114"""
+    net = net_with(2)
+    net.push_synapse(0, 1, 30.0, 0.2, 0.0)
+    sim = O.OSim(net, O.cfg())
+    _fire_once(sim)
+    sim.set_external(0, 0.0)
+    sim.run_steps(1)
+    assert sim.syn_current()[1] == 0.0
+    sim.run_steps(1)
+    assert abs(sim.syn_current()[1] - 30.0 * math.exp(-0.1 / 2.0)) < 1e-3
+    sim.run_steps(1)
+    assert abs(sim.syn_current()[1] - 30.0 * math.exp(-0.05) ** 2) < 1e-2
+
+
+def test_no_self_connection_and_csr_order():
+    """cpu_ref.rs:246-255"""
+    net = net_with(3)
+    net.connect(0, 1, 5.0)
+    net.connect(0, 2, 6.0)
+    net.connect(2, 0, 7.0)
+    c = net.csr(0.1)
+    assert list(c["src_ptr"]) == [0, 2, 2, 3]
+    assert list(c["tgt"]) == [1, 2, 0]
+
+
+def test_stimulus_reaches_only_its_targets():
+    """cpu_ref.rs:257-275"""
+    net = net_with(3)
+    net.add_input([(0, 1.0), (2, 2.0)])
+    sim = O.OSim(net, O.cfg())
+    sim.set_input_constant(0, 5.0)
+    s1 = sim.syn_current()[1]
+    sim.run_steps(1)
+    assert sim.syn_current()[1] == s1
+    v = sim.state(0)
+    assert abs(v[2] - v[0]) > 0.05
+    assert abs(v[0] - -64.8) < 0.2
+
+
+def test_played_series_is_step_locked():
+    """cpu_ref.rs:277-303"""
+    net = net_with(1)
+    net.add_input([(0, 1.0)])
+    sim = O.OSim(net, O.cfg())
+    sim.play_input(0, [10.0, 0.0, 0.0])
+    sim.run_steps(1)
+    assert abs(sim.state(0)[0] - (-64.3)) < 1e-4
+    assert sim.stim_value(0, 3) == 0.0
+    sim.play_input(0, [25.0] * 20)
+    spiked = False
+    for _ in range(20):
+        sim.run_steps(1)
+        spiked |= sim.trace()[0] == 1.0
+    assert spiked
+
+
+def test_noise_is_deterministic_per_seed():
+    """cpu_ref.rs:305-320"""
+    net = net_with(64)
+    a = O.OSim(net, O.cfg(noise_rate_hz=500.0))
+    b = O.OSim(net, O.cfg(noise_rate_hz=500.0))
+    c = O.OSim(net, O.cfg(noise_rate_hz=500.0, seed=2))
+    for s in (a, b, c):
+        s.run_steps(100)
+    assert np.array_equal(a.state(0), b.state(0))
+    assert not np.array_equal(a.state(0), c.state(0))
+
+
+def test_reset_clears_state():
+    """cpu_ref.rs:322-334"""
+    net = net_with(4)
+    net.connect(0, 1, 5.0)
+    sim = O.OSim(net, O.cfg())
+    sim.set_external(0, 30.0)
+    sim.run_steps(50)
+    sim.reset_state()
+    assert sim.t == 0
+    assert np.all(sim.state(0) == -65.0)
+    assert np.all(sim.syn_current() == 0.0)
+
+
+def test_inhibitory_source_suppresses_target():
+    """cpu_ref.rs:339-394"""
+
+    def pair(inh, synapse):
+        net = O.ONet()
+        net.add_neuron(0, 0, 0, O.INH if inh else O.EXC)
+        net.add_neuron(60.0, 0, 0, O.EXC)
+        if synapse:
+            net.connect(0, 1, 6.0)
+        return net
+
+    def run(net):
+        sim = O.OSim(net, O.cfg(record_spikes=1))
+        sim.set_external(0, 30.0)
+        sim.set_external(1, 12.0)
+        sim.run_steps(4000)
+        return int(sim.spike_counts(2**63)[1])
+
+    free, inh, exc = run(pair(True, False)), run(pair(True, True)), run(pair(False, True))
+    assert free > 0 and inh < free and exc > inh
+    assert np.all(pair(True, True).csr()["w"] < 0)
+    assert np.all(pair(False, True).csr()["w"] > 0)
+
+
+def test_delay_over_ring_is_an_error():
+    """cpu_ref.rs:447-462"""
+    net = O.ONet()
+    net.add_neuron(0, 0, 0, O.EXC)
+    net.add_neuron(10, 0, 0, O.EXC)
+    net.push_synapse(0, 1, 1.0, 7000.0, 0.0)
+    with pytest.raises(ValueError, match="exceeds"):
+        net.csr(0.1)
+
+
+def test_custom_tau_arrives_then_decays():
+    """cpu_ref.rs:116-165"""
+    net = net_with(2)
+    net.push_synapse(0, 1, 30.0, 0.2, 20.0)
+    sim = O.OSim(net, O.cfg())
+    _fire_once(sim)
+    sim.set_external(0, 0.0)
+    sim.run_steps(1)
+    assert sim.syn_current()[1] == 0.0
+    sim.run_steps(1)
+    assert sim.syn_current()[1] == 0.0  # custom synapse must not feed merged s
+
+
+def test_tau_below_dt_decays_safely():
+    """cpu_ref.rs:467-498"""
+    net = O.ONet()
+    net.add_neuron(0, 0, 0, O.EXC)
+    net.add_neuron(10, 0, 0, O.EXC)
+    net.push_synapse(0, 1, 5.0, 1.0, 0.05)
+    sim = O.OSim(net, O.cfg(record_spikes=1))
+    sim.set_external(0, 30.0)
+    sim.run_steps(300)
+    assert np.all(np.isfinite(sim.state(1)))
+    s = sim.syn_current()
+    assert np.all(np.isfinite(s)) and np.all(s >= 0.0)
+
+
+def _splitmix64(x):
+    M = (1 << 64) - 1
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & M
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & M
+    return x ^ (x >> 31)
+
+
+def test_noise_hash_is_splitmix64():
+    """sim/tests/noise_hash.rs:15-33 (six golden tuples through an independent splitmix64)"""
+    M = (1 << 64) - 1
+    for i, t, seed in [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (7, 4096, 42),
+                       (0xFFFFFFFF, (2**64 - 1) // 2, 0xDEADBEEF)]:
+        base = (i * 0x9E3779B97F4A7C15 + t * 0xBF58476D1CE4E5B9 + seed * 0x94D049BB133111EB) & M
+        assert O.noise_hash(i, t, seed) == _splitmix64(base) >> 32
+
+
+def test_noise_streams_are_uncorrelated():
+    """sim/tests/noise_hash.rs:37-80 (agreement of p=0.1 streams ~ 0.82)"""
+    p = f32(0.1)
+    fires = np.zeros((101, 501), bool)
+    for i in range(101):
+        for t in range(501):
+            fires[i, t] = f32(float(O.noise_hash(i, t, 7)) * f32(2.3283064e-10)) < p
+    a = fires[:100, :500]
+    agree_n = np.mean(a == fires[1:101, :500])
+    agree_t = np.mean(a == fires[:100, 1:501])
+    assert abs(agree_n - 0.82) < 0.02 and abs(agree_t - 0.82) < 0.02
+    assert abs(a.mean() - 0.1) < 0.01
+
+
+def test_spike_bits_cleared_on_ring_wrap():
+    """sim/tests/spike_ring.rs:25-37"""
+    net = O.ONet()
+    net.add_neuron(0, 0, 0, O.EXC)
+    sim = O.OSim(net, O.cfg(record_spikes=1, spike_record_steps=64))
+    sim.set_external(0, 40.0)
+    sim.run_steps(64 * 20)
+    sim.set_external(0, 0.0)
+    sim.run_steps(200)
+    before = sim.spikes_total()
+    sim.run_steps(64)
+    assert sim.spike_counts(64)[0] == sim.spikes_total() - before
+
+
+def test_spike_counts_window_semantics():
+    """sim/tests/spike_ring.rs:41-59"""
+    net = O.ONet()
+    net.add_neuron(0, 0, 0, O.EXC)
+    sim = O.OSim(net, O.cfg(record_spikes=1, spike_record_steps=64))
+    sim.set_external(0, 40.0)
+    sim.run_steps(300)
+    direct = int(sim.pn_total()[0])
+    assert direct > 0
+    assert sim.spike_counts(5000)[0] == direct
+    assert sim.spike_counts(64)[0] <= direct
+    with pytest.raises(ValueError, match="exceeds"):
+        sim.spike_counts(200)
+
+
+def test_playing_one_input_does_not_restart_others():
+    """sim/tests/stim_playhead.rs:9-24"""
+    net = O.ONet()
+    net.add_neuron(0, 0, 0, O.EXC)
+    net.add_input([(0, 1.0)])
+    net.add_input([(0, 1.0)])
+    sim = O.OSim(net, O.cfg())
+    sim.play_input(0, np.arange(100, dtype=np.float32))
+    sim.run_steps(50)
+    before = sim.stim_value(0, sim.t)
+    sim.play_input(1, np.zeros(10, np.float32))
+    assert sim.stim_value(0, sim.t) == before == 50.0
+
+
+def test_looped_series_repeats():
+    """sim/src/stim.rs:501-527 (loop_input phase)"""
+    net = O.ONet()
+    net.add_neuron(0, 0, 0, O.EXC)
+    net.add_input([(0, 10.0)])
+    net.add_input([(0, 10.0)])
+    sim = O.OSim(net, O.cfg())
+    sim.loop_input(1, [1.0, 2.0, 3.0])
+    assert [sim.stim_value(1, t) for t in range(7)] == [1, 2, 3, 1, 2, 3, 1]
+    sim.run_steps(1000)
+    assert sim.stim_value(1, sim.t) == 2.0
+
+
+ADEX_TONIC = [281.0, 30.0, -70.6, -50.4, 2.0, 4.0, 144.0, 80.5, -70.6, 20.0]
+
+
+def test_adex_mixed_net_fires_on_cpu():
+    """sim/tests/adex.rs:296-323"""
+    for exp_mode in (0, 1):
+        net = net_with(8)
+        for i in (1, 3, 6):
+            net.set_model(i, O.ADEX, ADEX_TONIC)
+        sim = O.OSim(net, O.cfg(record_spikes=1, exp_mode=exp_mode))
+        for i in (1, 3, 6):
+            sim.set_external(i, 1000.0)
+        sim.run_steps(3000)
+        c = sim.spike_counts(2**63)
+        assert all(c[i] >= 2 for i in (1, 3, 6)), c
+
+
+def test_adex_v_cut_at_vpeak():
+    """sim/tests/adex.rs:251-276 (every per-step v <= Vpeak)"""
+    net = O.ONet()
+    net.add_neuron(0, 0, 0, O.EXC)
+    net.set_model(0, O.ADEX, ADEX_TONIC)
+    sim = O.OSim(net, O.cfg(record_spikes=1, exp_mode=1))
+    sim.set_external(0, 1000.0)
+    vmax = -1e9
+    for _ in range(3000):
+        sim.step()
+        vmax = max(vmax, sim.state(0)[0])
+    assert sim.spike_counts(2**63)[0] >= 2
+    assert vmax <= 20.0
+
+
+def test_det_expf_against_libm():
+    """The deterministic exp of the AdEx step stays within 1 ulp of glibc expf
+    on a strided sweep of its argument range; the full sweep is recorded in the
+    design notes."""
+    import ctypes
+
+    libm = ctypes.CDLL("libm.so.6")
+    libm.expf.restype = ctypes.c_float
+    libm.expf.argtypes = [ctypes.c_float]
+    xs = np.concatenate([np.linspace(-103.0, 10.0, 20001, dtype=np.float32),
+                         np.array([0.0, -0.0, 1e-30, -1e-30, 88.7, 10.0, -87.3], np.float32)])
+    worst = 0
+    mism = 0
+    for x in xs:
+        a = O.det_expf(float(x))
+        b = libm.expf(float(x))
+        ia = struct.unpack("<i", struct.pack("<f", a))[0]
+        ib = struct.unpack("<i", struct.pack("<f", b))[0]
+        worst = max(worst, abs(ia - ib))
+        mism += ia != ib
+    assert worst <= 1
+    assert mism <= len(xs) // 100
+
+
+def test_gauss_noise_moments():
+    """Project noise definition: mean 0, variance 1 - 2^-32 on a seeded sample."""
+    z = np.array([O.gauss_numer(i, t, 5) for i in range(200) for t in range(200)], dtype=np.float64)
+    z *= math.sqrt(3.0) / 65536.0
+    assert abs(z.mean()) < 0.02
+    assert abs(z.var() - 1.0) < 0.03
+    assert np.abs(z).max() <= 2 * math.sqrt(3.0)

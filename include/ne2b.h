@@ -133,6 +133,12 @@ ne2b_status ne2b_external(ne2b_sim *sim, float *out);
 ne2b_status ne2b_set_noise(ne2b_sim *sim, float rate_hz, float kick_mv);
 ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd);                 /* new */
 
+/* Instrumentation (new): the CUDA stream the handle launches on (a
+ * cudaStream_t, for timing with events on the launching stream) and the
+ * number of kernels the handle has launched so far. */
+ne2b_status ne2b_stream(ne2b_sim *sim, void **stream);
+ne2b_status ne2b_kernel_launches(ne2b_sim *sim, uint64_t *launches);
+
 /* Editor observability (lib.rs:164-176): not provided by this backend. */
 ne2b_status ne2b_set_v_watch(ne2b_sim *sim, const uint32_t *ids, uint32_t count);
 ne2b_status ne2b_set_grid_watches(ne2b_sim *sim, const uint32_t *members, const uint32_t *group_ptr,
@@ -164,6 +170,8 @@ ne2b_status ne2b_batch_set_tile_shape(ne2b_batch *b, uint32_t block, uint32_t ne
                                       uint32_t blocks_per_sm);
 ne2b_status ne2b_batch_dev_mem_bytes(ne2b_batch *b, uint64_t *bytes);
 ne2b_status ne2b_batch_last_step_ms(ne2b_batch *b, float *ms);
+ne2b_status ne2b_batch_stream(ne2b_batch *b, void **stream);
+ne2b_status ne2b_batch_kernel_launches(ne2b_batch *b, uint64_t *launches);
 
 /* -------------------------------------------------------------- serving */
 /* Continuous batching of trial requests: requests are admitted into free
@@ -199,6 +207,8 @@ ne2b_status ne2b_server_take_result(ne2b_server *s, uint64_t request_id, uint16_
 ne2b_status ne2b_server_finished_ids(ne2b_server *s, uint64_t *ids, uint32_t cap, uint32_t *count);
 ne2b_status ne2b_server_stats(ne2b_server *s, uint64_t *admitted, uint64_t *retired, uint32_t *active,
                               uint64_t *neurons_used, uint64_t *synapses_used);
+ne2b_status ne2b_server_stream(ne2b_server *s, void **stream);
+ne2b_status ne2b_server_kernel_launches(ne2b_server *s, uint64_t *launches);
 
 /* ----------------------------------------------------------- net building */
 /* A host-side network owned by the library, in the ne2b_net_desc layout. */

@@ -138,6 +138,12 @@ _SIGS = {
     "ne2b_external": (C.c_int, [_p, _p]),
     "ne2b_set_noise": (C.c_int, [_p, _f32, _f32]),
     "ne2b_set_gauss_noise": (C.c_int, [_p, _f32]),
+    "ne2b_stream": (C.c_int, [_p, C.POINTER(_p)]),
+    "ne2b_kernel_launches": (C.c_int, [_p, _pu64]),
+    "ne2b_batch_stream": (C.c_int, [_p, C.POINTER(_p)]),
+    "ne2b_batch_kernel_launches": (C.c_int, [_p, _pu64]),
+    "ne2b_server_stream": (C.c_int, [_p, C.POINTER(_p)]),
+    "ne2b_server_kernel_launches": (C.c_int, [_p, _pu64]),
     "ne2b_set_v_watch": (C.c_int, [_p, _p, _u32]),
     "ne2b_set_grid_watches": (C.c_int, [_p, _p, _p, _u32]),
     "ne2b_batch_create": (C.c_int, [C.POINTER(NetDesc), C.POINTER(Config), _u32, C.c_int, C.POINTER(_p)]),

@@ -305,6 +305,18 @@ ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd) {
     return sim->eng.refresh_noise(*h);
 }
 
+ne2b_status ne2b_stream(ne2b_sim *sim, void **stream) {
+    if (!sim || !stream) return set_error(NE2B_EINVAL, "null argument");
+    *stream = (void *)sim->eng.stream();
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_kernel_launches(ne2b_sim *sim, uint64_t *launches) {
+    if (!sim || !launches) return set_error(NE2B_EINVAL, "null argument");
+    *launches = sim->eng.launches();
+    return NE2B_OK;
+}
+
 ne2b_status ne2b_set_v_watch(ne2b_sim *sim, const uint32_t *ids, uint32_t count) {
     (void)sim; (void)ids; (void)count;
     return set_error(NE2B_UNSUPPORTED, "v-watch recording is not provided by the B200 backend");
@@ -429,6 +441,18 @@ ne2b_status ne2b_batch_dev_mem_bytes(ne2b_batch *b, uint64_t *bytes) {
 ne2b_status ne2b_batch_last_step_ms(ne2b_batch *b, float *ms) {
     if (!b) return set_error(NE2B_EINVAL, "null batch handle");
     *ms = b->eng.last_ms();
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_batch_stream(ne2b_batch *b, void **stream) {
+    if (!b || !stream) return set_error(NE2B_EINVAL, "null argument");
+    *stream = (void *)b->eng.stream();
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_batch_kernel_launches(ne2b_batch *b, uint64_t *launches) {
+    if (!b || !launches) return set_error(NE2B_EINVAL, "null argument");
+    *launches = b->eng.launches();
     return NE2B_OK;
 }
 
@@ -584,6 +608,18 @@ ne2b_status ne2b_server_stats(ne2b_server *s, uint64_t *admitted, uint64_t *reti
     if (active) *active = act;
     if (neurons_used) *neurons_used = s->used_neurons;
     if (synapses_used) *synapses_used = s->used_syn;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_server_stream(ne2b_server *s, void **stream) {
+    if (!s || !stream) return set_error(NE2B_EINVAL, "null argument");
+    *stream = (void *)s->eng.stream();
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_server_kernel_launches(ne2b_server *s, uint64_t *launches) {
+    if (!s || !launches) return set_error(NE2B_EINVAL, "null argument");
+    *launches = s->eng.launches();
     return NE2B_OK;
 }
 

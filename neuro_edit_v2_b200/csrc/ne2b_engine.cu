@@ -499,6 +499,7 @@ ne2b_status Engine::reset_net(uint32_t slot) {
     NetHost &h = *hp;
     NetDev &d = h.dev;
     NE2B_CUDA(launch_reset_neurons(d, stream_));
+    launches_ += d.n_pad ? 1 : 0;
     NE2B_CUDA(cudaMemsetAsync(d.ring, 0, sizeof(uint32_t) * (size_t)h.D * h.n_pad, stream_));
     if (d.rec_bits) NE2B_CUDA(cudaMemsetAsync(d.rec_bits, 0, sizeof(uint32_t) * (size_t)d.rec_rows * (h.n_pad / 32), stream_));
     if (d.win_out) NE2B_CUDA(cudaMemsetAsync(d.win_out, 0, sizeof(uint16_t) * (size_t)d.max_windows * h.n_pad, stream_));
@@ -549,10 +550,12 @@ ne2b_status Engine::launch_group(uint32_t steps) {
             it = graphs_.emplace(steps, ex).first;
         }
         NE2B_CUDA(cudaGraphLaunch(it->second, stream_));
+        launches_ += steps + 1;
         return NE2B_OK;
     }
     for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, shape_.block, shape_.npt, d_eng_, k, g, stream_));
     NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
+    launches_ += steps + 1;
     return NE2B_OK;
 }
 
@@ -606,6 +609,7 @@ ne2b_status Engine::spike_counts(NetHost &h, uint64_t rows, uint32_t *out) {
     cudaError_t e;
     if (rows >= h.t) e = launch_pn_total(h.dev.pn_total, n, tmp, stream_);
     else e = launch_window_count(h.dev.rec_bits, h.dev.rec_rows, h.n_pad, n, h.t, (uint32_t)rows, tmp, stream_);
+    launches_ += 1;
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, stream_);
     cudaFreeAsync(tmp, stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);

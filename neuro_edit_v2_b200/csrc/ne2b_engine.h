@@ -91,6 +91,7 @@ class Engine {
     const TileShape &shape() const { return shape_; }
     cudaStream_t stream() const { return stream_; }
     bool int_ring() const { return int_ring_; }
+    uint64_t launches() const { return launches_; }
     uint32_t graph_steps = 64;
     uint64_t stim_chunk = 2048;
 
@@ -124,6 +125,7 @@ class Engine {
     std::map<uint32_t, cudaGraphExec_t> graphs_;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     float last_ms_ = 0.0f;
+    uint64_t launches_ = 0;  // kernels launched (graph nodes counted per replay)
 };
 
 }  // namespace ne2b

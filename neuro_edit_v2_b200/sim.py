@@ -187,6 +187,18 @@ class B200Sim:
         a = np.ascontiguousarray(ids, dtype=np.uint32)
         check(lib.ne2b_set_v_watch(self._h, ptr(a), len(a)))
 
+    # --- instrumentation (new) ------------------------------------------
+    def stream_handle(self) -> int:
+        """The cudaStream_t this sim launches on (for CUDA-event timing)."""
+        p = C.c_void_p()
+        check(lib.ne2b_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def kernel_launches(self) -> int:
+        v = C.c_uint64()
+        check(lib.ne2b_kernel_launches(self._h, C.byref(v)))
+        return int(v.value)
+
     # --- on-device window counts (new) ---------------------------------
     def windows_done(self) -> int:
         c = C.c_uint32()
@@ -264,6 +276,16 @@ class Batch:
         check(lib.ne2b_batch_dev_mem_bytes(self._h, C.byref(b)))
         return int(b.value)
 
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        check(lib.ne2b_batch_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def kernel_launches(self) -> int:
+        v = C.c_uint64()
+        check(lib.ne2b_batch_kernel_launches(self._h, C.byref(v)))
+        return int(v.value)
+
 
 class Server:
     """Continuous-batching trial server (admission by device footprint)."""
@@ -314,6 +336,16 @@ class Server:
         tot = C.c_uint64()
         check(lib.ne2b_server_take_result(self._h, rid, ptr(out), C.byref(tot)))
         return out, int(tot.value)
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        check(lib.ne2b_server_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def kernel_launches(self) -> int:
+        v = C.c_uint64()
+        check(lib.ne2b_server_kernel_launches(self._h, C.byref(v)))
+        return int(v.value)
 
     def stats(self) -> dict:
         a, r, act, nu, su = C.c_uint64(), C.c_uint64(), C.c_uint32(), C.c_uint64(), C.c_uint64()

@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 simulation core on the 100k-neuron workload.
+
+Workload (one bench step): a 1000 ms trial (10,000 steps at dt 0.1 ms) of the
+100,000-neuron random K=100 Izhikevich network (80% RS / 20% FS, positions
+U(-500,500)^3 um, delay = distance / 100 um/ms capped at 20 ms, |w| exc
+U(0,0.5), inh U(0,1), x0.7, Dale's law), tau_syn 5 ms, Gaussian current noise
+sd 1, fixed-point (int32, scale 4096) delay ring, reset to the initial state
+at the start of every trial.  Inputs (the ~10M-synapse CSR, ~130 MB with the
+ring) exceed the 126 MB L2, and L2 is also scrubbed between timed steps.
+
+Prints ONE JSON line (rank 0).  `value` is neuron-updates/s timed with CUDA
+events on the engine's stream; `e2e` is the same trial through the public C
+ABI with the host<->device copies in the timed region; `roofline` relates the
+step kernel's algorithmic bytes to the measured HBM peak; `cpu_baseline` is
+the C restatement of the reference CPU step (single thread, as the reference
+CpuSim) on a bounded sample of the same workload.
+
+`--impl reference` times that CPU restatement (the reference is Rust and
+cannot be built in this image) on the same workload and prints its line.
+With torchrun (N > 1) every rank runs an independent replica (replicas only:
+the path has no exchange step); value = all ranks' neuron-updates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 100_000
+K_OUT = 100
+TRIAL_STEPS = 10_000  # 1000 ms at dt 0.1
+SEED = 1
+B_NEURON = 60  # algorithmic bytes per Izhikevich neuron-update
+B_SPIKE = 24   # per spike
+B_EVENT = 17   # per delivered synaptic event
+ACTIVE_KICK_HZ = 100.0  # companion regime: Poisson kicks (sim/src/state.rs:15-22)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                except ValueError:
+                    continue
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, r in rows for k in range(4) if r[k].lower().startswith("active")})
+        load = [r[0] for r in rows if r[0] > 300] or [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def make_cfg(nb, active: bool):
+    return nb.default_config(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0,
+                             noise_rate_hz=ACTIVE_KICK_HZ if active else 0.0, noise_kick_mv=20.0, seed=SEED)
+
+
+def timed_trials(sim, steps: int, warmup: int, trial_steps: int, ws: int, torch, scrub):
+    """Run warmup + steps trials; return (total device ms, spikes, launches)."""
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    for _ in range(warmup):
+        sim.reset_state()
+        sim.run_steps(trial_steps)
+    sim.synchronize()
+    total_ms = 0.0
+    spikes = 0
+    launches0 = sim.kernel_launches()
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            scrub.fill_(1)  # L2 flush: 256 MB write, outside the timed interval
+        barrier(ws)
+        sim.synchronize()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.reset_state()
+        sim.run_steps(trial_steps)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        spikes += sim.spikes_total()
+    launches = sim.kernel_launches() - launches0
+    return total_ms, spikes, launches
+
+
+def run_profile(args):
+    """Short run for ncu: 3 warm-up trials + 1 trial of --trial-steps steps."""
+    import torch
+
+    import neuro_edit_v2_b200 as nb
+
+    net = nb.random_kout(N, K_OUT, SEED)
+    sim = nb.B200Sim(net, make_cfg(nb, args.active))
+    scrub = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
+    ms, spikes, launches = timed_trials(sim, 1, 3, args.trial_steps, 1, torch, scrub)
+    print(json.dumps({"profile_run": True, "trial_steps": args.trial_steps, "ms": ms, "spikes": spikes,
+                      "launches": launches}), flush=True)
+
+
+def run_ours(args):
+    ws, rank, local = dist_setup()
+    import numpy as np
+    import torch
+
+    import neuro_edit_v2_b200 as nb
+
+    torch.cuda.set_device(local)
+    dev = local
+    net = nb.random_kout(N, K_OUT, SEED + rank)
+    sim = nb.B200Sim(net, make_cfg(nb, False), device=dev)
+    scrub = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    with Clocks(dev) as clk:
+        total_ms, spikes, launches = timed_trials(sim, args.steps, args.warmup, TRIAL_STEPS, ws, torch, scrub)
+    total_ms = max_over_ranks(total_ms, ws)
+    n_updates = float(N) * TRIAL_STEPS * args.steps
+    value = sum_over_ranks(n_updates, ws) / (total_ms / 1000.0)
+    events = spikes * K_OUT
+    step_launches = TRIAL_STEPS * args.steps
+    launch_ms = total_ms / step_launches
+    alg_bytes = B_NEURON * N + B_SPIKE * spikes / step_launches + B_EVENT * events / step_launches
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (launch_ms / 1000.0) / 1e9
+    tr = load_traffic()
+
+    # active companion regime (same net, Poisson kicks on top)
+    act = nb.B200Sim(net, make_cfg(nb, True), device=dev)
+    a_ms, a_spikes, _ = timed_trials(act, max(1, args.steps // 2), 1, TRIAL_STEPS, ws, torch, scrub)
+    a_ms = max_over_ranks(a_ms, ws)
+    a_trials = max(1, args.steps // 2)
+    a_events = a_spikes * K_OUT
+    a_alg = B_NEURON * N + (B_SPIKE * a_spikes + B_EVENT * a_events) / (TRIAL_STEPS * a_trials)
+    del act
+
+    # end to end through the public API: pinned host drive in, v out
+    ext = torch.zeros(N, dtype=torch.float32).pin_memory().numpy()
+    e2e_steps = args.steps
+    sim.synchronize()
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.set_external_all(ext)
+        sim.reset_state()
+        sim.run_steps(TRIAL_STEPS)
+        v = sim.v()
+        tot = sim.spikes_total()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, ws)
+    e2e_val = sum_over_ranks(n_updates / args.steps * e2e_steps, ws) / e2e_s
+    del v, tot
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(TRIAL_STEPS)
+
+    line = {
+        "metric": "neuron-updates/s (synaptic events/s reported beside)",
+        "value": value,
+        "unit": "neuron-updates/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 state, int32 fixed-point ring",
+        "data": "synthetic: seeded generator of the 100k configuration (random K=100, distance delays)",
+        "config": {"workload": "100k izh random K=100, 1000 ms trial at dt 0.1 ms, Gaussian noise sd 1, "
+                               "tau_syn 5 ms, int32 ring",
+                   "neurons": N, "synapses": N * K_OUT, "trial_steps": TRIAL_STEPS, "ring_depth": sim.ring_depth(),
+                   "l2": "scrubbed (256 MB write) between timed steps; inputs ~130 MB > L2",
+                   "parallelism": f"replicas x{ws}"},
+        "synaptic_events_per_s": events / (total_ms / 1000.0) * ws,
+        "firing_rate_hz": spikes / (N * args.steps * TRIAL_STEPS * 1e-4),
+        "active_regime": {
+            "what": f"same net + Poisson kicks {ACTIVE_KICK_HZ:g} Hz x 20 mV",
+            "neuron_updates_per_s": float(N) * TRIAL_STEPS * a_trials / (a_ms / 1000.0) * ws,
+            "synaptic_events_per_s": a_events / (a_ms / 1000.0) * ws,
+            "firing_rate_hz": a_spikes / (N * a_trials * TRIAL_STEPS * 1e-4),
+            "ms_per_trial": a_ms / a_trials,
+            "roofline_frac": a_alg / (a_ms / (TRIAL_STEPS * a_trials) / 1000.0) / 1e9 / peak,
+        },
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                     "alg_bytes_per_launch": alg_bytes, "launch_us": launch_ms * 1000.0,
+                     "traffic": (tr or {}).get("bytes_per_launch"),
+                     "traffic_source": (tr or {}).get("source")},
+        "e2e": {"value": e2e_val, "unit": "neuron-updates/s", "h2d_bytes_per_step": 4 * N,
+                "d2h_bytes_per_step": 4 * N + 8},
+        "gpu_launches": launches,
+        "cpu_baseline": cpu,
+    }
+    line["clocks"] = clk.summary()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def cpu_baseline_sample(sample_steps: int):
+    """The C restatement of the reference CPU step (single thread) on the
+    same 100k net and config, `sample_steps` steps of the trial."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+
+    onet = O.ONet.random_kout(N, K_OUT, SEED)
+    sim = O.OSim(onet, O.cfg(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0, seed=SEED))
+    t0 = time.perf_counter()
+    sim.run_steps(sample_steps)
+    dt = time.perf_counter() - t0
+    return {"value": N * sample_steps / dt, "unit": "neuron-updates/s", "cores": 1, "kind": "port",
+            "sample": f"100k net, first {sample_steps} steps ({sample_steps / 10:g} ms) of the trial, "
+                      f"{dt:.1f} s on 1 host core (the reference CpuSim is single-threaded)",
+            "cpu": cpu_model()}
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip() + f" ({os.cpu_count()} cores visible)"
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+
+    sample = 500  # steps per bench step (50 ms of the 1000 ms trial)
+    onet = O.ONet.random_kout(N, K_OUT, SEED)
+    sim = O.OSim(onet, O.cfg(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0, seed=SEED))
+    for _ in range(args.warmup):
+        sim.run_steps(sample // 5)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.run_steps(sample)
+    dt = time.perf_counter() - t0
+    value = N * sample * args.steps / dt
+    print(json.dumps({
+        "impl": "reference",
+        "metric": "neuron-updates/s (synaptic events/s reported beside)",
+        "value": value, "unit": "neuron-updates/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1000.0 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 state, int32 fixed-point ring",
+        "data": "synthetic: seeded generator of the 100k configuration (random K=100, distance delays)",
+        "config": {"workload": "100k izh random K=100, 1000 ms trial at dt 0.1 ms, Gaussian noise sd 1, "
+                               "tau_syn 5 ms, int32 ring", "neurons": N, "synapses": N * K_OUT},
+        "cpu_baseline": {"value": value, "unit": "neuron-updates/s", "cores": 1, "kind": "port",
+                         "sample": f"{sample} steps of the 100k trial per bench step on 1 host core "
+                                   "(C restatement of the single-threaded reference CpuSim; the Rust "
+                                   "reference cannot be built here)", "cpu": cpu_model()},
+        "e2e": {"value": value, "unit": "neuron-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="short run for ncu captures")
+    ap.add_argument("--trial-steps", type=int, default=200, help="trial length in --profile mode")
+    ap.add_argument("--active", action="store_true", help="--profile the active (Poisson-kick) regime")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

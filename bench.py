@@ -25,6 +25,8 @@ from __future__ import annotations
 
 import argparse
 import json
+
+import numpy as np
 import os
 import statistics
 import subprocess
@@ -259,6 +261,18 @@ def run_ours(args):
     e2e_val = sum_over_ranks(n_updates / args.steps * e2e_steps, ws) / e2e_s
     del v, tot
 
+    extra = {}
+    if not args.no_extras and ws == 1:
+        peak_v, _ = load_peaks()
+        for name, fn in (("c1m_izh", lambda: bench_1m(nb, torch, scrub, nb.MODEL_IZH, 2, 3, peak_v)),
+                         ("c1m_adex", lambda: bench_1m(nb, torch, scrub, nb.MODEL_ADEX, 2, 3, peak_v)),
+                         ("batched_256", lambda: bench_batched(nb, torch, scrub, 2, 3)),
+                         ("serving", lambda: bench_serving(nb, args.serving_requests))):
+            try:
+                extra[name] = fn()
+            except Exception as e:  # report, never hide
+                extra[name] = {"error": repr(e)}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(TRIAL_STEPS)
@@ -300,6 +314,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": 4 * N + 8},
         "gpu_launches": launches,
         "cpu_baseline": cpu,
+        "extra": extra,
     }
     line["clocks"] = clk.summary()
     if rank == 0:
@@ -308,6 +323,167 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------- extras
+def bench_1m(nb, torch, scrub, model: int, steps: int, warmup: int, peak: float):
+    """1,000,000 neurons x K=100 (~100M synapses), 500 ms trials, izh or AdEx
+    (AdEx weights x C = 281 pF so a weight moves v by the same mV)."""
+    n, trial = 1_000_000, 5000
+    adex = model == nb.MODEL_ADEX
+    net = nb.random_kout(n, K_OUT, SEED, w_scale=0.7 * (281.0 if adex else 1.0))
+    if adex:
+        nb.to_adex(net)
+    sim = nb.B200Sim(net, nb.default_config(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0, seed=SEED))
+    del net
+    ms, spikes, launches = timed_trials(sim, steps, warmup, trial, 1, torch, scrub)
+    per_launch_s = ms / 1000.0 / (trial * steps)
+    b_neuron = 84 if adex else B_NEURON
+    alg = b_neuron * n + (B_SPIKE * spikes + B_EVENT * spikes * K_OUT) / (trial * steps)
+    achieved = alg / per_launch_s / 1e9
+    out = {"neurons": n, "synapses": n * K_OUT, "trial_steps": trial, "ring_depth": sim.ring_depth(),
+           "neuron_updates_per_s": n * trial * steps / (ms / 1000.0),
+           "synaptic_events_per_s": spikes * K_OUT / (ms / 1000.0),
+           "firing_rate_hz": spikes / (n * steps * trial * 1e-4), "ms_per_trial": ms / steps,
+           "roofline": {"achieved_gbs": achieved, "frac": achieved / peak, "alg_bytes_per_launch": alg,
+                        "launch_us": per_launch_s * 1e6, "bytes_per_neuron": b_neuron},
+           "gpu_launches": launches, "dev_mem_bytes": sim.dev_mem_bytes()}
+    sim.close()
+    return out
+
+
+def batch_trials(b, torch, scrub, steps: int, warmup: int, trial: int):
+    stream = torch.cuda.ExternalStream(b.stream_handle())
+    for _ in range(warmup):
+        b.reset_state()
+        b.run_steps(trial)
+    b.synchronize()
+    total = 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            scrub.fill_(1)
+        b.synchronize()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.reset_state()
+        b.run_steps(trial)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total
+
+
+def bench_batched(nb, torch, scrub, steps: int, warmup: int, serial_sample: int = 32):
+    from neuro_edit_v2_b200 import workloads as W
+
+    nets, inputs = W.batched_liquids(256)
+    trial = TRIAL_STEPS
+    wins = trial // W.WINDOW_STEPS
+    cfgs = [nb.default_config(int_weights=1, window_steps=W.WINDOW_STEPS, max_windows=wins, seed=k)
+            for k in range(len(nets))]
+    b = nb.Batch(nets, cfgs)
+    for k, x in enumerate(inputs):
+        b.set_input_matrix(k, x)
+    shape = b.autotune(128)
+    total_ms = batch_trials(b, torch, scrub, steps, warmup, trial)
+    neurons = sum(n.n for n in nets)
+    events = 0
+    spikes = 0
+    for k, net in enumerate(nets):
+        deg = W.outdegree(net)
+        for w in range(wins):
+            c = b.window_counts(k, w).astype(np.int64)
+            spikes += int(c.sum())
+            events += int((c * deg).sum())
+    launches = b.kernel_launches()
+    b.close()
+    # the same kernels, one network at a time, on a sample of the set
+    ser_ms = 0.0
+    for k in range(serial_sample):
+        one = nb.Batch([nets[k]], [cfgs[k]])
+        one.set_input_matrix(0, inputs[k])
+        ser_ms += batch_trials(one, torch, scrub, 1, 1, trial)
+        one.close()
+    batched_tps = len(nets) * steps / (total_ms / 1000.0)
+    serial_tps = serial_sample / (ser_ms / 1000.0)
+    return {"nets": len(nets), "neurons": neurons, "synapses": sum(n.n_syn for n in nets), "trial_steps": trial,
+            "windows_per_trial": wins, "tile_shape": {"block": shape[0], "neurons_per_thread": shape[1],
+                                                      "blocks_per_sm": shape[2]},
+            "trials_per_s": batched_tps, "ms_per_batch_trial": total_ms / steps,
+            "neuron_updates_per_s": neurons * trial * steps / (total_ms / 1000.0),
+            "synaptic_events_per_s": events / (total_ms / 1000.0 / steps),
+            "firing_rate_hz": spikes / (neurons * trial * 1e-4),
+            "serial_trials_per_s": serial_tps, "serial_sample": serial_sample,
+            "batched_vs_serial": batched_tps / serial_tps}
+
+
+def bench_serving(nb, count: int):
+    from neuro_edit_v2_b200 import workloads as W
+
+    reqs = W.request_stream(count)
+
+    def serve(arrivals):
+        srv = nb.Server(neuron_capacity=16 << 20, synapse_capacity=1 << 30, ring_capacity=6 << 30,
+                        max_requests=512, steps_per_launch=100)
+        order = sorted(range(count), key=lambda r: arrivals[r])
+        lat = [0.0] * count
+        ids = {}
+        nxt = 0
+        done = 0
+        refused = 0
+        t0 = time.perf_counter()
+        while done < count:
+            now = time.perf_counter() - t0
+            while nxt < count and arrivals[order[nxt]] <= now:
+                r = order[nxt]
+                rid = srv.submit(reqs[r].net, W.request_config(reqs[r], 11 + r), reqs[r].inputs, reqs[r].steps)
+                if rid is None:
+                    refused += 1
+                    break
+                ids[rid] = r
+                nxt += 1
+            if srv.stats()["active"] == 0:
+                if nxt < count:
+                    time.sleep(max(0.0, arrivals[order[nxt]] - (time.perf_counter() - t0)))
+                continue
+            srv.step()
+            for rid in srv.finished():
+                counts, _ = srv.take(rid)
+                r = ids[rid]
+                lat[r] = time.perf_counter() - t0 - arrivals[r]
+                done += 1
+        span = time.perf_counter() - t0
+        srv.close()
+        return lat, span, refused
+
+    arrivals = [q.arrival_s for q in reqs]
+    lat, span, refused = serve(arrivals)
+    sat_lat, sat_span, _ = serve([0.0] * count)
+    # one at a time: each request alone, back to back (sample)
+    sample = min(24, count)
+    t0 = time.perf_counter()
+    for r in range(sample):
+        srv = nb.Server(neuron_capacity=1 << 20, synapse_capacity=1 << 28, ring_capacity=1 << 30, max_requests=1,
+                        steps_per_launch=100)
+        srv.submit(reqs[r].net, W.request_config(reqs[r], 11 + r), reqs[r].inputs, reqs[r].steps)
+        while srv.stats()["active"]:
+            srv.step()
+        srv.close()
+    one_tps = sample / (time.perf_counter() - t0)
+    q = np.quantile(np.array(lat), [0.5, 0.99])
+    sq = np.quantile(np.array(sat_lat), [0.5, 0.99])
+    neuron_steps = sum(q_.n * q_.steps for q_ in reqs)
+    return {"requests": count, "offered_rate_hz": 200.0, "trials_per_s": count / span, "p50_ms": q[0] * 1e3,
+            "p99_ms": q[1] * 1e3, "refused_admissions": refused,
+            "saturated": {"trials_per_s": count / sat_span, "p50_ms": sq[0] * 1e3, "p99_ms": sq[1] * 1e3,
+                          "neuron_updates_per_s": neuron_steps / sat_span},
+            "one_at_a_time_trials_per_s": one_tps, "one_at_a_time_sample": sample,
+            "served_vs_one_at_a_time": (count / span) / one_tps,
+            "saturated_vs_one_at_a_time": (count / sat_span) / one_tps,
+            "mean_neurons": float(np.mean([q_.n for q_ in reqs])),
+            "mean_steps": float(np.mean([q_.steps for q_ in reqs]))}
 
 
 def cpu_baseline_sample(sample_steps: int):
@@ -380,6 +556,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the 1M, batched and serving measurements")
+    ap.add_argument("--serving-requests", type=int, default=200)
     ap.add_argument("--profile", action="store_true", help="short run for ncu captures")
     ap.add_argument("--trial-steps", type=int, default=200, help="trial length in --profile mode")
     ap.add_argument("--active", action="store_true", help="--profile the active (Poisson-kick) regime")

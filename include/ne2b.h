@@ -155,6 +155,10 @@ ne2b_status ne2b_batch_create(const ne2b_net_desc *nets, const ne2b_config *cfgs
 ne2b_status ne2b_batch_destroy(ne2b_batch *b);
 ne2b_status ne2b_batch_play_input(ne2b_batch *b, uint32_t net, uint32_t input, const float *series,
                                   uint64_t len);
+/* A fixed [steps x n_inputs] input matrix for one net, uploaded once and
+ * read on the device from the net's current step on (new; replaces the
+ * host-packed stimulus program for that net). */
+ne2b_status ne2b_batch_set_input_matrix(ne2b_batch *b, uint32_t net, const float *inputs, uint64_t steps);
 ne2b_status ne2b_batch_run_steps(ne2b_batch *b, uint64_t steps);
 ne2b_status ne2b_batch_reset_state(ne2b_batch *b);
 ne2b_status ne2b_batch_synchronize(ne2b_batch *b);

@@ -149,6 +149,7 @@ _SIGS = {
     "ne2b_batch_create": (C.c_int, [C.POINTER(NetDesc), C.POINTER(Config), _u32, C.c_int, C.POINTER(_p)]),
     "ne2b_batch_destroy": (C.c_int, [_p]),
     "ne2b_batch_play_input": (C.c_int, [_p, _u32, _u32, _p, _u64]),
+    "ne2b_batch_set_input_matrix": (C.c_int, [_p, _u32, _p, _u64]),
     "ne2b_batch_run_steps": (C.c_int, [_p, _u64]),
     "ne2b_batch_reset_state": (C.c_int, [_p]),
     "ne2b_batch_synchronize": (C.c_int, [_p]),

@@ -375,6 +375,11 @@ ne2b_status ne2b_batch_play_input(ne2b_batch *b, uint32_t net, uint32_t input, c
     })());
 }
 
+ne2b_status ne2b_batch_set_input_matrix(ne2b_batch *b, uint32_t net, const float *inputs, uint64_t steps) {
+    CHECK_BATCH_NET(b, net);
+    GUARD(b->eng.set_input_matrix(*h, inputs, steps));
+}
+
 ne2b_status ne2b_batch_run_steps(ne2b_batch *b, uint64_t steps) {
     if (!b) return set_error(NE2B_EINVAL, "null batch handle");
     GUARD(b->eng.run_steps(steps));

@@ -84,6 +84,7 @@ Engine::~Engine() {
         delete h;
     }
     if (stream_) cudaStreamSynchronize(stream_);
+    if (stage_) cudaFreeHost(stage_);
     cudaFree(d_nets_);
     cudaFree(d_counters_);
     cudaFree(d_ptab_);
@@ -516,15 +517,80 @@ ne2b_status Engine::sync() {
     return NE2B_OK;
 }
 
-ne2b_status Engine::pack_stim(NetHost &h, uint64_t steps) {
-    const uint32_t ni = h.n_inputs;
-    h.pack_buf.resize((size_t)steps * ni);
-    for (uint64_t s = 0; s < steps; ++s)
-        for (uint32_t k = 0; k < ni; ++k) h.pack_buf[(size_t)s * ni + k] = h.stim.value(k, h.t + s);  // stim.rs:118-127
-    NE2B_CUDA(cudaMemcpyAsync((void *)h.dev.stim_buf, h.pack_buf.data(), sizeof(float) * h.pack_buf.size(),
-                              cudaMemcpyHostToDevice, stream_));
+ne2b_status Engine::stage_reserve(size_t bytes) {
+    if (bytes <= stage_bytes_) return NE2B_OK;
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    if (stage_) cudaFreeHost(stage_);
+    stage_ = nullptr;
+    stage_bytes_ = 0;
+    size_t cap = 1 << 20;
+    while (cap < bytes) cap *= 2;
+    NE2B_CUDA(cudaMallocHost(&stage_, cap));
+    stage_bytes_ = cap;
+    return NE2B_OK;
+}
+
+// Pack the stimulus program of every net in `nets` for steps [t, t + rows)
+// (stim.rs:118-127 Stimulus::pack) into one pinned staging buffer, copy each
+// to its device buffer, then copy every net descriptor, and synchronise once.
+ne2b_status Engine::pack_stim(const std::vector<NetHost *> &nets) {
+    size_t bytes = 0;
+    for (NetHost *h : nets) bytes += sizeof(float) * (size_t)h->stim_cap * h->n_inputs;
+    bytes = (bytes + 255) / 256 * 256;
+    NE2B_TRY(stage_reserve(bytes + sizeof(NetDev) * nets_cap_));
+    uint8_t *base = (uint8_t *)stage_;
+    size_t off = 0;
+    for (NetHost *h : nets) {
+        const uint32_t ni = h->n_inputs;
+        const uint64_t rows = h->stim_cap;
+        float *dst = (float *)(base + off);
+        for (uint64_t r = 0; r < rows; ++r)
+            for (uint32_t k = 0; k < ni; ++k) dst[(size_t)r * ni + k] = h->stim.value(k, h->t + r);
+        const size_t b = sizeof(float) * (size_t)rows * ni;
+        NE2B_CUDA(cudaMemcpyAsync((void *)h->dev.stim_buf, dst, b, cudaMemcpyHostToDevice, stream_));
+        h->dev.stim_t0 = (long long)h->t;
+        h->dev.stim_len = (uint32_t)rows;
+        off += b;
+    }
+    NetDev *mirror = (NetDev *)(base + bytes);
+    for (uint32_t j = 0; j < nets_cap_; ++j) {
+        if (nets_[j]) mirror[j] = nets_[j]->dev;
+        else memset(&mirror[j], 0, sizeof(NetDev));
+    }
+    NE2B_CUDA(cudaMemcpyAsync(d_nets_, mirror, sizeof(NetDev) * nets_cap_, cudaMemcpyHostToDevice, stream_));
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return NE2B_OK;
+}
+
+// A fixed [steps x n_inputs] input matrix, device-resident from the current
+// step on: nothing is packed during runs (batched and served trials).
+ne2b_status Engine::set_input_matrix(NetHost &h, const float *x, uint64_t steps) {
+    if (!h.n_inputs || h.stim_ptr_host.empty()) return NE2B_OK;  // no stimulus routing
+    if (steps == 0 || !x) return set_error(NE2B_EINVAL, "empty input matrix");
+    if (steps > 0xffffffffull) return set_error(NE2B_EINVAL, "input matrix longer than 2^32-1 steps");
+    const size_t bytes = sizeof(float) * (size_t)steps * h.n_inputs;
+    void *p = nullptr;
+    NE2B_CUDA(cudaMallocAsync(&p, bytes, stream_));
+    cudaError_t e = cudaMemcpyAsync(p, x, bytes, cudaMemcpyHostToDevice, stream_);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(p, stream_);
+        return cuda_error(e, "input matrix upload");
+    }
+    void *old = (void *)h.dev.stim_buf;
+    for (auto &a : h.allocs)
+        if (a == old) {
+            NE2B_CUDA(cudaFreeAsync(old, stream_));
+            h.dev_bytes -= sizeof(float) * (size_t)(h.fixed_stim ? h.dev.stim_len : h.stim_cap) * h.n_inputs;
+            a = p;
+            old = nullptr;
+            break;
+        }
+    if (old) h.allocs.push_back(p);
+    h.dev_bytes += bytes;
+    h.dev.stim_buf = (const float *)p;
     h.dev.stim_t0 = (long long)h.t;
     h.dev.stim_len = (uint32_t)steps;
+    h.fixed_stim = true;
     return upload_net(h);
 }
 
@@ -565,11 +631,13 @@ ne2b_status Engine::run_steps(uint64_t steps) {
         uint64_t chunk = steps;
         for (NetHost *h : nets_)
             if (h && h->stim_cap && !h->fixed_stim) chunk = std::min<uint64_t>(chunk, h->stim_cap);
+        std::vector<NetHost *> repack;
         for (NetHost *h : nets_) {
             if (!h || !h->stim_cap || h->fixed_stim) continue;
             const uint64_t lo = (uint64_t)h->dev.stim_t0, hi = lo + h->dev.stim_len;
-            if (!(h->dev.stim_len > 0 && h->t >= lo && h->t + chunk <= hi)) NE2B_TRY(pack_stim(*h, h->stim_cap));
+            if (!(h->dev.stim_len > 0 && h->t >= lo && h->t + chunk <= hi)) repack.push_back(h);
         }
+        if (!repack.empty()) NE2B_TRY(pack_stim(repack));
         uint64_t left = chunk;
         while (left > 0) {
             const uint32_t g = (uint32_t)std::min<uint64_t>(left, graph_steps);

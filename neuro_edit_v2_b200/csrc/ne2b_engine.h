@@ -80,6 +80,7 @@ class Engine {
     ne2b_status spikes_total(NetHost &h, uint64_t *out);
     ne2b_status window_counts(NetHost &h, uint32_t window, uint16_t *out);
     ne2b_status set_ext(NetHost &h, const float *ext, uint32_t len);
+    ne2b_status set_input_matrix(NetHost &h, const float *x, uint64_t steps);
     ne2b_status refresh_noise(NetHost &h);
     ne2b_status snapshot(std::vector<std::vector<uint8_t>> &snap);
     ne2b_status restore(const std::vector<std::vector<uint8_t>> &snap);
@@ -97,7 +98,8 @@ class Engine {
 
   private:
     ne2b_status launch_group(uint32_t steps);
-    ne2b_status pack_stim(NetHost &h, uint64_t steps);
+    ne2b_status pack_stim(const std::vector<NetHost *> &nets);
+    ne2b_status stage_reserve(size_t bytes);
     ne2b_status param_index(uint32_t model, const float *p, uint32_t np, uint16_t *idx);
     ne2b_status upload_ptab();
     ne2b_status upload_eng();
@@ -126,6 +128,8 @@ class Engine {
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     float last_ms_ = 0.0f;
     uint64_t launches_ = 0;  // kernels launched (graph nodes counted per replay)
+    void *stage_ = nullptr;  // pinned staging for stimulus chunks and descriptors
+    size_t stage_bytes_ = 0;
 };
 
 }  // namespace ne2b

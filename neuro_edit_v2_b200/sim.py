@@ -235,6 +235,11 @@ class Batch:
         s = np.ascontiguousarray(series, dtype=np.float32)
         check(lib.ne2b_batch_play_input(self._h, net, input, ptr(s), len(s)))
 
+    def set_input_matrix(self, net: int, inputs) -> None:
+        """Device-resident [steps x n_inputs] inputs of one net from its current step."""
+        x = np.ascontiguousarray(inputs, dtype=np.float32)
+        check(lib.ne2b_batch_set_input_matrix(self._h, net, ptr(x), x.shape[0]))
+
     def run_steps(self, n: int) -> None:
         check(lib.ne2b_batch_run_steps(self._h, int(n)))
 

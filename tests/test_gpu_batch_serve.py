@@ -123,3 +123,29 @@ def test_server_rejects_oversized_request():
     big = nb.liquid(10, 1)
     with pytest.raises(nb.Ne2bError, match="total capacity"):
         srv.submit(big, cfg(1), streams(0, 100), 100)
+
+
+def test_batch_input_matrix_equals_played_series():
+    """Device-resident input matrices give the same trial as the host-packed
+    stimulus program (stim.rs:118-127) across chunk boundaries."""
+    nets = liquids()[:3]
+    cfgs = [cfg(40 + k) for k in range(3)]
+    steps = 4500  # crosses the 2048-step packing chunks
+    a = nb.Batch(nets, cfgs)
+    b = nb.Batch(nets, cfgs)
+    for k in range(3):
+        x = streams(50 + k, steps)
+        a.set_input_matrix(k, x)
+        for i in range(8):
+            b.play_input(k, i, x[:, i])
+    a.run_steps(steps)
+    b.run_steps(steps)
+    for k in range(3):
+        assert a.spikes_total(k) == b.spikes_total(k) > 0
+        for w in range(16):
+            assert np.array_equal(a.window_counts(k, w), b.window_counts(k, w))
+    # a second trial after reset replays the same matrix from t = 0
+    tot = [a.spikes_total(k) for k in range(3)]
+    a.reset_state()
+    a.run_steps(steps)
+    assert [a.spikes_total(k) for k in range(3)] == tot

@@ -133,6 +133,16 @@ ne2b_status ne2b_external(ne2b_sim *sim, float *out);
 ne2b_status ne2b_set_noise(ne2b_sim *sim, float rate_hz, float kick_mv);
 ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd);                 /* new */
 
+/* Step kernel selection (new): NE2B_KERNEL_AUTO picks the resident
+ * persistent kernel when every net's state fits in shared memory, else the
+ * streaming kernel; the other two force one (RESIDENT fails with
+ * NE2B_UNSUPPORTED when the nets do not fit).  *resident reports which
+ * kernel runs.  The environment variable NE2B_KERNEL=stream|resident sets
+ * the initial mode of every handle. */
+enum { NE2B_KERNEL_AUTO = 0, NE2B_KERNEL_STREAM = 1, NE2B_KERNEL_RESIDENT = 2 };
+ne2b_status ne2b_set_kernel_mode(ne2b_sim *sim, int32_t mode);
+ne2b_status ne2b_kernel_mode(ne2b_sim *sim, int32_t *mode, int32_t *resident);
+
 /* Instrumentation (new): the CUDA stream the handle launches on (a
  * cudaStream_t, for timing with events on the launching stream) and the
  * number of kernels the handle has launched so far. */
@@ -174,6 +184,8 @@ ne2b_status ne2b_batch_set_tile_shape(ne2b_batch *b, uint32_t block, uint32_t ne
                                       uint32_t blocks_per_sm);
 ne2b_status ne2b_batch_dev_mem_bytes(ne2b_batch *b, uint64_t *bytes);
 ne2b_status ne2b_batch_last_step_ms(ne2b_batch *b, float *ms);
+ne2b_status ne2b_batch_set_kernel_mode(ne2b_batch *b, int32_t mode);
+ne2b_status ne2b_batch_kernel_mode(ne2b_batch *b, int32_t *mode, int32_t *resident);
 ne2b_status ne2b_batch_stream(ne2b_batch *b, void **stream);
 ne2b_status ne2b_batch_kernel_launches(ne2b_batch *b, uint64_t *launches);
 

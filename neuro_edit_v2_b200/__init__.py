@@ -8,13 +8,15 @@ package is the Python mirror of that ABI; importing it loads the library and
 fails loudly if it is missing.
 """
 from . import _abi
-from ._abi import MODEL_ADEX, MODEL_IZH, Config, Ne2bError, default_config
+from ._abi import (KERNEL_AUTO, KERNEL_RESIDENT, KERNEL_STREAM, MODEL_ADEX, MODEL_IZH, Config, Ne2bError,
+                   default_config)
 from .net import FlatNet, NativeNet, from_synapses, liquid, random_kout, to_adex
 from .sim import B200Sim, Batch, Server, SpikeWindowError, footprint
 
 __all__ = [
     "B200Sim", "Batch", "Server", "SpikeWindowError", "footprint", "FlatNet", "NativeNet", "from_synapses",
     "liquid", "random_kout", "to_adex", "Config", "default_config", "Ne2bError", "MODEL_IZH", "MODEL_ADEX",
+    "KERNEL_AUTO", "KERNEL_STREAM", "KERNEL_RESIDENT",
     "expf",
 ]
 

@@ -28,6 +28,10 @@ STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "EWINDOW", 5: 
 MODEL_IZH = 0
 MODEL_ADEX = 1
 
+KERNEL_AUTO = 0
+KERNEL_STREAM = 1
+KERNEL_RESIDENT = 2
+
 
 class NetDesc(C.Structure):
     _fields_ = [
@@ -138,6 +142,10 @@ _SIGS = {
     "ne2b_external": (C.c_int, [_p, _p]),
     "ne2b_set_noise": (C.c_int, [_p, _f32, _f32]),
     "ne2b_set_gauss_noise": (C.c_int, [_p, _f32]),
+    "ne2b_set_kernel_mode": (C.c_int, [_p, _i32]),
+    "ne2b_kernel_mode": (C.c_int, [_p, C.POINTER(_i32), C.POINTER(_i32)]),
+    "ne2b_batch_set_kernel_mode": (C.c_int, [_p, _i32]),
+    "ne2b_batch_kernel_mode": (C.c_int, [_p, C.POINTER(_i32), C.POINTER(_i32)]),
     "ne2b_stream": (C.c_int, [_p, C.POINTER(_p)]),
     "ne2b_kernel_launches": (C.c_int, [_p, _pu64]),
     "ne2b_batch_stream": (C.c_int, [_p, C.POINTER(_p)]),

@@ -160,7 +160,7 @@ ne2b_status ne2b_dev_mem_bytes(const ne2b_sim *sim, uint64_t *bytes) {
 
 ne2b_status ne2b_read_trace(ne2b_sim *sim, float *out) {
     CHECK_SIM(sim);
-    return sim->eng.read_f32(h->dev.trace, h->n, out);
+    return sim->eng.read_trace(*h, out);
 }
 
 ne2b_status ne2b_read_state(ne2b_sim *sim, uint32_t slot, float *out) {
@@ -305,6 +305,18 @@ ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd) {
     return sim->eng.refresh_noise(*h);
 }
 
+ne2b_status ne2b_set_kernel_mode(ne2b_sim *sim, int32_t mode) {
+    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
+    GUARD(sim->eng.set_mode(mode));
+}
+
+ne2b_status ne2b_kernel_mode(ne2b_sim *sim, int32_t *mode, int32_t *resident) {
+    if (!sim || !mode || !resident) return set_error(NE2B_EINVAL, "null argument");
+    *mode = sim->eng.mode();
+    *resident = sim->eng.resident() ? 1 : 0;
+    return NE2B_OK;
+}
+
 ne2b_status ne2b_stream(ne2b_sim *sim, void **stream) {
     if (!sim || !stream) return set_error(NE2B_EINVAL, "null argument");
     *stream = (void *)sim->eng.stream();
@@ -446,6 +458,18 @@ ne2b_status ne2b_batch_dev_mem_bytes(ne2b_batch *b, uint64_t *bytes) {
 ne2b_status ne2b_batch_last_step_ms(ne2b_batch *b, float *ms) {
     if (!b) return set_error(NE2B_EINVAL, "null batch handle");
     *ms = b->eng.last_ms();
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_batch_set_kernel_mode(ne2b_batch *b, int32_t mode) {
+    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
+    GUARD(b->eng.set_mode(mode));
+}
+
+ne2b_status ne2b_batch_kernel_mode(ne2b_batch *b, int32_t *mode, int32_t *resident) {
+    if (!b || !mode || !resident) return set_error(NE2B_EINVAL, "null argument");
+    *mode = b->eng.mode();
+    *resident = b->eng.resident() ? 1 : 0;
     return NE2B_OK;
 }
 

@@ -90,6 +90,8 @@ Engine::~Engine() {
     cudaFree(d_ptab_);
     cudaFree(d_tiles_);
     cudaFree(d_eng_);
+    cudaFree(d_block_tiles_);
+    cudaFree(d_barrier_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -130,6 +132,13 @@ ne2b_status Engine::init(int device, bool int_ring, uint32_t max_nets) {
     NE2B_CUDA(cudaMalloc(&d_tiles_, sizeof(Tile) * tiles_cap_));
     NE2B_CUDA(cudaEventCreate(&ev0_));
     NE2B_CUDA(cudaEventCreate(&ev1_));
+    NE2B_CUDA(cudaMalloc(&d_barrier_, 2 * sizeof(unsigned int)));
+    NE2B_CUDA(cudaMemset(d_barrier_, 0, 2 * sizeof(unsigned int)));
+    d_err_ = d_barrier_ + 1;
+    if (const char *m = getenv("NE2B_KERNEL")) {
+        if (!strcmp(m, "stream")) mode_ = kModeStream;
+        else if (!strcmp(m, "resident")) mode_ = kModeResident;
+    }
     nets_.assign(nets_cap_, nullptr);
     return upload_eng();
 }
@@ -142,6 +151,11 @@ ne2b_status Engine::upload_eng() {
     e.nets = d_nets_;
     e.ptab = d_ptab_;
     e.counters = d_counters_;
+    e.block_tiles = d_block_tiles_;
+    e.block_neurons = res_neurons_;
+    e.pad0 = 0;
+    e.barrier = d_barrier_;
+    e.err = d_err_;
     NE2B_CUDA(cudaMemcpyAsync(d_eng_, &e, sizeof e, cudaMemcpyHostToDevice, stream_));
     // the source lives on this stack frame: wait for the copy
     NE2B_CUDA(cudaStreamSynchronize(stream_));
@@ -293,7 +307,7 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     NET_TRY(alloc(&p, sizeof(float) * np)); d.v = (float *)p;
     NET_TRY(alloc(&p, sizeof(float) * np)); d.u = (float *)p;
     NET_TRY(alloc(&p, sizeof(float) * np)); d.s = (float *)p;
-    NET_TRY(alloc(&p, sizeof(float) * np)); d.trace = (float *)p;
+    NET_TRY(alloc(&p, sizeof(uint16_t) * np)); d.tk = (uint16_t *)p;
     NET_TRY(alloc(&p, sizeof(float) * np)); d.ext = (float *)p;
     NET_TRY(alloc(&p, sizeof(float) * np)); d.v0 = (const float *)p;
     NET_TRY(alloc(&p, sizeof(float) * np)); d.u0 = (const float *)p;
@@ -395,6 +409,25 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     d.dt = cfg->dt_ms;
     d.decay_s = host_decay(cfg->dt_ms, cfg->synapse_tau_ms);
     d.decay_t = host_decay(cfg->dt_ms, cfg->readout_tau_ms);
+    {
+        // trace after k non-spiking steps = 1.0 * decay_t * ... * decay_t (k
+        // f32 multiplies in order, cpu.rs:252-256); the table stops at 0 or
+        // at the subnormal fixed point, where the trace stays forever
+        std::vector<float> tab(1, 1.0f);
+        while (true) {
+            const float nx = tab.back() * d.decay_t;
+            if (nx == tab.back()) break;
+            tab.push_back(nx);
+            if (nx == 0.0f) break;
+            if (tab.size() > 65534) return fail(set_error(NE2B_UNSUPPORTED,
+                "readout_tau_ms %g at dt %g needs more than 65534 trace steps", (double)cfg->readout_tau_ms,
+                (double)cfg->dt_ms));
+        }
+        NET_TRY(alloc(&p, sizeof(float) * tab.size())); d.trace_tab = (const float *)p;
+        NET_TRY(up((void *)d.trace_tab, tab.data(), sizeof(float) * tab.size()));
+        NET_TRY(cuda_error(cudaStreamSynchronize(stream_), "trace table upload"));
+        d.trace_last = (uint32_t)tab.size() - 1;
+    }
     fill_noise(d, *cfg);
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
               (cfg->window_steps ? kNetWindows : 0u);
@@ -449,6 +482,56 @@ uint32_t Engine::grid() const {
     return g < nt ? g : nt;
 }
 
+// Resident plan: G co-resident blocks, each owning a contiguous range of
+// tiles balanced by neuron count, with the owned state (v, u, s: 12 B;
+// tk, pidx: 4 B per neuron) in dynamic shared memory.  Chooses the most
+// blocks per SM whose shared memory still fits; false when nothing fits.
+bool Engine::plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &block_tiles) {
+    if (tiles.empty() || mode_ == kModeStream) return false;
+    uint64_t total = 0;
+    for (const Tile &t : tiles) total += t.count;
+    const uint32_t head = resident_head(shape_.block, shape_.npt);
+    const uint32_t max_bps = std::max<uint32_t>(1, 2048 / shape_.block);
+    for (uint32_t bps = shape_.blocks_per_sm ? shape_.blocks_per_sm : max_bps; bps >= 1; --bps) {
+        const uint32_t G = (uint32_t)std::min<uint64_t>((uint64_t)sm_count_ * bps, tiles.size());
+        const uint64_t target = (total + G - 1) / G;
+        std::vector<uint32_t> bt(1, 0);
+        uint64_t acc = 0, m = 0;
+        for (uint32_t k = 0; k < tiles.size(); ++k) {
+            const uint32_t remaining_tiles = (uint32_t)tiles.size() - k;
+            const uint32_t remaining_blocks = G - (uint32_t)(bt.size() - 1);
+            if (acc > 0 && remaining_blocks > 1 &&
+                (acc + tiles[k].count > target || remaining_tiles < remaining_blocks)) {
+                bt.push_back(k);
+                m = std::max(m, acc);
+                acc = 0;
+            }
+            acc += tiles[k].count;
+        }
+        bt.push_back((uint32_t)tiles.size());
+        m = std::max(m, acc);
+        const size_t smem = head + 16 * (size_t)((m + 3) / 4 * 4);
+        if (smem > 227 * 1024) continue;
+        const int occ = resident_occupancy(int_ring_, shape_.block, shape_.npt, smem);
+        const uint32_t blocks = (uint32_t)bt.size() - 1;
+        if (occ < 1 || (uint64_t)occ * sm_count_ < blocks) continue;
+        // smem offsets within each block
+        for (uint32_t b = 0; b + 1 < bt.size(); ++b) {
+            uint32_t off = 0;
+            for (uint32_t k = bt[b]; k < bt[b + 1]; ++k) {
+                tiles[k].smem_off = off;
+                off += tiles[k].count;
+            }
+        }
+        block_tiles = bt;
+        res_neurons_ = (uint32_t)((m + 3) / 4 * 4);
+        res_smem_ = smem;
+        res_grid_ = blocks;
+        return true;
+    }
+    return false;
+}
+
 ne2b_status Engine::rebuild_tiles() {
     const uint32_t tile = shape_.block * shape_.npt;
     std::vector<Tile> tiles;
@@ -456,6 +539,7 @@ ne2b_status Engine::rebuild_tiles() {
         if (!h) continue;
         for (uint32_t start = 0; start < h->n_pad; start += tile) {
             Tile t;
+            memset(&t, 0, sizeof t);
             t.net = h->slot;
             t.start = start;
             t.count = std::min(tile, h->n_pad - start);
@@ -468,21 +552,50 @@ ne2b_status Engine::rebuild_tiles() {
         }
     }
     const uint32_t old_grid = grid();
+    std::vector<uint32_t> block_tiles;
+    resident_ = plan_resident(tiles, block_tiles);
+    if (mode_ == kModeResident && !resident_ && !tiles.empty())
+        return set_error(NE2B_UNSUPPORTED, "the nets do not fit the resident kernel's shared memory");
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
     if (tiles.size() > tiles_cap_) {
         uint32_t cap = tiles_cap_;
         while (cap < tiles.size()) cap *= 2;
-        NE2B_CUDA(cudaStreamSynchronize(stream_));
         NE2B_CUDA(cudaFree(d_tiles_));
         d_tiles_ = nullptr;
         NE2B_CUDA(cudaMalloc(&d_tiles_, sizeof(Tile) * cap));
         tiles_cap_ = cap;
     }
+    if (block_tiles.size() > block_tiles_cap_) {
+        uint32_t cap = std::max<uint32_t>(block_tiles_cap_, 64);
+        while (cap < block_tiles.size()) cap *= 2;
+        NE2B_CUDA(cudaFree(d_block_tiles_));
+        d_block_tiles_ = nullptr;
+        NE2B_CUDA(cudaMalloc(&d_block_tiles_, sizeof(uint32_t) * cap));
+        block_tiles_cap_ = cap;
+    }
     if (!tiles.empty())
-        NE2B_CUDA(cudaMemcpyAsync(d_tiles_, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, stream_));
+        NE2B_CUDA(cudaMemcpy(d_tiles_, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
+    if (!block_tiles.empty())
+        NE2B_CUDA(cudaMemcpy(d_block_tiles_, block_tiles.data(), sizeof(uint32_t) * block_tiles.size(),
+                             cudaMemcpyHostToDevice));
     n_tiles_ = (uint32_t)tiles.size();
     NE2B_TRY(upload_eng());
     if (grid() != old_grid) clear_graphs();
     return NE2B_OK;
+}
+
+ne2b_status Engine::set_mode(int m) {
+    if (m < kModeAuto || m > kModeResident) return set_error(NE2B_EINVAL, "kernel mode %d", m);
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    const int old = mode_;
+    mode_ = m;
+    clear_graphs();
+    ne2b_status st = rebuild_tiles();
+    if (st != NE2B_OK) {
+        mode_ = old;
+        rebuild_tiles();
+    }
+    return st;
 }
 
 ne2b_status Engine::set_shape(const TileShape &s) {
@@ -514,6 +627,18 @@ ne2b_status Engine::reset_net(uint32_t slot) {
 
 ne2b_status Engine::sync() {
     NE2B_CUDA(cudaStreamSynchronize(stream_));
+    return check_err();
+}
+
+// A grid barrier of the resident kernel that timed out leaves a flag; the
+// state of that launch is not trustworthy, so the next sync reports it.
+ne2b_status Engine::check_err() {
+    unsigned int e = 0;
+    NE2B_CUDA(cudaMemcpy(&e, d_err_, sizeof e, cudaMemcpyDeviceToHost));
+    if (e) {
+        NE2B_CUDA(cudaMemset(d_err_, 0, sizeof e));
+        return set_error(NE2B_ECUDA, "resident kernel: a grid barrier wait exceeded its limit; state is invalid");
+    }
     return NE2B_OK;
 }
 
@@ -596,6 +721,13 @@ ne2b_status Engine::set_input_matrix(NetHost &h, const float *x, uint64_t steps)
 
 ne2b_status Engine::launch_group(uint32_t steps) {
     if (n_tiles_ == 0 || steps == 0) return NE2B_OK;
+    if (resident_) {
+        NE2B_CUDA(cudaMemsetAsync(d_barrier_, 0, sizeof(unsigned int), stream_));
+        NE2B_CUDA(launch_resident(int_ring_, shape_.block, shape_.npt, d_eng_, 0, steps, res_grid_, res_smem_, stream_));
+        NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
+        launches_ += 2;
+        return NE2B_OK;
+    }
     const uint32_t g = grid();
     if (steps == graph_steps) {
         auto it = graphs_.find(steps);
@@ -639,8 +771,9 @@ ne2b_status Engine::run_steps(uint64_t steps) {
         }
         if (!repack.empty()) NE2B_TRY(pack_stim(repack));
         uint64_t left = chunk;
+        const uint64_t group = resident_ ? std::max<uint64_t>(graph_steps, resident_steps) : graph_steps;
         while (left > 0) {
-            const uint32_t g = (uint32_t)std::min<uint64_t>(left, graph_steps);
+            const uint32_t g = (uint32_t)std::min<uint64_t>(left, group);
             NE2B_TRY(launch_group(g));
             left -= g;
         }
@@ -659,7 +792,20 @@ ne2b_status Engine::read_f32(const float *dev, uint32_t n, float *out) {
     if (n == 0) return NE2B_OK;
     NE2B_CUDA(cudaMemcpyAsync(out, dev, sizeof(float) * n, cudaMemcpyDeviceToHost, stream_));
     NE2B_CUDA(cudaStreamSynchronize(stream_));
-    return NE2B_OK;
+    return check_err();
+}
+
+ne2b_status Engine::read_trace(NetHost &h, float *out) {
+    if (h.n == 0) return NE2B_OK;
+    float *tmp = nullptr;
+    NE2B_CUDA(cudaMallocAsync((void **)&tmp, sizeof(float) * h.n, stream_));
+    cudaError_t e = launch_trace(h.dev.tk, h.dev.trace_tab, h.n, tmp, stream_);
+    launches_ += 1;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(float) * h.n, cudaMemcpyDeviceToHost, stream_);
+    cudaFreeAsync(tmp, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    NE2B_TRY(cuda_error(e, "trace readback"));
+    return check_err();
 }
 
 ne2b_status Engine::spike_counts(NetHost &h, uint64_t rows, uint32_t *out) {
@@ -752,7 +898,7 @@ ne2b_status Engine::snapshot(std::vector<std::vector<uint8_t>> &snap) {
         NE2B_TRY(grab(d.v, 4 * np));
         NE2B_TRY(grab(d.u, 4 * np));
         NE2B_TRY(grab(d.s, 4 * np));
-        NE2B_TRY(grab(d.trace, 4 * np));
+        NE2B_TRY(grab(d.tk, 2 * np));
         NE2B_TRY(grab(d.pn_total, 8 * np));
         NE2B_TRY(grab(d.ring, 4 * (size_t)h->D * np));
         NE2B_TRY(grab(d.rec_bits, d.rec_bits ? 4 * (size_t)d.rec_rows * (np / 32) : 0));
@@ -778,7 +924,7 @@ ne2b_status Engine::restore(const std::vector<std::vector<uint8_t>> &snap) {
         NE2B_TRY(put(d.v));
         NE2B_TRY(put(d.u));
         NE2B_TRY(put(d.s));
-        NE2B_TRY(put(d.trace));
+        NE2B_TRY(put(d.tk));
         NE2B_TRY(put(d.pn_total));
         NE2B_TRY(put(d.ring));
         NE2B_TRY(put(d.rec_bits));

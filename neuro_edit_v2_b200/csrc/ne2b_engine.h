@@ -49,6 +49,8 @@ struct NetHost {
     std::vector<float> pack_buf;
 };
 
+enum KernelMode { kModeAuto = 0, kModeStream = 1, kModeResident = 2 };
+
 struct TileShape {
     uint32_t block = 256;
     uint32_t npt = 2;
@@ -75,6 +77,8 @@ class Engine {
     ne2b_status upload_net(NetHost &h);
 
     ne2b_status read_f32(const float *dev, uint32_t n, float *out);
+    ne2b_status read_trace(NetHost &h, float *out);
+    ne2b_status check_err();
     ne2b_status spike_counts(NetHost &h, uint64_t rows, uint32_t *out);
     ne2b_status spike_row(NetHost &h, uint32_t back, uint64_t *out);
     ne2b_status spikes_total(NetHost &h, uint64_t *out);
@@ -93,7 +97,11 @@ class Engine {
     cudaStream_t stream() const { return stream_; }
     bool int_ring() const { return int_ring_; }
     uint64_t launches() const { return launches_; }
+    bool resident() const { return resident_; }
+    int mode() const { return mode_; }
+    ne2b_status set_mode(int m);
     uint32_t graph_steps = 64;
+    uint32_t resident_steps = 4096;  // max steps per resident launch
     uint64_t stim_chunk = 2048;
 
   private:
@@ -104,6 +112,7 @@ class Engine {
     ne2b_status upload_ptab();
     ne2b_status upload_eng();
     uint32_t grid() const;
+    bool plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &block_tiles);
     void clear_graphs();
 
     int device_ = 0;
@@ -128,6 +137,16 @@ class Engine {
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     float last_ms_ = 0.0f;
     uint64_t launches_ = 0;  // kernels launched (graph nodes counted per replay)
+    // resident kernel
+    int mode_ = kModeAuto;
+    bool resident_ = false;
+    uint32_t *d_block_tiles_ = nullptr;
+    uint32_t block_tiles_cap_ = 0;
+    uint32_t res_neurons_ = 0;
+    size_t res_smem_ = 0;
+    uint32_t res_grid_ = 0;
+    unsigned int *d_barrier_ = nullptr;
+    unsigned int *d_err_ = nullptr;
     void *stage_ = nullptr;  // pinned staging for stimulus chunks and descriptors
     size_t stage_bytes_ = 0;
 };

@@ -1,26 +1,32 @@
-// ne2b_kernels.cu — the per-step kernel and its helpers.
+// ne2b_kernels.cu — the step kernels and their helpers.
 //
-// One launch = one dt step of every active network in the engine.  The grid
-// is persistent (a multiple of the SM count) and strides over tiles; a tile
-// is `count` consecutive neurons of one network.  Per tile the block:
+// A tile is `count` consecutive neurons of one network.  Processing one tile
+// for one dt step (process_tile):
 //
-//   1. streams the neurons' state (SoA, coalesced) and the ring slot of this
-//      step, zeroing the slot words that held arrivals
-//        (sim/src/cpu.rs:218-222, kernels.rs:104-107);
-//   2. assembles the input current s + ext (+ stimulus) (+ noise) in the
-//      reference order and runs the model step (cpu.rs:223-250);
-//   3. updates trace and s with the host-computed decays (cpu.rs:252-260);
-//   4. compacts the tile's spikes with warp ballots and a block prefix sum
-//      into shared memory, writing the spike-record words straight from the
-//      ballots (replaces the global atomicAdd slot of kernels.rs:150-156);
-//   5. delivers its own spikes: one warp per spiking neuron, lanes striding
-//      the neuron's source-major CSR row, a no-return atomic add into
+//   1. read the tile's state and its ring slot for this step, zeroing the slot
+//      words that held arrivals (sim/src/cpu.rs:218-222, kernels.rs:104-107);
+//   2. assemble the input current s + ext (+ stimulus) (+ noise) in the
+//      reference order and run the model step (cpu.rs:223-250);
+//   3. update s and the trace with the host-computed decays (cpu.rs:252-260);
+//      the trace is kept as "steps since the last spike" into a table of the
+//      exact f32 products 1.0 * decay_t * decay_t ..., which reproduces the
+//      reference's repeated multiply bit-for-bit at 2 bytes per neuron;
+//   4. compact the tile's spikes with warp ballots and a block prefix sum into
+//      shared memory, writing the spike-record words straight from the ballots
+//      (replaces the global atomicAdd slot of kernels.rs:150-156);
+//   5. deliver its own spikes: one warp per spiking neuron, lanes striding its
+//      source-major CSR row, a no-return atomic add into
 //      ring[(t + delay) % D][tgt] (cpu.rs:264-278, kernels.rs:174-204).
 //
-// No cross-block ordering is needed inside a step: step t reads ring slot
-// t % D and every delivery of step t lands in slot (t + d) % D with
-// 1 <= d < D, a different slot.  The kernel boundary orders step t's
-// deliveries before step t+1's reads.
+// Within a step no cross-block ordering is needed: step t reads slot t % D and
+// every delivery of step t lands in slot (t + d) % D, 1 <= d < D.  Between
+// steps, step t's deliveries must land before step t+1 reads:
+//   * step_kernel (streaming): one launch per step, the kernel boundary orders
+//     the steps; state is streamed from HBM every step.
+//   * resident_kernel (persistent, cooperative): each block owns a fixed set
+//     of tiles whose state stays in shared memory for the whole launch; steps
+//     are separated by a grid barrier whose wait is bounded by %globaltimer
+//     (2 s, then the launch stops and reports an error flag).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -29,197 +35,317 @@
 
 namespace ne2b {
 
-template <bool INT, int BLOCK, int NPT>
-__global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
-    constexpr int NW = BLOCK / 32;
-    constexpr int TILE = BLOCK * NPT;
-    __shared__ uint32_t s_list[TILE];
-    __shared__ uint32_t s_woff[NW];
-    __shared__ uint32_t s_total;
+struct SmemLists {
+    uint32_t *list;   // [tile size] spiking local ids
+    uint32_t *woff;   // [warps] prefix offsets
+    uint32_t *total;  // [1]
+};
 
+template <bool INT, int BLOCK, int NPT, bool RES>
+__device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const Tile &tile, uint32_t k_step,
+                                             float *vs, float *us, float *ss, uint16_t *tks, const uint16_t *pis,
+                                             const SmemLists &sl) {
+    constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const uint32_t n_tiles = eng->n_tiles;
-    const Tile *__restrict__ tiles = eng->tiles;
-    NetDev *__restrict__ nets = eng->nets;
+    const NetDev &nd = eng->nets[tile.net];
+    const uint32_t flags = nd.flags;
+    if (!(flags & kNetActive)) return;  // uniform across the block
+    const uint64_t t = nd.t + k_step;
+    if (t >= nd.t_end) return;  // uniform across the block
+
+    const uint32_t n = nd.n, n_pad = nd.n_pad, D = nd.D;
+    const uint32_t tmod = (nd.tmod + k_step) % D;
+    const size_t slot_off = (size_t)tmod * n_pad;
+    const float dt = nd.dt, decay_s = nd.decay_s;
+    const float pkick = nd.pkick, kick = nd.kick, gauss_k = nd.gauss_k;
+    const uint64_t seed = nd.seed;
+    const uint32_t tlast = nd.trace_last;
+    uint32_t *__restrict__ ringw = (uint32_t *)nd.ring;
+    const bool has_ext = flags & kNetHasExt;
+    const bool has_stim = tile.flags & kTileHasStim;
+    const bool windows = flags & kNetWindows;
+    bool win_end = false;
+    uint32_t widx = 0;
+    if (windows) {
+        win_end = ((t + 1) % nd.win_steps) == 0;
+        widx = (uint32_t)((t + 1) / nd.win_steps) - 1u;
+    }
     const ParamRow *__restrict__ ptab = eng->ptab;
 
-    for (uint32_t tix = blockIdx.x; tix < n_tiles; tix += gridDim.x) {
-        const Tile tile = tiles[tix];
-        const NetDev &nd = nets[tile.net];
-        const uint32_t flags = nd.flags;
-        if (!(flags & kNetActive)) continue;
-        const uint64_t t = nd.t + k_step;
-        if (t >= nd.t_end) continue;
+    uint32_t li[NPT];
+    bool valid[NPT];
+    float v[NPT], u[NPT], s[NPT], ex[NPT];
+    uint32_t rw[NPT], tk[NPT], pi[NPT];
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) {
+        const uint32_t off = q * BLOCK + threadIdx.x;
+        li[q] = tile.start + off;
+        valid[q] = off < tile.count && li[q] < n;
+        if (valid[q]) {
+            rw[q] = RES ? __ldcg(ringw + slot_off + li[q]) : ringw[slot_off + li[q]];
+            v[q] = vs[off];
+            u[q] = us[off];
+            s[q] = ss[off];
+            tk[q] = tks[off];
+            pi[q] = pis[off];
+            ex[q] = has_ext ? nd.ext[li[q]] : 0.0f;
+        }
+    }
 
-        const uint32_t n = nd.n, n_pad = nd.n_pad, D = nd.D;
-        const uint32_t tmod = (nd.tmod + k_step) % D;
-        const size_t slot_off = (size_t)tmod * n_pad;
-        const float dt = nd.dt, decay_s = nd.decay_s, decay_t = nd.decay_t;
-        const float pkick = nd.pkick, kick = nd.kick, gauss_k = nd.gauss_k;
-        const uint64_t seed = nd.seed;
-        uint32_t *__restrict__ ringw = (uint32_t *)nd.ring;
-        float *__restrict__ va = nd.v;
-        float *__restrict__ ua = nd.u;
-        float *__restrict__ sa = nd.s;
-        float *__restrict__ ta = nd.trace;
-        const bool has_ext = flags & kNetHasExt;
-        const bool has_stim = tile.flags & kTileHasStim;
-        const bool windows = flags & kNetWindows;
-        bool win_end = false;
-        uint32_t widx = 0;
+    bool spk[NPT];
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) {
+        spk[q] = false;
+        if (!valid[q]) continue;
+        const uint32_t i = li[q];
+        const uint32_t off = q * BLOCK + threadIdx.x;
+        const float arr = INT ? __fmul_rn(__int2float_rn((int)rw[q]), 0x1p-12f)  // rt_get, kernels.rs:60
+                              : __uint_as_float(rw[q]);
+        if (rw[q] != 0u) ringw[slot_off + i] = 0u;
+        const float sv = __fadd_rn(s[q], arr);
+        float I = __fadd_rn(sv, ex[q]);
+        if (has_stim) {
+            // the host provides the [steps x inputs] values covering every
+            // launched step; the range check only guards the read
+            const long long rel = (long long)t - nd.stim_t0;
+            const float *row = (rel >= 0 && rel < (long long)nd.stim_len) ? nd.stim_buf + (size_t)rel * nd.n_inputs
+                                                                          : nullptr;
+            const uint32_t lo = nd.stim_ptr[i], hi = nd.stim_ptr[i + 1];
+            if (row)
+                for (uint32_t j = lo; j < hi; ++j) I = __fadd_rn(I, __fmul_rn(nd.stim_w[j], row[nd.stim_in[j]]));
+        }
+        const ParamRow &pr = ptab[pi[q]];
+        float p[10];
+        const float4 p0 = *reinterpret_cast<const float4 *>(&pr.p[0]);
+        const float4 p1 = *reinterpret_cast<const float4 *>(&pr.p[4]);
+        const float4 p2 = *reinterpret_cast<const float4 *>(&pr.p[8]);
+        p[0] = p0.x; p[1] = p0.y; p[2] = p0.z; p[3] = p0.w;
+        p[4] = p1.x; p[5] = p1.y; p[6] = p1.z; p[7] = p1.w;
+        p[8] = p2.x; p[9] = p2.y;
+        const uint32_t model = pr.model;
+        const float gain = model == 1u ? p[0] : 1.0f;  // model/mod.rs:104-106, adex.rs:189-191
+        if (pkick > 0.0f || gauss_k != 0.0f) {
+            const uint64_t base = noise_base(i, t, seed);
+            if (pkick > 0.0f && noise_fires(base, pkick)) I = __fadd_rn(I, __fmul_rn(kick, gain));
+            if (gauss_k != 0.0f)
+                I = __fadd_rn(I, __fmul_rn(__int2float_rn(gauss_numer(base)), __fmul_rn(gauss_k, gain)));
+        }
+        const bool sp = model == 1u ? adex_step(p, v[q], u[q], I, dt) : izh_step(p, v[q], u[q], I, dt);
+        // trace: 1 on spike, else one more multiply by decay_t (saturating at
+        // the table's last entry, 0 or the subnormal fixed point)
+        uint32_t k = tk[q];
+        k = sp ? 0u : (k == kTraceZero ? k : (k < tlast ? k + 1u : tlast));
+        vs[off] = v[q];
+        us[off] = u[q];
+        ss[off] = __fmul_rn(sv, decay_s);
+        tks[off] = (uint16_t)k;
+        if (sp) nd.pn_total[i] += 1ull;
         if (windows) {
-            win_end = ((t + 1) % nd.win_steps) == 0;
-            widx = (uint32_t)((t + 1) / nd.win_steps) - 1u;
+            if (win_end) {
+                const uint32_t c = nd.wcount[i] + (sp ? 1u : 0u);
+                if (widx < nd.max_windows) nd.win_out[(size_t)widx * n_pad + i] = (uint16_t)(c > 65535u ? 65535u : c);
+                nd.wcount[i] = 0u;
+            } else if (sp) {
+                nd.wcount[i] += 1u;
+            }
         }
+        spk[q] = sp;
+    }
 
-        uint32_t li[NPT];
-        bool valid[NPT];
-        float v[NPT], u[NPT], s[NPT], tr[NPT], ex[NPT];
-        uint32_t rw[NPT];
-        uint32_t pi[NPT];
+    // ---- compaction: warp ballots -> record words + block prefix sum
+    uint32_t mask[NPT];
+    uint32_t wcnt = 0;
 #pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-            const uint32_t off = q * BLOCK + threadIdx.x;
-            li[q] = tile.start + off;
-            valid[q] = off < tile.count && li[q] < n;
-            if (valid[q]) {
-                rw[q] = ringw[slot_off + li[q]];
-                v[q] = va[li[q]];
-                u[q] = ua[li[q]];
-                s[q] = sa[li[q]];
-                tr[q] = ta[li[q]];
-                pi[q] = nd.pidx[li[q]];
-                ex[q] = has_ext ? nd.ext[li[q]] : 0.0f;
-            }
-        }
-
-        bool spk[NPT];
-#pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-            spk[q] = false;
-            if (!valid[q]) continue;
-            const uint32_t i = li[q];
-            float arr;
-            if (INT) {
-                arr = __fmul_rn(__int2float_rn((int)rw[q]), 0x1p-12f);  // rt_get, kernels.rs:60
-            } else {
-                arr = __uint_as_float(rw[q]);
-            }
-            if (rw[q] != 0u) ringw[slot_off + i] = 0u;
-            const float sv = __fadd_rn(s[q], arr);
-            float I = __fadd_rn(sv, ex[q]);
-            if (has_stim) {
-                // the host uploads the [steps x inputs] values covering every
-                // launched step; the range check only guards the read
-                const long long rel = (long long)t - nd.stim_t0;
-                const float *row = (rel >= 0 && rel < (long long)nd.stim_len) ? nd.stim_buf + (size_t)rel * nd.n_inputs : nullptr;
-                const uint32_t lo = nd.stim_ptr[i], hi = nd.stim_ptr[i + 1];
-                if (row)
-                    for (uint32_t j = lo; j < hi; ++j) I = __fadd_rn(I, __fmul_rn(nd.stim_w[j], row[nd.stim_in[j]]));
-            }
-            const ParamRow &pr = ptab[pi[q]];
-            float p[10];
-            const float4 p0 = *reinterpret_cast<const float4 *>(&pr.p[0]);
-            const float4 p1 = *reinterpret_cast<const float4 *>(&pr.p[4]);
-            const float4 p2 = *reinterpret_cast<const float4 *>(&pr.p[8]);
-            p[0] = p0.x; p[1] = p0.y; p[2] = p0.z; p[3] = p0.w;
-            p[4] = p1.x; p[5] = p1.y; p[6] = p1.z; p[7] = p1.w;
-            p[8] = p2.x; p[9] = p2.y;
-            const uint32_t model = pr.model;
-            const float gain = model == 1u ? p[0] : 1.0f;  // model/mod.rs:104-106, adex.rs:189-191
-            if (pkick > 0.0f || gauss_k != 0.0f) {
-                const uint64_t base = noise_base(i, t, seed);
-                if (pkick > 0.0f && noise_fires(base, pkick)) I = __fadd_rn(I, __fmul_rn(kick, gain));
-                if (gauss_k != 0.0f)
-                    I = __fadd_rn(I, __fmul_rn(__int2float_rn(gauss_numer(base)), __fmul_rn(gauss_k, gain)));
-            }
-            bool sp = model == 1u ? adex_step(p, v[q], u[q], I, dt) : izh_step(p, v[q], u[q], I, dt);
-            tr[q] = sp ? 1.0f : __fmul_rn(tr[q], decay_t);
-            va[i] = v[q];
-            ua[i] = u[q];
-            sa[i] = __fmul_rn(sv, decay_s);
-            ta[i] = tr[q];
-            if (sp) nd.pn_total[i] += 1ull;
-            if (windows) {
-                if (win_end) {
-                    const uint32_t c = nd.wcount[i] + (sp ? 1u : 0u);
-                    if (widx < nd.max_windows) nd.win_out[(size_t)widx * n_pad + i] = (uint16_t)(c > 65535u ? 65535u : c);
-                    nd.wcount[i] = 0u;
-                } else if (sp) {
-                    nd.wcount[i] += 1u;
-                }
-            }
-            spk[q] = sp;
-        }
-
-        // ---- compaction: warp ballots -> record words + block prefix sum
-        uint32_t mask[NPT];
-        uint32_t wcnt = 0;
-#pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-            mask[q] = __ballot_sync(0xffffffffu, spk[q]);
-            wcnt += __popc(mask[q]);
-        }
-        if (flags & kNetRecord) {
-            const uint32_t row = (uint32_t)(t % nd.rec_rows);
-            const uint32_t words32 = n_pad >> 5;
-            if (lane == 0) {
-#pragma unroll
-                for (int q = 0; q < NPT; ++q) {
-                    const uint32_t off = q * BLOCK + warp * 32;
-                    if (off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask[q];
-                }
-            }
-        }
-        if (lane == 0) s_woff[warp] = wcnt;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t c = lane < NW ? s_woff[lane] : 0u;
-            uint32_t incl = c;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            if (lane < NW) s_woff[lane] = incl - c;
-            if (lane == 31) s_total = incl;
-        }
-        __syncthreads();
-        {
-            uint32_t pos = s_woff[warp];
-            const uint32_t lt = (1u << lane) - 1u;
+    for (int q = 0; q < NPT; ++q) {
+        mask[q] = __ballot_sync(0xffffffffu, spk[q]);
+        wcnt += __popc(mask[q]);
+    }
+    if (flags & kNetRecord) {
+        const uint32_t row = (uint32_t)(t % nd.rec_rows);
+        const uint32_t words32 = n_pad >> 5;
+        if (lane == 0) {
 #pragma unroll
             for (int q = 0; q < NPT; ++q) {
-                if (spk[q]) s_list[pos + __popc(mask[q] & lt)] = li[q];
-                pos += __popc(mask[q]);
+                const uint32_t off = q * BLOCK + warp * 32;
+                if (off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask[q];
             }
         }
-        __syncthreads();
-        const uint32_t total = s_total;
-        if (total) {
-            if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
-            const uint32_t *__restrict__ rowptr = nd.rowptr;
-            const uint32_t *__restrict__ tgt = nd.tgt;
-            const bool d16 = flags & kNetDelay16;
-            for (uint32_t si = warp; si < total; si += NW) {
-                const uint32_t i = s_list[si];
-                const uint32_t lo = rowptr[i], hi = rowptr[i + 1];
-                for (uint32_t j = lo + lane; j < hi; j += 32) {
-                    const uint32_t tg = tgt[j];
-                    const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
-                    uint32_t sl = tmod + d;
-                    if (sl >= D) sl -= D;
-                    const size_t idx = (size_t)sl * n_pad + tg;
-                    if (INT) {
-                        atomicAdd((int *)ringw + idx, ((const int *)nd.w)[j]);
-                    } else {
-                        atomicAdd((float *)ringw + idx, ((const float *)nd.w)[j]);
-                    }
+    }
+    if (lane == 0) sl.woff[warp] = wcnt;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t c = lane < NW ? sl.woff[lane] : 0u;
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < NW) sl.woff[lane] = incl - c;
+        if (lane == 31) *sl.total = incl;
+    }
+    __syncthreads();
+    {
+        uint32_t pos = sl.woff[warp];
+        const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+            if (spk[q]) sl.list[pos + __popc(mask[q] & lt)] = li[q];
+            pos += __popc(mask[q]);
+        }
+    }
+    __syncthreads();
+    const uint32_t total = *sl.total;
+    if (total) {
+        if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
+        const uint32_t *__restrict__ rowptr = nd.rowptr;
+        const uint32_t *__restrict__ tgt = nd.tgt;
+        const bool d16 = flags & kNetDelay16;
+        for (uint32_t si = warp; si < total; si += NW) {
+            const uint32_t i = sl.list[si];
+            const uint32_t lo = rowptr[i], hi = rowptr[i + 1];
+            for (uint32_t j = lo + lane; j < hi; j += 32) {
+                const uint32_t tg = tgt[j];
+                const uint32_t d =
+                    d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
+                uint32_t slot = tmod + d;
+                if (slot >= D) slot -= D;
+                const size_t idx = (size_t)slot * n_pad + tg;
+                if (INT) {
+                    atomicAdd((int *)ringw + idx, ((const int *)nd.w)[j]);
+                } else {
+                    atomicAdd((float *)ringw + idx, ((const float *)nd.w)[j]);
                 }
             }
         }
-        __syncthreads();
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------ streaming kernel
+template <bool INT, int BLOCK, int NPT>
+__global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
+    __shared__ uint32_t s_list[BLOCK * NPT];
+    __shared__ uint32_t s_woff[BLOCK / 32];
+    __shared__ uint32_t s_total;
+    const SmemLists sl{s_list, s_woff, &s_total};
+    const uint32_t n_tiles = eng->n_tiles;
+    for (uint32_t tix = blockIdx.x; tix < n_tiles; tix += gridDim.x) {
+        const Tile tile = eng->tiles[tix];
+        const NetDev &nd = eng->nets[tile.net];
+        process_tile<INT, BLOCK, NPT, false>(eng, tile, k_step, nd.v + tile.start, nd.u + tile.start,
+                                             nd.s + tile.start, nd.tk + tile.start, nd.pidx + tile.start, sl);
+    }
+}
+
+// ------------------------------------------------------- resident kernel
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s
+
+// Grid barrier for a cooperative launch.  Arrival: block-wide barrier, a
+// gpu-scope fence by thread 0 (publishes the block's ring deliveries), one
+// atomic increment of the counter.  Wait: thread 0 polls the counter with
+// acquire loads until every block of the grid has arrived; it gives up
+// after kBarrierLimitNs or as soon as another block has flagged an error.
+// Returns false (for every thread of the block) when the launch must stop.
+__device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int target, unsigned int *err,
+                                             unsigned int *s_flag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(counter, 1u);
+        unsigned int ok = 1u;
+        if (ld_acquire_gpu(counter) < target) {
+            const unsigned long long t0 = globaltimer_ns();
+            while (ld_acquire_gpu(counter) < target) {
+                if (ld_acquire_gpu(err) != 0u) {
+                    ok = 0u;
+                    break;
+                }
+                if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+                    atomicExch(err, 1u);
+                    ok = 0u;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        *s_flag = ok;
+    }
+    __syncthreads();
+    return *s_flag != 0u;
+}
+
+// Shared memory: [spike list TILE u32][woff NW u32][total, flag u32]
+//                [v M f32][u M f32][s M f32][tk M u16][pidx M u16]
+template <int BLOCK, int NPT>
+__host__ __device__ constexpr uint32_t resident_head_bytes() {
+    return (uint32_t)((BLOCK * NPT + BLOCK / 32 + 2) * 4 + 15) / 16 * 16;
+}
+
+template <bool INT, int BLOCK, int NPT>
+__global__ void __launch_bounds__(BLOCK) resident_kernel(const EngineDev *__restrict__ eng, uint32_t k0,
+                                                         uint32_t nsteps) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int TILE = BLOCK * NPT;
+    uint32_t *head = reinterpret_cast<uint32_t *>(smem);
+    const SmemLists sl{head, head + TILE, head + TILE + BLOCK / 32};
+    unsigned int *s_flag = head + TILE + BLOCK / 32 + 1;
+    const uint32_t M = eng->block_neurons;
+    float *sv = reinterpret_cast<float *>(smem + resident_head_bytes<BLOCK, NPT>());
+    float *su = sv + M;
+    float *ss = su + M;
+    uint16_t *stk = reinterpret_cast<uint16_t *>(ss + M);
+    uint16_t *spi = stk + M;
+    const uint32_t t_lo = eng->block_tiles[blockIdx.x], t_hi = eng->block_tiles[blockIdx.x + 1];
+
+    for (uint32_t tix = t_lo; tix < t_hi; ++tix) {
+        const Tile tile = eng->tiles[tix];
+        const NetDev &nd = eng->nets[tile.net];
+        for (uint32_t j = threadIdx.x; j < tile.count; j += BLOCK) {
+            const uint32_t i = tile.start + j, o = tile.smem_off + j;
+            sv[o] = nd.v[i];
+            su[o] = nd.u[i];
+            ss[o] = nd.s[i];
+            stk[o] = nd.tk[i];
+            spi[o] = nd.pidx[i];
+        }
+    }
+    __syncthreads();
+
+    for (uint32_t k = 0; k < nsteps; ++k) {
+        for (uint32_t tix = t_lo; tix < t_hi; ++tix) {
+            const Tile tile = eng->tiles[tix];
+            const uint32_t o = tile.smem_off;
+            process_tile<INT, BLOCK, NPT, true>(eng, tile, k0 + k, sv + o, su + o, ss + o, stk + o, spi + o, sl);
+        }
+        if (k + 1 < nsteps && !grid_barrier(eng->barrier, (k + 1) * gridDim.x, eng->err, s_flag)) break;
+    }
+    __syncthreads();
+
+    for (uint32_t tix = t_lo; tix < t_hi; ++tix) {
+        const Tile tile = eng->tiles[tix];
+        const NetDev &nd = eng->nets[tile.net];
+        for (uint32_t j = threadIdx.x; j < tile.count; j += BLOCK) {
+            const uint32_t i = tile.start + j, o = tile.smem_off + j;
+            nd.v[i] = sv[o];
+            nd.u[i] = su[o];
+            nd.s[i] = ss[o];
+            nd.tk[i] = stk[o];
+        }
     }
 }
 
@@ -242,9 +368,17 @@ __global__ void reset_neurons_kernel(NetDev nd) {
     nd.v[i] = nd.v0[i];
     nd.u[i] = nd.u0[i];
     nd.s[i] = 0.0f;
-    nd.trace[i] = 0.0f;
+    nd.tk[i] = kTraceZero;
     nd.pn_total[i] = 0ull;
     if (nd.wcount) nd.wcount[i] = 0u;
+}
+
+// Backend::trace (lib.rs:137): trace_tab[tk], 0 for kTraceZero.
+__global__ void trace_kernel(const uint16_t *tk, const float *tab, uint32_t n, float *out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint16_t k = tk[i];
+    out[i] = k == kTraceZero ? 0.0f : tab[k];
 }
 
 // spike_counts over the last `rows` record rows (cpu.rs:424-458): thread per
@@ -270,26 +404,7 @@ __global__ void pn_total_kernel(const unsigned long long *pn, uint32_t n, uint32
     out[i] = c > 0xffffffffull ? 0xffffffffu : (uint32_t)c;
 }
 
-// L2 flush helper for timing hygiene: writes a buffer larger than L2.
-__global__ void scrub_kernel(uint4 *buf, size_t n16) {
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n16; k += (size_t)gridDim.x * blockDim.x)
-        buf[k] = make_uint4((uint32_t)k, 0u, 0u, 0u);
-}
-
 // ------------------------------------------------------------- launchers
-template <bool INT, int BLOCK, int NPT>
-static cudaError_t launch_step_t(const EngineDev *eng, uint32_t k_step, uint32_t grid, cudaStream_t st) {
-    step_kernel<INT, BLOCK, NPT><<<grid, BLOCK, 0, st>>>(eng, k_step);
-    return cudaGetLastError();
-}
-
-template <bool INT, int BLOCK, int NPT>
-static int occupancy_t() {
-    int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, BLOCK, NPT>, BLOCK, 0);
-    return b;
-}
-
 #define NE2B_SHAPES(X) \
     X(128, 1) X(128, 2) X(128, 4) X(256, 1) X(256, 2) X(256, 4) X(512, 1) X(512, 2)
 
@@ -308,15 +423,11 @@ void shape_list(uint32_t *blocks, uint32_t *npts, uint32_t *count) {
     *count = c;
 }
 
-cudaError_t launch_step(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,
-                        uint32_t grid, cudaStream_t st) {
-#define X(B, P)                                                                         \
-    if (block == B && npt == P)                                                         \
-        return int_ring ? launch_step_t<true, B, P>(eng, k_step, grid, st)              \
-                        : launch_step_t<false, B, P>(eng, k_step, grid, st);
-    NE2B_SHAPES(X)
-#undef X
-    return cudaErrorInvalidValue;
+template <bool INT, int BLOCK, int NPT>
+static int occupancy_t() {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, BLOCK, NPT>, BLOCK, 0);
+    return b;
 }
 
 int step_occupancy(bool int_ring, uint32_t block, uint32_t npt) {
@@ -325,6 +436,69 @@ int step_occupancy(bool int_ring, uint32_t block, uint32_t npt) {
     NE2B_SHAPES(X)
 #undef X
     return 0;
+}
+
+cudaError_t launch_step(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,
+                        uint32_t grid, cudaStream_t st) {
+#define X(B, P)                                                                \
+    if (block == B && npt == P) {                                              \
+        if (int_ring) step_kernel<true, B, P><<<grid, B, 0, st>>>(eng, k_step);  \
+        else step_kernel<false, B, P><<<grid, B, 0, st>>>(eng, k_step);          \
+        return cudaGetLastError();                                             \
+    }
+    NE2B_SHAPES(X)
+#undef X
+    return cudaErrorInvalidValue;
+}
+
+uint32_t resident_head(uint32_t block, uint32_t npt) {
+#define X(B, P) if (block == B && npt == P) return resident_head_bytes<B, P>();
+    NE2B_SHAPES(X)
+#undef X
+    return 0;
+}
+
+template <bool INT, int BLOCK, int NPT>
+static int resident_occupancy_t(size_t smem) {
+    if (cudaFuncSetAttribute(resident_kernel<INT, BLOCK, NPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return 0;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, resident_kernel<INT, BLOCK, NPT>, BLOCK, smem) !=
+        cudaSuccess)
+        return 0;
+    return b;
+}
+
+int resident_occupancy(bool int_ring, uint32_t block, uint32_t npt, size_t smem) {
+#define X(B, P)                                                                                              \
+    if (block == B && npt == P)                                                                              \
+        return int_ring ? resident_occupancy_t<true, B, P>(smem) : resident_occupancy_t<false, B, P>(smem);
+    NE2B_SHAPES(X)
+#undef X
+    return 0;
+}
+
+template <bool INT, int BLOCK, int NPT>
+static cudaError_t launch_resident_t(const EngineDev *eng, uint32_t k0, uint32_t nsteps, uint32_t grid, size_t smem,
+                                     cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(resident_kernel<INT, BLOCK, NPT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    void *args[] = {(void *)&eng, (void *)&k0, (void *)&nsteps};
+    return cudaLaunchCooperativeKernel((const void *)resident_kernel<INT, BLOCK, NPT>, dim3(grid), dim3(BLOCK), args,
+                                       smem, st);
+}
+
+cudaError_t launch_resident(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k0,
+                            uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st) {
+#define X(B, P)                                                                               \
+    if (block == B && npt == P)                                                               \
+        return int_ring ? launch_resident_t<true, B, P>(eng, k0, nsteps, grid, smem, st)       \
+                        : launch_resident_t<false, B, P>(eng, k0, nsteps, grid, smem, st);
+    NE2B_SHAPES(X)
+#undef X
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st) {
@@ -339,6 +513,12 @@ cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_trace(const uint16_t *tk, const float *tab, uint32_t n, float *out, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    trace_kernel<<<(n + 255) / 256, 256, 0, st>>>(tk, tab, n, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_window_count(const uint32_t *rec_bits, uint32_t rec_rows, uint32_t n_pad, uint32_t n,
                                 unsigned long long t, uint32_t rows, uint32_t *out, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
@@ -349,11 +529,6 @@ cudaError_t launch_window_count(const uint32_t *rec_bits, uint32_t rec_rows, uin
 cudaError_t launch_pn_total(const unsigned long long *pn, uint32_t n, uint32_t *out, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     pn_total_kernel<<<(n + 255) / 256, 256, 0, st>>>(pn, n, out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_scrub(void *buf, size_t bytes, cudaStream_t st) {
-    scrub_kernel<<<1184, 256, 0, st>>>((uint4 *)buf, bytes / 16);
     return cudaGetLastError();
 }
 

@@ -12,11 +12,15 @@ void shape_list(uint32_t *blocks, uint32_t *npts, uint32_t *count);
 int step_occupancy(bool int_ring, uint32_t block, uint32_t npt);
 cudaError_t launch_step(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,
                         uint32_t grid, cudaStream_t st);
+uint32_t resident_head(uint32_t block, uint32_t npt);
+int resident_occupancy(bool int_ring, uint32_t block, uint32_t npt, size_t smem);
+cudaError_t launch_resident(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k0,
+                            uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st);
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st);
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st);
+cudaError_t launch_trace(const uint16_t *tk, const float *tab, uint32_t n, float *out, cudaStream_t st);
 cudaError_t launch_window_count(const uint32_t *rec_bits, uint32_t rec_rows, uint32_t n_pad, uint32_t n,
                                 unsigned long long t, uint32_t rows, uint32_t *out, cudaStream_t st);
 cudaError_t launch_pn_total(const unsigned long long *pn, uint32_t n, uint32_t *out, cudaStream_t st);
-cudaError_t launch_scrub(void *buf, size_t bytes, cudaStream_t st);
 
 }  // namespace ne2b

@@ -4,7 +4,8 @@
 // HBM layout per network (every array is the net's own allocation, so nets
 // can be admitted and retired independently):
 //   neuron state, structure-of-arrays, n_pad = round_up(n, 64) entries:
-//     v, u (model state slots 0/1), s (merged synaptic current), trace,
+//     v, u (model state slots 0/1), s (merged synaptic current), tk (u16
+//     steps since the last spike: trace = trace_tab[tk], 0xFFFF = trace 0),
 //     ext, v0/u0 (reset rows), pidx (u16 index into the param table),
 //     pn_total (u64 lifetime spike counts), wcount (u32 current-window counts)
 //   delay ring: D x n_pad words (int32 fixed point or f32), slot-major, so the
@@ -42,16 +43,22 @@ struct alignas(16) ParamRow {
 
 struct alignas(16) Tile {
     uint32_t net;
-    uint32_t start;  // first local neuron
-    uint32_t count;  // neurons in this tile (<= tile size)
+    uint32_t start;     // first local neuron
+    uint32_t count;     // neurons in this tile (<= tile size)
     uint32_t flags;
+    uint32_t smem_off;  // resident kernel: offset of the tile's state in its block's shared memory
+    uint32_t pad[3];
 };
+
+constexpr uint16_t kTraceZero = 0xFFFFu;  // tk value of a zero trace
 
 // Per-network descriptor.  Device copy read by the kernels; the host keeps a
 // mirror and rewrites the fields it changes.
 struct alignas(16) NetDev {
     // neuron arrays
-    float *v, *u, *s, *trace, *ext;
+    float *v, *u, *s, *ext;
+    uint16_t *tk;              // steps since last spike (trace_tab index), kTraceZero = 0
+    const float *trace_tab;    // trace_tab[k] = decay_t applied k times to 1.0 (f32, in order)
     const float *v0, *u0;
     const uint16_t *pidx;
     unsigned long long *pn_total;
@@ -80,7 +87,8 @@ struct alignas(16) NetDev {
     uint32_t n_inputs, stim_len;
     uint32_t rec_rows, win_steps, max_windows, flags;
     float dt, pkick, kick, decay_s, decay_t, gauss_k;
-    uint32_t pad[2];
+    uint32_t trace_last;  // last index of trace_tab (saturation)
+    uint32_t pad[1];
 };
 
 // Mutable per-net counters, kept apart from the read-mostly descriptor.
@@ -97,6 +105,12 @@ struct EngineDev {
     NetDev *nets;
     const ParamRow *ptab;
     NetCounters *counters;
+    // resident kernel: block b owns tiles [block_tiles[b], block_tiles[b+1])
+    const uint32_t *block_tiles;
+    uint32_t block_neurons;  // shared-memory state capacity per block
+    uint32_t pad0;
+    unsigned int *barrier;   // grid-barrier arrival counter (zeroed before each launch)
+    unsigned int *err;       // nonzero: a grid barrier timed out
 };
 
 }  // namespace ne2b

@@ -187,6 +187,16 @@ class B200Sim:
         a = np.ascontiguousarray(ids, dtype=np.uint32)
         check(lib.ne2b_set_v_watch(self._h, ptr(a), len(a)))
 
+    # --- kernel selection (new) -----------------------------------------
+    def set_kernel_mode(self, mode: int) -> None:
+        """_abi.KERNEL_AUTO / KERNEL_STREAM / KERNEL_RESIDENT."""
+        check(lib.ne2b_set_kernel_mode(self._h, mode))
+
+    def kernel_mode(self) -> tuple[int, bool]:
+        m, r = C.c_int32(), C.c_int32()
+        check(lib.ne2b_kernel_mode(self._h, C.byref(m), C.byref(r)))
+        return int(m.value), bool(r.value)
+
     # --- instrumentation (new) ------------------------------------------
     def stream_handle(self) -> int:
         """The cudaStream_t this sim launches on (for CUDA-event timing)."""
@@ -285,6 +295,14 @@ class Batch:
         p = C.c_void_p()
         check(lib.ne2b_batch_stream(self._h, C.byref(p)))
         return int(p.value or 0)
+
+    def set_kernel_mode(self, mode: int) -> None:
+        check(lib.ne2b_batch_set_kernel_mode(self._h, mode))
+
+    def kernel_mode(self) -> tuple[int, bool]:
+        m, r = C.c_int32(), C.c_int32()
+        check(lib.ne2b_batch_kernel_mode(self._h, C.byref(m), C.byref(r)))
+        return int(m.value), bool(r.value)
 
     def kernel_launches(self) -> int:
         v = C.c_uint64()

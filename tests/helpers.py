@@ -35,12 +35,16 @@ def rows_equal(g: nb.B200Sim, o: O.OSim, rows: int) -> int:
 
 
 def lockstep(onet: O.ONet, steps: int, int_weights: bool = True, chunk: int = 64, exp_mode: int = 1,
-             drive=None, flat=None, **cfg_kw):
+             drive=None, flat=None, mode: int | None = None, **cfg_kw):
     """Run both backends `steps` steps in chunks; return (gpu, oracle,
-    first_divergent_step or -1)."""
+    first_divergent_step or -1).  `mode` forces the step kernel
+    (nb.KERNEL_STREAM / nb.KERNEL_RESIDENT)."""
     flat = flat if flat is not None else onet.flat(cfg_kw.get("dt_ms", 0.1))
     gc, oc = configs(int_weights, chunk, exp_mode, **cfg_kw)
     g = nb.B200Sim(flat, gc)
+    if mode is not None:
+        g.set_kernel_mode(mode)
+        assert g.kernel_mode()[1] == (mode == nb.KERNEL_RESIDENT)
     o = O.OSim(onet, oc)
     if drive:
         drive(g)

@@ -15,6 +15,8 @@ from helpers import FP32_COUNT_RTOL, assert_state_bits_equal, lockstep, set_ext
 
 pytestmark = pytest.mark.gpu
 
+MODES = pytest.mark.parametrize("mode", [nb.KERNEL_STREAM, nb.KERNEL_RESIDENT], ids=["stream", "resident"])
+
 ADEX_TONIC = [281.0, 30.0, -70.6, -50.4, 2.0, 4.0, 144.0, 80.5, -70.6, 20.0]
 
 
@@ -37,8 +39,10 @@ def lsm_like_net(n_side, seed):
     return net
 
 
-def test_fingerprint_net_int_ring_bit_exact():
-    g, o, first = lockstep(fingerprint_net(), 400, int_weights=True, noise_rate_hz=20.0, noise_kick_mv=0.8, seed=7)
+@MODES
+def test_fingerprint_net_int_ring_bit_exact(mode):
+    g, o, first = lockstep(fingerprint_net(), 400, int_weights=True, noise_rate_hz=20.0, noise_kick_mv=0.8, seed=7,
+                           mode=mode)
     assert first < 0, f"raster diverged at step {first}"
     assert_state_bits_equal(g, o)
 
@@ -52,42 +56,46 @@ def test_fingerprint_net_fp32_ring_reproduces_reference_fingerprint():
     assert first < 0 or first > 100, f"fp32 raster diverged at step {first}"
 
 
+@MODES
 @pytest.mark.parametrize("n", [10_000])
-def test_random_kout_gauss_noise_int_ring_bit_exact(n):
+def test_random_kout_gauss_noise_int_ring_bit_exact(n, mode):
     """10k workload net (random K=100, U(0,0.5)/U(0,1)x0.7 weights, distance
     delays), Gaussian current noise sd 1, tau_syn 5 ms, 2000 steps."""
     onet = O.ONet.random_kout(n, 100, 1)
     g, o, first = lockstep(onet, 2000, int_weights=True, chunk=100, gauss_sd=1.0, synapse_tau_ms=5.0,
-                           drive=lambda s: set_ext(s, n, range(0, n, 7), 6.0))
+                           drive=lambda s: set_ext(s, n, range(0, n, 7), 6.0), mode=mode)
     assert first < 0, f"raster diverged at step {first}"
     assert g.spikes_total() > 0
     assert_state_bits_equal(g, o)
 
 
-def test_bench_net_event_heavy_int_ring_bit_exact():
+@MODES
+def test_bench_net_event_heavy_int_ring_bit_exact(mode):
     """bench_net regime (sim/src/bench.rs:10-52): 500 Hz x 20 mV kicks, w 4.2/5."""
     onet = O.ONet.bench_net(4000, 100, 5, 0.7, 5.0)
     g, o, first = lockstep(onet, 1500, int_weights=True, chunk=100, noise_rate_hz=500.0, noise_kick_mv=20.0,
-                           seed=3)
+                           seed=3, mode=mode)
     assert first < 0, f"raster diverged at step {first}"
     rate = o.mean_rate_hz()
     assert rate > 5.0, rate
     assert_state_bits_equal(g, o)
 
 
-def test_adex_random_net_int_ring_bit_exact():
+@MODES
+def test_adex_random_net_int_ring_bit_exact(mode):
     onet = O.ONet.random_kout(3000, 50, 4, w_scale=0.7 * 281.0)
     for i in range(onet.n):
         onet.set_model(i, O.ADEX, ADEX_TONIC)
     g, o, first = lockstep(onet, 1500, int_weights=True, chunk=100, gauss_sd=1.0, exp_mode=1,
-                           drive=lambda s: set_ext(s, 3000, range(0, 3000, 5), 900.0))
+                           drive=lambda s: set_ext(s, 3000, range(0, 3000, 5), 900.0), mode=mode)
     assert first < 0, f"raster diverged at step {first}"
     assert g.spikes_total() > 0
     assert_state_bits_equal(g, o)
 
 
+@MODES
 @pytest.mark.parametrize("model", [O.IZH, O.ADEX])
-def test_liquid_with_input_streams_int_ring_bit_exact(model):
+def test_liquid_with_input_streams_int_ring_bit_exact(model, mode):
     onet = O.ONet.liquid(12, 7, model=model)
     rng = np.random.default_rng(3)
     bits = (rng.random((200, 8)) < 0.05).astype(np.float32)
@@ -97,7 +105,7 @@ def test_liquid_with_input_streams_int_ring_bit_exact(model):
         for k in range(8):
             s.play_input(k, series[:, k])
 
-    g, o, first = lockstep(onet, 2000, int_weights=True, chunk=100, drive=drive)
+    g, o, first = lockstep(onet, 2000, int_weights=True, chunk=100, drive=drive, mode=mode)
     assert first < 0, f"raster diverged at step {first}"
     assert g.spikes_total() > 0
     assert_state_bits_equal(g, o)
@@ -179,12 +187,54 @@ def test_int_weights_close_to_float():
     assert abs(tf - ti) / tf < 0.3
 
 
-def test_100k_workload_int_ring_bit_exact_first_1000_steps():
+@MODES
+def test_100k_workload_int_ring_bit_exact_first_1000_steps(mode):
     """The 100k configuration (random K=100, ~10M synapses) against the
     oracle for 1000 steps, every raster row compared."""
     onet = O.ONet.random_kout(100_000, 100, 1)
     g, o, first = lockstep(onet, 1000, int_weights=True, chunk=100, gauss_sd=1.0, synapse_tau_ms=5.0,
-                           drive=lambda s: set_ext(s, 100_000, range(0, 100_000, 11), 8.0))
+                           drive=lambda s: set_ext(s, 100_000, range(0, 100_000, 11), 8.0), mode=mode)
     assert first < 0, f"raster diverged at step {first}"
     assert g.spikes_total() > 0
     assert_state_bits_equal(g, o)
+
+
+def test_auto_mode_picks_resident_when_state_fits_and_stream_when_not():
+    small = nb.random_kout(20_000, 10, 1)
+    g = nb.B200Sim(small)
+    assert g.kernel_mode() == (nb.KERNEL_AUTO, True)
+    n = 3_000_000  # 16 B of on-chip state per neuron exceeds 148 SMs x 227 KB
+    big = nb.FlatNet(model=np.zeros(n, np.uint8), params=np.tile(np.float32([0.02, 0.2, -65, 8]), (n, 1)),
+                     src_ptr=np.zeros(n + 1, np.uint32), tgt=np.zeros(0, np.uint32), w=np.zeros(0, np.float32),
+                     delay_steps=np.zeros(0, np.uint16))
+    b = nb.B200Sim(big, int_weights=1)
+    assert b.kernel_mode() == (nb.KERNEL_AUTO, False)
+    with pytest.raises(nb.Ne2bError, match="UNSUPPORTED"):
+        b.set_kernel_mode(nb.KERNEL_RESIDENT)
+    assert b.kernel_mode() == (nb.KERNEL_AUTO, False)
+    b.set_external_all(np.full(n, 10.0, np.float32))
+    b.run_steps(20)
+    assert b.step_count() == 20 and b.spikes_total() == 0
+
+
+def test_resident_and_stream_agree_over_many_launches():
+    """Long run crossing many resident launches (4096 steps each) and stimulus
+    chunks: both kernels give the same state bit-for-bit."""
+    onet = O.ONet.liquid(10, 3)
+    flat = onet.flat()
+    x = (np.random.default_rng(5).random((1000, 8)) < 0.05).astype(np.float32).repeat(10, axis=0)
+    sims = []
+    for mode in (nb.KERNEL_STREAM, nb.KERNEL_RESIDENT):
+        s = nb.B200Sim(flat, int_weights=1, record_spikes=1, gauss_sd=2.0, noise_rate_hz=50.0)
+        s.set_kernel_mode(mode)
+        for k in range(8):
+            s.play_input(k, x[:, k])
+        s.run_steps(9000)
+        s.run_steps(1000)
+        sims.append(s)
+    a, b = sims
+    assert a.spikes_total() == b.spikes_total() > 0
+    for slot in (0, 1):
+        assert np.array_equal(a.state(slot).view(np.uint32), b.state(slot).view(np.uint32))
+    assert np.array_equal(a.trace().view(np.uint32), b.trace().view(np.uint32))
+    assert np.array_equal(a.spike_counts(400), b.spike_counts(400))

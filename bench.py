@@ -202,8 +202,10 @@ def run_profile(args):
 
     import neuro_edit_v2_b200 as nb
 
-    net = nb.random_kout(N, K_OUT, SEED)
+    net = nb.random_kout(args.profile_neurons, K_OUT, SEED)
     sim = nb.B200Sim(net, make_cfg(nb, args.active))
+    if args.kernel:
+        sim.set_kernel_mode({"stream": nb.KERNEL_STREAM, "resident": nb.KERNEL_RESIDENT}[args.kernel])
     scrub = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
     ms, spikes, launches = timed_trials(sim, 1, 3, args.trial_steps, 1, torch, scrub)
     print(json.dumps({"profile_run": True, "trial_steps": args.trial_steps, "ms": ms, "spikes": spikes,
@@ -433,6 +435,7 @@ def bench_serving(nb, count: int):
         nxt = 0
         done = 0
         refused = 0
+        ready = []
         t0 = time.perf_counter()
         while done < count:
             now = time.perf_counter() - t0
@@ -449,11 +452,21 @@ def bench_serving(nb, count: int):
                     time.sleep(max(0.0, arrivals[order[nxt]] - (time.perf_counter() - t0)))
                 continue
             srv.step()
-            for rid in srv.finished():
+            # results of requests retired by the previous launch are ready (or
+            # nearly): taking them one launch late keeps the device busy
+            for rid in ready:
                 counts, _ = srv.take(rid)
                 r = ids[rid]
                 lat[r] = time.perf_counter() - t0 - arrivals[r]
                 done += 1
+            ready = srv.finished()
+            if srv.stats()["active"] == 0 and nxt >= count:
+                for rid in ready:
+                    counts, _ = srv.take(rid)
+                    r = ids[rid]
+                    lat[r] = time.perf_counter() - t0 - arrivals[r]
+                    done += 1
+                ready = []
         span = time.perf_counter() - t0
         srv.close()
         return lat, span, refused
@@ -561,6 +574,8 @@ def main():
     ap.add_argument("--profile", action="store_true", help="short run for ncu captures")
     ap.add_argument("--trial-steps", type=int, default=200, help="trial length in --profile mode")
     ap.add_argument("--active", action="store_true", help="--profile the active (Poisson-kick) regime")
+    ap.add_argument("--profile-neurons", type=int, default=N, help="network size in --profile mode")
+    ap.add_argument("--kernel", choices=["stream", "resident"], default=None, help="force the step kernel")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -31,11 +31,12 @@ struct ne2b_batch {
 
 struct ne2b_server {
     struct Req {
-        uint32_t slot = 0, n = 0, windows = 0;
+        uint32_t slot = 0, n = 0, n_pad = 0, windows = 0;
         uint64_t steps = 0, fp_neurons = 0, fp_syn = 0, fp_ring = 0;
         bool done = false;
-        std::vector<uint16_t> counts;
-        uint64_t spikes = 0;
+        uint16_t *d_win = nullptr;           // window counts, kept on device until taken
+        unsigned long long *d_spk = nullptr; // spike total copied at retirement
+        cudaEvent_t ev = nullptr;            // retirement copies complete
     };
     Engine eng;
     ne2b_server_config cfg{};
@@ -43,6 +44,20 @@ struct ne2b_server {
     std::vector<uint64_t> finished;
     uint64_t used_neurons = 0, used_syn = 0, used_ring = 0;
     uint64_t next_id = 1, admitted = 0, retired = 0;
+    cudaStream_t rstream = nullptr;  // result copies
+    cudaEvent_t step_ev[2] = {nullptr, nullptr};
+    uint64_t step_no = 0;
+    ~ne2b_server() {
+        eng.sync();
+        for (auto &kv : reqs) {
+            if (kv.second.d_win) cudaFree(kv.second.d_win);
+            if (kv.second.d_spk) cudaFree(kv.second.d_spk);
+            if (kv.second.ev) cudaEventDestroy(kv.second.ev);
+        }
+        for (cudaEvent_t e : step_ev)
+            if (e) cudaEventDestroy(e);
+        if (rstream) cudaStreamDestroy(rstream);
+    }
 };
 
 #define GUARD(expr)                                                            \
@@ -508,11 +523,16 @@ ne2b_status ne2b_server_create(const ne2b_server_config *cfg, int device, ne2b_s
         s->cfg = *cfg;
         if (s->cfg.steps_per_launch == 0) s->cfg.steps_per_launch = 64;
         ne2b_status st = s->eng.init(device, cfg->int_weights != 0, cfg->max_requests);
+        if (st == NE2B_OK) st = s->eng.set_mode(ne2b::kModeStream);
+        if (st == NE2B_OK) st = ne2b::cuda_error(cudaStreamCreateWithFlags(&s->rstream, cudaStreamNonBlocking), "result stream");
+        for (int k = 0; k < 2 && st == NE2B_OK; ++k)
+            st = ne2b::cuda_error(cudaEventCreateWithFlags(&s->step_ev[k], cudaEventDisableTiming), "event");
         if (st != NE2B_OK) {
             delete s;
             return st;
         }
         s->eng.graph_steps = s->cfg.steps_per_launch;
+        s->eng.fixed_grid = true;
         *out = s;
         return NE2B_OK;
     })());
@@ -547,6 +567,7 @@ ne2b_status ne2b_server_submit(ne2b_server *s, const ne2b_net_desc *net, const n
         ne2b_status st2 = s->eng.add_net(net, &cfg, inputs, steps, &r.slot);
         if (st2 != NE2B_OK) return st2;
         r.n = net->n;
+        r.n_pad = (uint32_t)fn;
         r.windows = (uint32_t)(steps / cfg.window_steps);
         r.steps = steps;
         r.fp_neurons = fn;
@@ -566,30 +587,51 @@ ne2b_status ne2b_server_submit(ne2b_server *s, const ne2b_net_desc *net, const n
 ne2b_status ne2b_server_step(ne2b_server *s, uint32_t *active_out, uint32_t *finished_out) {
     if (!s) return set_error(NE2B_EINVAL, "null server handle");
     GUARD(([&]() -> ne2b_status {
+        // at most two launch groups in flight: host admission and retirement
+        // work overlaps the device without queueing unboundedly ahead of it
+        cudaEvent_t &ev = s->step_ev[s->step_no & 1];
+        if (s->step_no >= 2) {
+            ne2b_status st0 = ne2b::cuda_error(cudaEventSynchronize(ev), "step event");
+            if (st0 != NE2B_OK) return st0;
+        }
         ne2b_status st = s->eng.run_steps(s->cfg.steps_per_launch);
         if (st != NE2B_OK) return st;
+        st = ne2b::cuda_error(cudaEventRecord(ev, s->eng.stream()), "step event");
+        if (st != NE2B_OK) return st;
+        s->step_no++;
         uint32_t fin = 0, act = 0;
         for (auto &kv : s->reqs) {
             ne2b_server::Req &r = kv.second;
             if (r.done) continue;
             NetHost *h = s->eng.net(r.slot);
-            if (h && h->t >= h->t_end) {
-                r.counts.resize((size_t)r.windows * r.n);
-                for (uint32_t w = 0; w < r.windows && st == NE2B_OK; ++w)
-                    st = s->eng.window_counts(*h, w, r.counts.data() + (size_t)w * r.n);
-                if (st == NE2B_OK) st = s->eng.spikes_total(*h, &r.spikes);
-                if (st == NE2B_OK) st = s->eng.remove_net(r.slot);
-                if (st != NE2B_OK) return st;
-                r.done = true;
-                s->used_neurons -= r.fp_neurons;
-                s->used_syn -= r.fp_syn;
-                s->used_ring -= r.fp_ring;
-                s->retired++;
-                s->finished.push_back(kv.first);
-                ++fin;
-            } else {
+            if (!(h && h->t >= h->t_end)) {
                 ++act;
+                continue;
             }
+            // retire, stream-ordered after the launch that finished it: the
+            // spike total is copied out of the shared counter array, the
+            // window counts stay allocated until the result is taken
+            r.d_win = h->dev.win_out;
+            cudaStream_t st_main = s->eng.stream();
+            st = ne2b::cuda_error(cudaMallocAsync((void **)&r.d_spk, sizeof(unsigned long long), st_main), "result");
+            if (st == NE2B_OK)
+                st = ne2b::cuda_error(cudaMemcpyAsync(r.d_spk, s->eng.counter_ptr(r.slot), sizeof(unsigned long long),
+                                                      cudaMemcpyDeviceToDevice, st_main), "result");
+            if (st == NE2B_OK) st = s->eng.remove_net(r.slot, false, r.d_win);
+            if (st == NE2B_OK) st = ne2b::cuda_error(cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming), "event");
+            if (st == NE2B_OK) st = ne2b::cuda_error(cudaEventRecord(r.ev, st_main), "event");
+            if (st != NE2B_OK) return st;
+            r.done = true;
+            s->used_neurons -= r.fp_neurons;
+            s->used_syn -= r.fp_syn;
+            s->used_ring -= r.fp_ring;
+            s->retired++;
+            s->finished.push_back(kv.first);
+            ++fin;
+        }
+        if (fin) {
+            st = s->eng.rebuild_tiles();
+            if (st != NE2B_OK) return st;
         }
         if (active_out) *active_out = act;
         if (finished_out) *finished_out = fin;
@@ -610,13 +652,33 @@ ne2b_status ne2b_server_take_result(ne2b_server *s, uint64_t id, uint16_t *count
     if (!s) return set_error(NE2B_EINVAL, "null server handle");
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return set_error(NE2B_EINVAL, "unknown request %llu", (unsigned long long)id);
-    if (!it->second.done) return set_error(NE2B_ENODATA, "request %llu is still running", (unsigned long long)id);
-    if (counts && !it->second.counts.empty())
-        memcpy(counts, it->second.counts.data(), sizeof(uint16_t) * it->second.counts.size());
-    if (spikes_total) *spikes_total = it->second.spikes;
-    s->reqs.erase(it);
-    s->finished.erase(std::remove(s->finished.begin(), s->finished.end(), id), s->finished.end());
-    return NE2B_OK;
+    ne2b_server::Req &r = it->second;
+    if (!r.done) return set_error(NE2B_ENODATA, "request %llu is still running", (unsigned long long)id);
+    GUARD(([&]() -> ne2b_status {
+        // the copies wait only for this request's retirement, not for the
+        // launches queued after it
+        ne2b_status st = ne2b::cuda_error(cudaStreamWaitEvent(s->rstream, r.ev, 0), "result wait");
+        std::vector<uint16_t> rows((size_t)r.windows * r.n_pad);
+        unsigned long long tot = 0;
+        if (st == NE2B_OK && !rows.empty() && r.d_win)
+            st = ne2b::cuda_error(cudaMemcpyAsync(rows.data(), r.d_win, sizeof(uint16_t) * rows.size(),
+                                                  cudaMemcpyDeviceToHost, s->rstream), "result copy");
+        if (st == NE2B_OK && r.d_spk)
+            st = ne2b::cuda_error(cudaMemcpyAsync(&tot, r.d_spk, sizeof tot, cudaMemcpyDeviceToHost, s->rstream),
+                                  "result copy");
+        if (st == NE2B_OK) st = ne2b::cuda_error(cudaStreamSynchronize(s->rstream), "result copy");
+        if (st != NE2B_OK) return st;
+        if (counts)
+            for (uint32_t w = 0; w < r.windows; ++w)
+                memcpy(counts + (size_t)w * r.n, rows.data() + (size_t)w * r.n_pad, sizeof(uint16_t) * r.n);
+        if (spikes_total) *spikes_total = tot;
+        if (r.d_win) cudaFreeAsync(r.d_win, s->rstream);
+        if (r.d_spk) cudaFreeAsync(r.d_spk, s->rstream);
+        cudaEventDestroy(r.ev);
+        s->reqs.erase(it);
+        s->finished.erase(std::remove(s->finished.begin(), s->finished.end(), id), s->finished.end());
+        return NE2B_OK;
+    })());
 }
 
 ne2b_status ne2b_server_finished_ids(ne2b_server *s, uint64_t *ids, uint32_t cap, uint32_t *count) {

@@ -85,6 +85,10 @@ Engine::~Engine() {
     }
     if (stream_) cudaStreamSynchronize(stream_);
     if (stage_) cudaFreeHost(stage_);
+    for (PinnedBlock &b : pin_) {
+        cudaFreeHost(b.p);
+        cudaEventDestroy(b.ev);
+    }
     cudaFree(d_nets_);
     cudaFree(d_counters_);
     cudaFree(d_ptab_);
@@ -135,6 +139,7 @@ ne2b_status Engine::init(int device, bool int_ring, uint32_t max_nets) {
     NE2B_CUDA(cudaMalloc(&d_barrier_, 2 * sizeof(unsigned int)));
     NE2B_CUDA(cudaMemset(d_barrier_, 0, 2 * sizeof(unsigned int)));
     d_err_ = d_barrier_ + 1;
+    if (const char *pdl = getenv("NE2B_PDL")) set_pdl(strcmp(pdl, "0") != 0);
     if (const char *m = getenv("NE2B_KERNEL")) {
         if (!strcmp(m, "stream")) mode_ = kModeStream;
         else if (!strcmp(m, "resident")) mode_ = kModeResident;
@@ -156,9 +161,9 @@ ne2b_status Engine::upload_eng() {
     e.pad0 = 0;
     e.barrier = d_barrier_;
     e.err = d_err_;
+    // pageable source: the runtime copies it to staging before returning, so
+    // the stack frame may go away without waiting for the device
     NE2B_CUDA(cudaMemcpyAsync(d_eng_, &e, sizeof e, cudaMemcpyHostToDevice, stream_));
-    // the source lives on this stack frame: wait for the copy
-    NE2B_CUDA(cudaStreamSynchronize(stream_));
     return NE2B_OK;
 }
 
@@ -198,7 +203,6 @@ ne2b_status Engine::upload_ptab() {
     }
     NE2B_CUDA(cudaMemcpyAsync(d_ptab_, h_ptab_.data(), sizeof(ParamRow) * h_ptab_.size(), cudaMemcpyHostToDevice,
                               stream_));
-    NE2B_CUDA(cudaStreamSynchronize(stream_));
     ptab_dirty_ = false;
     return NE2B_OK;
 }
@@ -215,8 +219,52 @@ static void fill_noise(NetDev &d, const ne2b_config &c) {
     d.gauss_k = c.gauss_sd != 0.0f ? (float)((double)c.gauss_sd * 1.7320508075688772 / 65536.0) : 0.0f;
 }
 
+// Host-to-device copy through a pool of pinned staging blocks: the source
+// is copied into pinned memory and the DMA is issued asynchronously, so a
+// large upload never waits for the kernels in flight.  Small copies go
+// straight from pageable memory (the runtime stages them on the call).
+ne2b_status Engine::pin_copy(void *dst, const void *src, size_t bytes) {
+    if (!bytes) return NE2B_OK;
+    if (bytes <= (64u << 10)) {
+        NE2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
+        return NE2B_OK;
+    }
+    const size_t need = (bytes + 255) / 256 * 256;
+    if (pin_cur_ >= 0 && pin_[pin_cur_].used + need > pin_[pin_cur_].cap) NE2B_TRY(pin_close());
+    if (pin_cur_ < 0) {
+        for (size_t k = 0; k < pin_.size(); ++k) {
+            if (pin_[k].cap >= need && cudaEventQuery(pin_[k].ev) == cudaSuccess) {
+                pin_cur_ = (int)k;
+                break;
+            }
+        }
+        if (pin_cur_ < 0) {
+            PinnedBlock b;
+            b.cap = std::max<size_t>(need, (size_t)64 << 20);
+            NE2B_CUDA(cudaMallocHost(&b.p, b.cap));
+            NE2B_CUDA(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming));
+            pin_.push_back(b);
+            pin_cur_ = (int)pin_.size() - 1;
+        }
+        pin_[pin_cur_].used = 0;
+    }
+    PinnedBlock &b = pin_[pin_cur_];
+    uint8_t *stage = (uint8_t *)b.p + b.used;
+    memcpy(stage, src, bytes);
+    b.used += need;
+    NE2B_CUDA(cudaMemcpyAsync(dst, stage, bytes, cudaMemcpyHostToDevice, stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::pin_close() {
+    if (pin_cur_ < 0) return NE2B_OK;
+    NE2B_CUDA(cudaEventRecord(pin_[pin_cur_].ev, stream_));
+    pin_cur_ = -1;
+    return NE2B_OK;
+}
+
 ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
-                            uint32_t *slot_out) {
+                            uint32_t *slot_out, bool rebuild) {
     if (!net || !cfg) return set_error(NE2B_EINVAL, "add_net: null net or config");
     const uint32_t n = net->n;
     if (!(cfg->dt_ms >= 0.001f && cfg->dt_ms <= 100.0f))  // lib.rs:35-39 valid_dt_ms
@@ -289,11 +337,7 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
         delete h;
         return st;
     };
-    auto up = [&](void *dst, const void *src, size_t bytes) -> ne2b_status {
-        if (!bytes) return NE2B_OK;
-        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_);
-        return e == cudaSuccess ? NE2B_OK : cuda_error(e, "cudaMemcpyAsync (net upload)");
-    };
+    auto up = [&](void *dst, const void *src, size_t bytes) -> ne2b_status { return pin_copy(dst, src, bytes); };
 #define NET_TRY(x)                          \
     do {                                    \
         ne2b_status _s = (x);               \
@@ -425,37 +469,39 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
         }
         NET_TRY(alloc(&p, sizeof(float) * tab.size())); d.trace_tab = (const float *)p;
         NET_TRY(up((void *)d.trace_tab, tab.data(), sizeof(float) * tab.size()));
-        NET_TRY(cuda_error(cudaStreamSynchronize(stream_), "trace table upload"));
         d.trace_last = (uint32_t)tab.size() - 1;
     }
     fill_noise(d, *cfg);
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
               (cfg->window_steps ? kNetWindows : 0u);
     nets_[slot] = h;
+    NET_TRY(pin_close());
     NET_TRY(reset_net(slot));
-    NET_TRY(rebuild_tiles());
+    if (rebuild) NET_TRY(rebuild_tiles());
 #undef NET_TRY
     *slot_out = slot;
     return NE2B_OK;
 }
 
-ne2b_status Engine::remove_net(uint32_t slot) {
+// Stream-ordered removal: the descriptor is cleared and the net's arrays
+// freed after every kernel already queued; `keep` (if not null) is an
+// allocation handed over to the caller instead of being freed.
+ne2b_status Engine::remove_net(uint32_t slot, bool rebuild, const void *keep) {
     NetHost *h = net(slot);
     if (!h) return set_error(NE2B_EINVAL, "no net in slot %u", slot);
     NetDev z;
     memset(&z, 0, sizeof z);
     NE2B_CUDA(cudaMemcpyAsync(d_nets_ + slot, &z, sizeof z, cudaMemcpyHostToDevice, stream_));
-    for (void *p : h->allocs) NE2B_CUDA(cudaFreeAsync(p, stream_));
-    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    for (void *p : h->allocs)
+        if (p != keep) NE2B_CUDA(cudaFreeAsync(p, stream_));
     nets_[slot] = nullptr;
     delete h;
-    return rebuild_tiles();
+    return rebuild ? rebuild_tiles() : NE2B_OK;
 }
 
 ne2b_status Engine::upload_net(NetHost &h) {
+    // pageable source, staged by the runtime before the call returns
     NE2B_CUDA(cudaMemcpyAsync(d_nets_ + h.slot, &h.dev, sizeof(NetDev), cudaMemcpyHostToDevice, stream_));
-    // h.dev may change right after this returns: wait for the copy
-    NE2B_CUDA(cudaStreamSynchronize(stream_));
     return NE2B_OK;
 }
 
@@ -477,6 +523,7 @@ uint32_t Engine::grid() const {
     const int occ = step_occupancy(int_ring_, shape_.block, shape_.npt);
     if (bps == 0 || (int)bps > occ) bps = (uint32_t)(occ > 0 ? occ : 1);
     uint32_t g = (uint32_t)sm_count_ * bps;
+    if (fixed_grid) return g;  // serving: graphs stay valid as nets come and go
     // never more blocks than tiles: idle blocks still cost launch time
     const uint32_t nt = n_tiles_ ? n_tiles_ : 1;
     return g < nt ? g : nt;
@@ -494,26 +541,30 @@ bool Engine::plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &bloc
     const uint32_t max_bps = std::max<uint32_t>(1, 2048 / shape_.block);
     for (uint32_t bps = shape_.blocks_per_sm ? shape_.blocks_per_sm : max_bps; bps >= 1; --bps) {
         const uint32_t G = (uint32_t)std::min<uint64_t>((uint64_t)sm_count_ * bps, tiles.size());
-        const uint64_t target = (total + G - 1) / G;
-        std::vector<uint32_t> bt(1, 0);
-        uint64_t acc = 0, m = 0;
+        // tile k goes to block floor(prefix_k * G / total): contiguous,
+        // never more than G blocks, balanced to within one tile
+        std::vector<uint32_t> bt(G + 1, (uint32_t)tiles.size());
+        std::vector<uint64_t> sum(G, 0);
+        uint64_t prefix = 0;
+        uint32_t prev = 0;
+        bt[0] = 0;
         for (uint32_t k = 0; k < tiles.size(); ++k) {
-            const uint32_t remaining_tiles = (uint32_t)tiles.size() - k;
-            const uint32_t remaining_blocks = G - (uint32_t)(bt.size() - 1);
-            if (acc > 0 && remaining_blocks > 1 &&
-                (acc + tiles[k].count > target || remaining_tiles < remaining_blocks)) {
-                bt.push_back(k);
-                m = std::max(m, acc);
-                acc = 0;
-            }
-            acc += tiles[k].count;
+            uint32_t blk = (uint32_t)std::min<uint64_t>(G - 1, prefix * G / total);
+            if (blk < prev) blk = prev;
+            for (uint32_t b2 = prev + 1; b2 <= blk; ++b2) bt[b2] = k;
+            prev = blk;
+            sum[blk] += tiles[k].count;
+            prefix += tiles[k].count;
         }
-        bt.push_back((uint32_t)tiles.size());
-        m = std::max(m, acc);
+        for (uint32_t b2 = prev + 1; b2 <= G; ++b2) bt[b2] = (uint32_t)tiles.size();
+        uint64_t m = 0;
+        for (uint64_t x : sum) m = std::max(m, x);
         const size_t smem = head + 16 * (size_t)((m + 3) / 4 * 4);
-        if (smem > 227 * 1024) continue;
-        const int occ = resident_occupancy(int_ring_, shape_.block, shape_.npt, smem);
+        const int occ = smem > 227 * 1024 ? 0 : resident_occupancy(int_ring_, shape_.block, shape_.npt, smem);
         const uint32_t blocks = (uint32_t)bt.size() - 1;
+        if (getenv("NE2B_DEBUG"))
+            fprintf(stderr, "ne2b plan: block %u npt %u bps %u -> %u blocks, %llu neurons/block, smem %zu, occ %d\n",
+                    shape_.block, shape_.npt, bps, blocks, (unsigned long long)m, smem, occ);
         if (occ < 1 || (uint64_t)occ * sm_count_ < blocks) continue;
         // smem offsets within each block
         for (uint32_t b = 0; b + 1 < bt.size(); ++b) {
@@ -556,7 +607,7 @@ ne2b_status Engine::rebuild_tiles() {
     resident_ = plan_resident(tiles, block_tiles);
     if (mode_ == kModeResident && !resident_ && !tiles.empty())
         return set_error(NE2B_UNSUPPORTED, "the nets do not fit the resident kernel's shared memory");
-    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    if (tiles.size() > tiles_cap_ || block_tiles.size() > block_tiles_cap_) NE2B_CUDA(cudaStreamSynchronize(stream_));
     if (tiles.size() > tiles_cap_) {
         uint32_t cap = tiles_cap_;
         while (cap < tiles.size()) cap *= 2;
@@ -573,11 +624,10 @@ ne2b_status Engine::rebuild_tiles() {
         NE2B_CUDA(cudaMalloc(&d_block_tiles_, sizeof(uint32_t) * cap));
         block_tiles_cap_ = cap;
     }
-    if (!tiles.empty())
-        NE2B_CUDA(cudaMemcpy(d_tiles_, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
+    if (!tiles.empty()) NE2B_TRY(pin_copy(d_tiles_, tiles.data(), sizeof(Tile) * tiles.size()));
     if (!block_tiles.empty())
-        NE2B_CUDA(cudaMemcpy(d_block_tiles_, block_tiles.data(), sizeof(uint32_t) * block_tiles.size(),
-                             cudaMemcpyHostToDevice));
+        NE2B_TRY(pin_copy(d_block_tiles_, block_tiles.data(), sizeof(uint32_t) * block_tiles.size()));
+    NE2B_TRY(pin_close());
     n_tiles_ = (uint32_t)tiles.size();
     NE2B_TRY(upload_eng());
     if (grid() != old_grid) clear_graphs();
@@ -696,10 +746,11 @@ ne2b_status Engine::set_input_matrix(NetHost &h, const float *x, uint64_t steps)
     const size_t bytes = sizeof(float) * (size_t)steps * h.n_inputs;
     void *p = nullptr;
     NE2B_CUDA(cudaMallocAsync(&p, bytes, stream_));
-    cudaError_t e = cudaMemcpyAsync(p, x, bytes, cudaMemcpyHostToDevice, stream_);
-    if (e != cudaSuccess) {
+    ne2b_status cs = pin_copy(p, x, bytes);
+    if (cs == NE2B_OK) cs = pin_close();
+    if (cs != NE2B_OK) {
         cudaFreeAsync(p, stream_);
-        return cuda_error(e, "input matrix upload");
+        return cs;
     }
     void *old = (void *)h.dev.stim_buf;
     for (auto &a : h.allocs)

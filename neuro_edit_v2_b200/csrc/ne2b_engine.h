@@ -51,6 +51,12 @@ struct NetHost {
 
 enum KernelMode { kModeAuto = 0, kModeStream = 1, kModeResident = 2 };
 
+struct PinnedBlock {
+    void *p = nullptr;
+    size_t cap = 0, used = 0;
+    cudaEvent_t ev = nullptr;
+};
+
 struct TileShape {
     uint32_t block = 256;
     uint32_t npt = 2;
@@ -66,8 +72,10 @@ class Engine {
     // Adds a net (slot returned).  inputs/steps: a fixed [steps x n_inputs]
     // input matrix (serving); NULL = host-packed stimulus program.
     ne2b_status add_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
-                        uint32_t *slot);
-    ne2b_status remove_net(uint32_t slot);
+                        uint32_t *slot, bool rebuild = true);
+    ne2b_status remove_net(uint32_t slot, bool rebuild = true, const void *keep = nullptr);
+    ne2b_status pin_copy(void *dst, const void *src, size_t bytes);
+    ne2b_status pin_close();
     ne2b_status run_steps(uint64_t steps);
     ne2b_status reset_net(uint32_t slot);
     ne2b_status sync();
@@ -90,6 +98,7 @@ class Engine {
     ne2b_status restore(const std::vector<std::vector<uint8_t>> &snap);
 
     NetHost *net(uint32_t slot) { return slot < nets_.size() ? nets_[slot] : nullptr; }
+    unsigned long long *counter_ptr(uint32_t slot) { return &d_counters_[slot].spikes_total; }
     uint32_t active_nets() const;
     uint64_t dev_bytes() const;
     float last_ms() const { return last_ms_; }
@@ -100,6 +109,7 @@ class Engine {
     bool resident() const { return resident_; }
     int mode() const { return mode_; }
     ne2b_status set_mode(int m);
+    bool fixed_grid = false;  // grid independent of the tile count (serving)
     uint32_t graph_steps = 64;
     uint32_t resident_steps = 4096;  // max steps per resident launch
     uint64_t stim_chunk = 2048;
@@ -147,6 +157,8 @@ class Engine {
     uint32_t res_grid_ = 0;
     unsigned int *d_barrier_ = nullptr;
     unsigned int *d_err_ = nullptr;
+    std::vector<PinnedBlock> pin_;  // pinned staging pool for uploads
+    int pin_cur_ = -1;
     void *stage_ = nullptr;  // pinned staging for stimulus chunks and descriptors
     size_t stage_bytes_ = 0;
 };

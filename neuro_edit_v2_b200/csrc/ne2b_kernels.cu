@@ -172,6 +172,8 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             }
         }
     }
+    // quiet tile: one block barrier, no scan, no delivery
+    if (!__syncthreads_or(wcnt != 0u)) return;
     if (lane == 0) sl.woff[warp] = wcnt;
     __syncthreads();
     if (warp == 0) {
@@ -197,35 +199,35 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     }
     __syncthreads();
     const uint32_t total = *sl.total;
-    if (total) {
-        if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
-        const uint32_t *__restrict__ rowptr = nd.rowptr;
-        const uint32_t *__restrict__ tgt = nd.tgt;
-        const bool d16 = flags & kNetDelay16;
-        for (uint32_t si = warp; si < total; si += NW) {
-            const uint32_t i = sl.list[si];
-            const uint32_t lo = rowptr[i], hi = rowptr[i + 1];
-            for (uint32_t j = lo + lane; j < hi; j += 32) {
-                const uint32_t tg = tgt[j];
-                const uint32_t d =
-                    d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
-                uint32_t slot = tmod + d;
-                if (slot >= D) slot -= D;
-                const size_t idx = (size_t)slot * n_pad + tg;
-                if (INT) {
-                    atomicAdd((int *)ringw + idx, ((const int *)nd.w)[j]);
-                } else {
-                    atomicAdd((float *)ringw + idx, ((const float *)nd.w)[j]);
-                }
+    if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
+    const uint32_t *__restrict__ rowptr = nd.rowptr;
+    const uint32_t *__restrict__ tgt = nd.tgt;
+    const bool d16 = flags & kNetDelay16;
+    for (uint32_t si = warp; si < total; si += NW) {
+        const uint32_t i = sl.list[si];
+        const uint32_t lo = rowptr[i], hi = rowptr[i + 1];
+        for (uint32_t j = lo + lane; j < hi; j += 32) {
+            const uint32_t tg = tgt[j];
+            const uint32_t d =
+                d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
+            uint32_t slot = tmod + d;
+            if (slot >= D) slot -= D;
+            const size_t idx = (size_t)slot * n_pad + tg;
+            if (INT) {
+                atomicAdd((int *)ringw + idx, ((const int *)nd.w)[j]);
+            } else {
+                atomicAdd((float *)ringw + idx, ((const float *)nd.w)[j]);
             }
         }
     }
+    // the next tile reuses the shared spike list
     __syncthreads();
 }
 
 // ------------------------------------------------------ streaming kernel
 template <bool INT, int BLOCK, int NPT>
 __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
+    pdl_enter();
     __shared__ uint32_t s_list[BLOCK * NPT];
     __shared__ uint32_t s_woff[BLOCK / 32];
     __shared__ uint32_t s_total;
@@ -254,35 +256,43 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p) {
 
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s
 
-// Grid barrier for a cooperative launch.  Arrival: block-wide barrier, a
-// gpu-scope fence by thread 0 (publishes the block's ring deliveries), one
-// atomic increment of the counter.  Wait: thread 0 polls the counter with
-// acquire loads until every block of the grid has arrived; it gives up
-// after kBarrierLimitNs or as soon as another block has flagged an error.
-// Returns false (for every thread of the block) when the launch must stop.
+__device__ __forceinline__ unsigned int atom_add_release_gpu(unsigned int *p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// Grid barrier for a cooperative launch.  Arrival: block-wide barrier, then
+// thread 0 publishes the block's ring deliveries (gpu-scope fence) and
+// increments the counter with a release atomic; the last block to arrive
+// sees target - 1 and does not wait.  The others poll the counter with
+// acquire loads; every 64 polls they check the error flag (another block
+// gave up) and the %globaltimer limit, after which they flag the error and
+// stop.  Returns false (for every thread of the block) when the launch must
+// stop.
 __device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int target, unsigned int *err,
                                              unsigned int *s_flag) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        atomicAdd(counter, 1u);
         unsigned int ok = 1u;
-        if (ld_acquire_gpu(counter) < target) {
+        if (atom_add_release_gpu(counter, 1u) + 1u < target) {
             const unsigned long long t0 = globaltimer_ns();
-            while (ld_acquire_gpu(counter) < target) {
-                if (ld_acquire_gpu(err) != 0u) {
-                    ok = 0u;
-                    break;
+            for (uint32_t polls = 1;; ++polls) {
+                if (ld_acquire_gpu(counter) >= target) break;
+                if ((polls & 63u) == 0u) {
+                    if (ld_acquire_gpu(err) != 0u) {
+                        ok = 0u;
+                        break;
+                    }
+                    if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+                        atomicExch(err, 1u);
+                        ok = 0u;
+                        break;
+                    }
                 }
-                if (globaltimer_ns() - t0 > kBarrierLimitNs) {
-                    atomicExch(err, 1u);
-                    ok = 0u;
-                    break;
-                }
-                __nanosleep(64);
             }
         }
-        __threadfence();
         *s_flag = ok;
     }
     __syncthreads();
@@ -351,6 +361,7 @@ __global__ void __launch_bounds__(BLOCK) resident_kernel(const EngineDev *__rest
 
 // Advance every active net by `steps` after a launch group (t and t % D).
 __global__ void advance_kernel(NetDev *nets, uint32_t n_nets, uint32_t steps) {
+    pdl_enter();
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_nets) return;
     NetDev &nd = nets[j];
@@ -438,14 +449,31 @@ int step_occupancy(bool int_ring, uint32_t block, uint32_t npt) {
     return 0;
 }
 
+static bool g_pdl = true;
+void set_pdl(bool on) { g_pdl = on; }
+
+template <typename... Args>
+static cudaError_t launch_ex(void (*kernel)(Args...), uint32_t grid, uint32_t block, cudaStream_t st,
+                             Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g_pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 cudaError_t launch_step(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,
                         uint32_t grid, cudaStream_t st) {
-#define X(B, P)                                                                \
-    if (block == B && npt == P) {                                              \
-        if (int_ring) step_kernel<true, B, P><<<grid, B, 0, st>>>(eng, k_step);  \
-        else step_kernel<false, B, P><<<grid, B, 0, st>>>(eng, k_step);          \
-        return cudaGetLastError();                                             \
-    }
+#define X(B, P)                                                                            \
+    if (block == B && npt == P)                                                            \
+        return int_ring ? launch_ex(step_kernel<true, B, P>, grid, B, st, eng, k_step)     \
+                        : launch_ex(step_kernel<false, B, P>, grid, B, st, eng, k_step);
     NE2B_SHAPES(X)
 #undef X
     return cudaErrorInvalidValue;
@@ -503,8 +531,7 @@ cudaError_t launch_resident(bool int_ring, uint32_t block, uint32_t npt, const E
 
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st) {
     if (n_nets == 0) return cudaSuccess;
-    advance_kernel<<<(n_nets + 127) / 128, 128, 0, st>>>(nets, n_nets, steps);
-    return cudaGetLastError();
+    return launch_ex(advance_kernel, (n_nets + 127) / 128, 128, st, nets, n_nets, steps);
 }
 
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st) {

@@ -8,6 +8,7 @@
 namespace ne2b {
 
 bool shape_supported(uint32_t block, uint32_t npt);
+void set_pdl(bool on);  // programmatic dependent launch of the streaming kernels (default on)
 void shape_list(uint32_t *blocks, uint32_t *npts, uint32_t *count);
 int step_occupancy(bool int_ring, uint32_t block, uint32_t npt);
 cudaError_t launch_step(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,

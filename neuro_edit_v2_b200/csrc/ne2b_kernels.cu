@@ -224,6 +224,15 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     __syncthreads();
 }
 
+// Programmatic dependent launch: let the next kernel of the stream be
+// scheduled now, then wait until the previous one has completed and its
+// memory is visible (griddepcontrol.wait).  Both are no-ops for a kernel
+// launched without the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ------------------------------------------------------ streaming kernel
 template <bool INT, int BLOCK, int NPT>
 __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {

@@ -223,6 +223,7 @@ def run_ours(args):
     dev = local
     net = nb.random_kout(N, K_OUT, SEED + rank)
     sim = nb.B200Sim(net, make_cfg(nb, False), device=dev)
+    tiling = sim.autotune(256)
     scrub = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
 
     with Clocks(dev) as clk:
@@ -240,6 +241,7 @@ def run_ours(args):
 
     # active companion regime (same net, Poisson kicks on top)
     act = nb.B200Sim(net, make_cfg(nb, True), device=dev)
+    a_tiling = act.autotune(256)
     a_ms, a_spikes, _ = timed_trials(act, max(1, args.steps // 2), 1, TRIAL_STEPS, ws, torch, scrub)
     a_ms = max_over_ranks(a_ms, ws)
     a_trials = max(1, args.steps // 2)
@@ -306,7 +308,9 @@ def run_ours(args):
             "firing_rate_hz": a_spikes / (N * a_trials * TRIAL_STEPS * 1e-4),
             "ms_per_trial": a_ms / a_trials,
             "roofline_frac": a_alg / (a_ms / (TRIAL_STEPS * a_trials) / 1000.0) / 1e9 / peak,
+            "tiling": a_tiling,
         },
+        "tiling": tiling,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
                      "alg_bytes_per_launch": alg_bytes, "launch_us": launch_ms * 1000.0,
@@ -338,6 +342,7 @@ def bench_1m(nb, torch, scrub, model: int, steps: int, warmup: int, peak: float)
         nb.to_adex(net)
     sim = nb.B200Sim(net, nb.default_config(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0, seed=SEED))
     del net
+    tiling = sim.autotune(128)
     ms, spikes, launches = timed_trials(sim, steps, warmup, trial, 1, torch, scrub)
     per_launch_s = ms / 1000.0 / (trial * steps)
     b_neuron = 84 if adex else B_NEURON
@@ -349,7 +354,7 @@ def bench_1m(nb, torch, scrub, model: int, steps: int, warmup: int, peak: float)
            "firing_rate_hz": spikes / (n * steps * trial * 1e-4), "ms_per_trial": ms / steps,
            "roofline": {"achieved_gbs": achieved, "frac": achieved / peak, "alg_bytes_per_launch": alg,
                         "launch_us": per_launch_s * 1e6, "bytes_per_neuron": b_neuron},
-           "gpu_launches": launches, "dev_mem_bytes": sim.dev_mem_bytes()}
+           "gpu_launches": launches, "dev_mem_bytes": sim.dev_mem_bytes(), "tiling": tiling}
     sim.close()
     return out
 
@@ -474,16 +479,18 @@ def bench_serving(nb, count: int):
     arrivals = [q.arrival_s for q in reqs]
     lat, span, refused = serve(arrivals)
     sat_lat, sat_span, _ = serve([0.0] * count)
-    # one at a time: each request alone, back to back (sample)
+    # one at a time: the same server and kernels, each request admitted only
+    # after the previous one finished (sample of the stream)
     sample = min(24, count)
+    srv = nb.Server(neuron_capacity=16 << 20, synapse_capacity=1 << 30, ring_capacity=6 << 30, max_requests=1,
+                    steps_per_launch=100)
     t0 = time.perf_counter()
     for r in range(sample):
-        srv = nb.Server(neuron_capacity=1 << 20, synapse_capacity=1 << 28, ring_capacity=1 << 30, max_requests=1,
-                        steps_per_launch=100)
-        srv.submit(reqs[r].net, W.request_config(reqs[r], 11 + r), reqs[r].inputs, reqs[r].steps)
+        rid = srv.submit(reqs[r].net, W.request_config(reqs[r], 11 + r), reqs[r].inputs, reqs[r].steps)
         while srv.stats()["active"]:
             srv.step()
-        srv.close()
+        srv.take(rid)
+    srv.close()
     one_tps = sample / (time.perf_counter() - t0)
     q = np.quantile(np.array(lat), [0.5, 0.99])
     sq = np.quantile(np.array(sat_lat), [0.5, 0.99])

@@ -142,6 +142,12 @@ ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd);                 /* ne
 enum { NE2B_KERNEL_AUTO = 0, NE2B_KERNEL_STREAM = 1, NE2B_KERNEL_RESIDENT = 2 };
 ne2b_status ne2b_set_kernel_mode(ne2b_sim *sim, int32_t mode);
 ne2b_status ne2b_kernel_mode(ne2b_sim *sim, int32_t *mode, int32_t *resident);
+/* Time every (kernel, tile shape, occupancy) candidate on this sim for
+ * steps_per_trial steps from a device snapshot of its state and keep the
+ * fastest (the state is restored afterwards; AUTO mode may switch kernel). */
+ne2b_status ne2b_autotune(ne2b_sim *sim, uint32_t steps_per_trial);
+ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *neurons_per_thread,
+                            uint32_t *blocks_per_sm);
 
 /* Instrumentation (new): the CUDA stream the handle launches on (a
  * cudaStream_t, for timing with events on the launching stream) and the
@@ -175,8 +181,7 @@ ne2b_status ne2b_batch_synchronize(ne2b_batch *b);
 ne2b_status ne2b_batch_window_counts(ne2b_batch *b, uint32_t net, uint32_t window, uint16_t *out);
 ne2b_status ne2b_batch_spikes_total(ne2b_batch *b, uint32_t net, uint64_t *total);
 ne2b_status ne2b_batch_read_state(ne2b_batch *b, uint32_t net, uint32_t slot, float *out);
-/* Time candidate tile shapes on a snapshot of the batch and keep the
- * fastest (state is restored afterwards). */
+/* As ne2b_autotune, over every net of the batch. */
 ne2b_status ne2b_batch_autotune(ne2b_batch *b, uint32_t steps_per_trial);
 ne2b_status ne2b_batch_tile_shape(ne2b_batch *b, uint32_t *block, uint32_t *neurons_per_thread,
                                   uint32_t *blocks_per_sm);

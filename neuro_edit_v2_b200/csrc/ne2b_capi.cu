@@ -332,6 +332,19 @@ ne2b_status ne2b_kernel_mode(ne2b_sim *sim, int32_t *mode, int32_t *resident) {
     return NE2B_OK;
 }
 
+ne2b_status ne2b_autotune(ne2b_sim *sim, uint32_t steps_per_trial) {
+    CHECK_SIM(sim);
+    GUARD(sim->eng.autotune(steps_per_trial));
+}
+
+ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *npt, uint32_t *bps) {
+    if (!sim || !block || !npt || !bps) return set_error(NE2B_EINVAL, "null argument");
+    *block = sim->eng.shape().block;
+    *npt = sim->eng.shape().npt;
+    *bps = sim->eng.shape().blocks_per_sm;
+    return NE2B_OK;
+}
+
 ne2b_status ne2b_stream(ne2b_sim *sim, void **stream) {
     if (!sim || !stream) return set_error(NE2B_EINVAL, "null argument");
     *stream = (void *)sim->eng.stream();

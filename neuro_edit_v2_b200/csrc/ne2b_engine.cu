@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 
 #include "ne2b_kernels.h"
 
@@ -168,10 +169,19 @@ ne2b_status Engine::upload_eng() {
 }
 
 ne2b_status Engine::param_index(uint32_t model, const float *p, uint32_t np, uint16_t *idx) {
-    std::vector<uint32_t> key(kMaxParams + 1, 0u);
+    std::array<uint32_t, kMaxParams + 1> key{};
     key[0] = model;
     for (uint32_t k = 0; k < np && k < kMaxParams; ++k) memcpy(&key[k + 1], &p[k], 4);
+    if (last_key_valid_ && key == last_key_) {  // consecutive neurons usually share a row
+        *idx = last_idx_;
+        return NE2B_OK;
+    }
     auto it = ptab_index_.find(key);
+    if (it != ptab_index_.end()) {
+        last_key_ = key;
+        last_idx_ = it->second;
+        last_key_valid_ = true;
+    }
     if (it != ptab_index_.end()) {
         *idx = it->second;
         return NE2B_OK;
@@ -186,6 +196,9 @@ ne2b_status Engine::param_index(uint32_t model, const float *p, uint32_t np, uin
     h_ptab_.push_back(r);
     ptab_index_[key] = *idx;
     ptab_dirty_ = true;
+    last_key_ = key;
+    last_idx_ = *idx;
+    last_key_valid_ = true;
     return NE2B_OK;
 }
 
@@ -537,6 +550,9 @@ bool Engine::plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &bloc
     if (tiles.empty() || mode_ == kModeStream) return false;
     uint64_t total = 0;
     for (const Tile &t : tiles) total += t.count;
+    // AUTO: the resident kernel's grid barrier pays off only while a step's
+    // work is small (measured crossover between 100k and 300k neurons)
+    if (mode_ == kModeAuto && total > kResidentAutoMax) return false;
     const uint32_t head = resident_head(shape_.block, shape_.npt);
     const uint32_t max_bps = std::max<uint32_t>(1, 2048 / shape_.block);
     for (uint32_t bps = shape_.blocks_per_sm ? shape_.blocks_per_sm : max_bps; bps >= 1; --bps) {
@@ -930,21 +946,23 @@ ne2b_status Engine::refresh_noise(NetHost &h) {
 }
 
 // Snapshot of every mutable device array (state, ring, record, windows,
-// descriptors, counters) for the autotuner's trial runs.
-ne2b_status Engine::snapshot(std::vector<std::vector<uint8_t>> &snap) {
-    NE2B_CUDA(cudaStreamSynchronize(stream_));
-    snap.clear();
-    auto grab = [&](const void *p, size_t bytes) -> ne2b_status {
-        std::vector<uint8_t> b(bytes);
-        if (bytes) NE2B_CUDA(cudaMemcpy(b.data(), p, bytes, cudaMemcpyDeviceToHost));
-        snap.push_back(std::move(b));
+// descriptors, counters) in device memory, for the autotuner's trials.
+ne2b_status Engine::snapshot(EngineSnapshot &snap) {
+    snap.items.clear();
+    snap.hosts.clear();
+    auto grab = [&](void *live, size_t bytes) -> ne2b_status {
+        if (!live || !bytes) return NE2B_OK;
+        void *b = nullptr;
+        NE2B_CUDA(cudaMallocAsync(&b, bytes, stream_));
+        snap.items.push_back({live, b, bytes});
+        NE2B_CUDA(cudaMemcpyAsync(b, live, bytes, cudaMemcpyDeviceToDevice, stream_));
         return NE2B_OK;
     };
     NE2B_TRY(grab(d_nets_, sizeof(NetDev) * nets_cap_));
     NE2B_TRY(grab(d_counters_, sizeof(NetCounters) * nets_cap_));
     for (NetHost *h : nets_) {
         if (!h) continue;
-        const NetDev &d = h->dev;
+        NetDev &d = h->dev;
         const size_t np = h->n_pad;
         NE2B_TRY(grab(d.v, 4 * np));
         NE2B_TRY(grab(d.u, 4 * np));
@@ -955,79 +973,84 @@ ne2b_status Engine::snapshot(std::vector<std::vector<uint8_t>> &snap) {
         NE2B_TRY(grab(d.rec_bits, d.rec_bits ? 4 * (size_t)d.rec_rows * (np / 32) : 0));
         NE2B_TRY(grab(d.wcount, d.wcount ? 4 * np : 0));
         NE2B_TRY(grab(d.win_out, d.win_out ? 2 * (size_t)d.max_windows * np : 0));
+        snap.hosts.push_back({h->slot, h->t, h->dev});
     }
     return NE2B_OK;
 }
 
-ne2b_status Engine::restore(const std::vector<std::vector<uint8_t>> &snap) {
-    NE2B_CUDA(cudaStreamSynchronize(stream_));
-    size_t k = 0;
-    auto put = [&](void *p) -> ne2b_status {
-        const std::vector<uint8_t> &b = snap[k++];
-        if (!b.empty()) NE2B_CUDA(cudaMemcpy(p, b.data(), b.size(), cudaMemcpyHostToDevice));
-        return NE2B_OK;
-    };
-    NE2B_TRY(put(d_nets_));
-    NE2B_TRY(put(d_counters_));
-    for (NetHost *h : nets_) {
+ne2b_status Engine::restore(const EngineSnapshot &snap) {
+    for (const auto &it : snap.items)
+        NE2B_CUDA(cudaMemcpyAsync(it.live, it.backup, it.bytes, cudaMemcpyDeviceToDevice, stream_));
+    for (const auto &hs : snap.hosts) {
+        NetHost *h = net(hs.slot);
         if (!h) continue;
-        NetDev &d = h->dev;
-        NE2B_TRY(put(d.v));
-        NE2B_TRY(put(d.u));
-        NE2B_TRY(put(d.s));
-        NE2B_TRY(put(d.tk));
-        NE2B_TRY(put(d.pn_total));
-        NE2B_TRY(put(d.ring));
-        NE2B_TRY(put(d.rec_bits));
-        NE2B_TRY(put(d.wcount));
-        NE2B_TRY(put(d.win_out));
-        // host mirrors follow the restored descriptor
-        const NetDev *dd = reinterpret_cast<const NetDev *>(snap[0].data()) + h->slot;
-        h->t = dd->t;
-        h->dev.t = dd->t;
-        h->dev.tmod = dd->tmod;
-        h->dev.stim_t0 = dd->stim_t0;
-        h->dev.stim_len = dd->stim_len;
+        h->t = hs.t;
+        h->dev = hs.dev;
     }
     return NE2B_OK;
 }
 
-// Time each compiled tile shape (and half occupancy) on the live nets for
-// `steps_per_trial` steps, restoring the state after every trial; keep the
-// fastest.
+void Engine::drop(EngineSnapshot &snap) {
+    for (const auto &it : snap.items) cudaFreeAsync(it.backup, stream_);
+    snap.items.clear();
+    snap.hosts.clear();
+}
+
+// Time every (kernel, tile shape, occupancy) candidate on the live nets for
+// `steps_per_trial` steps, restoring the state after each trial, and keep
+// the fastest.  Candidates: the streaming kernel at full and half
+// occupancy, the resident kernel wherever its shared-memory plan fits.
 ne2b_status Engine::autotune(uint32_t steps_per_trial) {
     if (steps_per_trial == 0) steps_per_trial = graph_steps;
-    std::vector<std::vector<uint8_t>> snap;
+    EngineSnapshot snap;
     NE2B_TRY(snapshot(snap));
     uint32_t blocks[32], npts[32], count = 0;
     shape_list(blocks, npts, &count);
+    const int saved_mode = mode_;
     TileShape best = shape_;
+    int best_mode = mode_ == kModeAuto ? (resident_ ? kModeResident : kModeStream) : mode_;
     float best_ms = 1e30f;
-    for (uint32_t c = 0; c < count; ++c) {
-        const int occ = step_occupancy(int_ring_, blocks[c], npts[c]);
-        for (int half = 0; half < 2; ++half) {
-            TileShape s;
-            s.block = blocks[c];
-            s.npt = npts[c];
-            s.blocks_per_sm = half ? (uint32_t)std::max(1, occ / 2) : 0;
-            if (half && occ < 2) continue;
-            NE2B_TRY(set_shape(s));
-            NE2B_TRY(restore(snap));
-            NE2B_TRY(run_steps(graph_steps));  // capture + warm
-            NE2B_CUDA(cudaEventRecord(ev0_, stream_));
-            NE2B_TRY(run_steps(steps_per_trial));
-            NE2B_CUDA(cudaEventRecord(ev1_, stream_));
-            NE2B_CUDA(cudaEventSynchronize(ev1_));
-            float ms = 0.0f;
-            NE2B_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
-            if (ms < best_ms) {
-                best_ms = ms;
-                best = s;
+    for (int m : {(int)kModeStream, (int)kModeResident}) {
+        for (uint32_t c = 0; c < count; ++c) {
+            const int occ = step_occupancy(int_ring_, blocks[c], npts[c]);
+            for (int half = 0; half < 2; ++half) {
+                if (half && (m == kModeResident || occ < 2)) continue;
+                TileShape s;
+                s.block = blocks[c];
+                s.npt = npts[c];
+                s.blocks_per_sm = half ? (uint32_t)std::max(1, occ / 2) : 0;
+                mode_ = m;
+                shape_ = s;
+                clear_graphs();
+                if (rebuild_tiles() != NE2B_OK) continue;  // resident plan does not fit
+                NE2B_TRY(restore(snap));
+                NE2B_TRY(run_steps(graph_steps));  // capture + warm
+                NE2B_CUDA(cudaEventRecord(ev0_, stream_));
+                NE2B_TRY(run_steps(steps_per_trial));
+                NE2B_CUDA(cudaEventRecord(ev1_, stream_));
+                NE2B_CUDA(cudaEventSynchronize(ev1_));
+                NE2B_TRY(check_err());
+                float ms = 0.0f;
+                NE2B_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = s;
+                    best_mode = m;
+                }
             }
         }
     }
-    NE2B_TRY(set_shape(best));
+    mode_ = saved_mode == kModeAuto ? best_mode : saved_mode;
+    if (saved_mode != kModeAuto && best_mode != saved_mode) {
+        // a forced kernel keeps its mode; take its best shape instead
+        mode_ = saved_mode;
+    }
+    shape_ = best;
+    clear_graphs();
+    NE2B_TRY(rebuild_tiles());
     NE2B_TRY(restore(snap));
+    drop(snap);
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
     last_ms_ = best_ms;
     return NE2B_OK;
 }

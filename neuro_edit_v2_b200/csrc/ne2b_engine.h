@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <array>
 #include <map>
 #include <string>
 #include <vector>
@@ -50,6 +51,22 @@ struct NetHost {
 };
 
 enum KernelMode { kModeAuto = 0, kModeStream = 1, kModeResident = 2 };
+
+constexpr uint64_t kResidentAutoMax = 150000;  // neurons
+
+struct EngineSnapshot {
+    struct Item {
+        void *live, *backup;
+        size_t bytes;
+    };
+    struct Host {
+        uint32_t slot;
+        uint64_t t;
+        NetDev dev;
+    };
+    std::vector<Item> items;
+    std::vector<Host> hosts;
+};
 
 struct PinnedBlock {
     void *p = nullptr;
@@ -94,8 +111,9 @@ class Engine {
     ne2b_status set_ext(NetHost &h, const float *ext, uint32_t len);
     ne2b_status set_input_matrix(NetHost &h, const float *x, uint64_t steps);
     ne2b_status refresh_noise(NetHost &h);
-    ne2b_status snapshot(std::vector<std::vector<uint8_t>> &snap);
-    ne2b_status restore(const std::vector<std::vector<uint8_t>> &snap);
+    ne2b_status snapshot(EngineSnapshot &snap);
+    ne2b_status restore(const EngineSnapshot &snap);
+    void drop(EngineSnapshot &snap);
 
     NetHost *net(uint32_t slot) { return slot < nets_.size() ? nets_[slot] : nullptr; }
     unsigned long long *counter_ptr(uint32_t slot) { return &d_counters_[slot].spikes_total; }
@@ -134,7 +152,10 @@ class Engine {
     NetCounters *d_counters_ = nullptr;
     uint32_t nets_cap_ = 0;
     std::vector<ParamRow> h_ptab_;
-    std::map<std::vector<uint32_t>, uint16_t> ptab_index_;
+    std::map<std::array<uint32_t, kMaxParams + 1>, uint16_t> ptab_index_;
+    std::array<uint32_t, kMaxParams + 1> last_key_{};
+    uint16_t last_idx_ = 0;
+    bool last_key_valid_ = false;
     ParamRow *d_ptab_ = nullptr;
     uint32_t ptab_cap_ = 0;
     bool ptab_dirty_ = false;

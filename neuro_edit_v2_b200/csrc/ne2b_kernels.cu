@@ -426,7 +426,7 @@ __global__ void pn_total_kernel(const unsigned long long *pn, uint32_t n, uint32
 
 // ------------------------------------------------------------- launchers
 #define NE2B_SHAPES(X) \
-    X(128, 1) X(128, 2) X(128, 4) X(256, 1) X(256, 2) X(256, 4) X(512, 1) X(512, 2)
+    X(128, 1) X(128, 2) X(128, 4) X(128, 8) X(256, 1) X(256, 2) X(256, 4) X(256, 8) X(512, 1) X(512, 2) X(512, 4)
 
 bool shape_supported(uint32_t block, uint32_t npt) {
 #define X(B, P) if (block == B && npt == P) return true;

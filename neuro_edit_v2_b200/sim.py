@@ -197,6 +197,17 @@ class B200Sim:
         check(lib.ne2b_kernel_mode(self._h, C.byref(m), C.byref(r)))
         return int(m.value), bool(r.value)
 
+    def autotune(self, steps_per_trial: int = 128) -> dict:
+        """Pick the fastest kernel and tile shape for this net (state kept)."""
+        check(lib.ne2b_autotune(self._h, steps_per_trial))
+        return self.tiling()
+
+    def tiling(self) -> dict:
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib.ne2b_tile_shape(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"kernel": "resident" if self.kernel_mode()[1] else "stream", "block": int(a.value),
+                "neurons_per_thread": int(b.value), "blocks_per_sm": int(c.value)}
+
     # --- instrumentation (new) ------------------------------------------
     def stream_handle(self) -> int:
         """The cudaStream_t this sim launches on (for CUDA-event timing)."""

@@ -164,3 +164,22 @@ def test_window_counts_equal_sliding_spike_counts():
         ref = g.spike_counts(250)
         assert np.array_equal(g.window_counts(w).astype(np.uint32), ref)
     assert g.windows_done() == 6
+
+
+def test_sim_autotune_restores_state_and_keeps_results():
+    """Autotuning times candidate kernels on device snapshots and restores
+    the state: a tuned sim continues bit-identically to an untuned one."""
+    onet = O.ONet.bench_net(6000, 40, 9, 0.7, 5.0)
+    a = nb.B200Sim(onet.flat(), int_weights=1, record_spikes=1, noise_rate_hz=300.0)
+    b = nb.B200Sim(onet.flat(), int_weights=1, record_spikes=1, noise_rate_hz=300.0)
+    a.run_steps(300)
+    b.run_steps(300)
+    tiling = a.autotune(64)
+    assert tiling["kernel"] in ("stream", "resident") and tiling["block"] in (128, 256, 512)
+    assert a.step_count() == 300
+    a.run_steps(700)
+    b.run_steps(700)
+    assert a.spikes_total() == b.spikes_total() > 0
+    assert np.array_equal(a.v().view(np.uint32), b.v().view(np.uint32))
+    assert np.array_equal(a.trace().view(np.uint32), b.trace().view(np.uint32))
+    assert np.array_equal(a.spike_counts(512), b.spike_counts(512))

@@ -444,7 +444,10 @@ def bench_serving(nb, count: int):
         t0 = time.perf_counter()
         while done < count:
             now = time.perf_counter() - t0
+            budget = time.perf_counter() + 0.002  # admit for <= 2 ms, then keep the device fed
             while nxt < count and arrivals[order[nxt]] <= now:
+                if time.perf_counter() > budget and srv.stats()["active"] > 0:
+                    break
                 r = order[nxt]
                 rid = srv.submit(reqs[r].net, W.request_config(reqs[r], 11 + r), reqs[r].inputs, reqs[r].steps)
                 if rid is None:

@@ -10,10 +10,31 @@
 
 #include <algorithm>
 #include <array>
+#include <mutex>
+#include <thread>
 
 #include "ne2b_kernels.h"
 
 namespace ne2b {
+
+// Split [0, n) over up to 8 host threads when n is large (synapse-sized
+// loops of admission); small ranges run inline.
+template <class F>
+static void parallel_for(uint64_t n, F f) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned T = std::min(8u, hw ? hw : 1u);
+    if (n < (1u << 20) || T <= 1) {
+        f((uint64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const uint64_t chunk = (n + T - 1) / T;
+    for (unsigned k = 0; k < T; ++k) {
+        const uint64_t lo = k * chunk, hi = std::min(n, lo + chunk);
+        if (lo < hi) th.emplace_back(f, lo, hi);
+    }
+    for (auto &x : th) x.join();
+}
 
 static thread_local std::string g_err;
 
@@ -236,12 +257,7 @@ static void fill_noise(NetDev &d, const ne2b_config &c) {
 // is copied into pinned memory and the DMA is issued asynchronously, so a
 // large upload never waits for the kernels in flight.  Small copies go
 // straight from pageable memory (the runtime stages them on the call).
-ne2b_status Engine::pin_copy(void *dst, const void *src, size_t bytes) {
-    if (!bytes) return NE2B_OK;
-    if (bytes <= (64u << 10)) {
-        NE2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
-        return NE2B_OK;
-    }
+ne2b_status Engine::pin_reserve(size_t bytes, void **host) {
     const size_t need = (bytes + 255) / 256 * 256;
     if (pin_cur_ >= 0 && pin_[pin_cur_].used + need > pin_[pin_cur_].cap) NE2B_TRY(pin_close());
     if (pin_cur_ < 0) {
@@ -262,11 +278,26 @@ ne2b_status Engine::pin_copy(void *dst, const void *src, size_t bytes) {
         pin_[pin_cur_].used = 0;
     }
     PinnedBlock &b = pin_[pin_cur_];
-    uint8_t *stage = (uint8_t *)b.p + b.used;
-    memcpy(stage, src, bytes);
+    *host = (uint8_t *)b.p + b.used;
     b.used += need;
-    NE2B_CUDA(cudaMemcpyAsync(dst, stage, bytes, cudaMemcpyHostToDevice, stream_));
     return NE2B_OK;
+}
+
+ne2b_status Engine::pin_issue(void *dst, const void *host, size_t bytes) {
+    NE2B_CUDA(cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, stream_));
+    return NE2B_OK;
+}
+
+ne2b_status Engine::pin_copy(void *dst, const void *src, size_t bytes) {
+    if (!bytes) return NE2B_OK;
+    if (bytes <= (64u << 10)) {
+        NE2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
+        return NE2B_OK;
+    }
+    void *stage = nullptr;
+    NE2B_TRY(pin_reserve(bytes, &stage));
+    parallel_for(bytes, [&](uint64_t lo, uint64_t hi) { memcpy((uint8_t *)stage + lo, (const uint8_t *)src + lo, hi - lo); });
+    return pin_issue(dst, stage, bytes);
 }
 
 ne2b_status Engine::pin_close() {
@@ -289,18 +320,38 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
         return set_error(NE2B_EINVAL, "src_ptr[n] = %u but n_syn = %llu", net->src_ptr[n],
                          (unsigned long long)net->n_syn);
     if (net->n_syn > 0xffffffffull) return set_error(NE2B_UNSUPPORTED, "more than 2^32-1 synapses in one net");
-    uint32_t maxd = 1;
     for (uint32_t i = 0; i < n; ++i)
         if (net->src_ptr[i] > net->src_ptr[i + 1]) return set_error(NE2B_EINVAL, "src_ptr not monotone at %u", i);
-    for (uint64_t j = 0; j < net->n_syn; ++j) {
-        if (net->tgt[j] >= n) return set_error(NE2B_EINVAL, "synapse %llu targets %u >= n %u", (unsigned long long)j, net->tgt[j], n);
-        const uint32_t d = net->delay_steps[j];
-        if (d < 1) return set_error(NE2B_EINVAL, "synapse %llu has delay 0 steps", (unsigned long long)j);
-        if (d > maxd) maxd = d;
-        if (net->tau_ms && net->tau_ms[j] > 0.0f)
-            return set_error(NE2B_UNSUPPORTED, "per-synapse tau (synapse %llu) is not supported by this backend",
-                             (unsigned long long)j);
+    // one parallel pass over the synapses: target range, delay range, tau
+    uint32_t maxd = 1, mind = 0xffff, maxt = 0;
+    bool any_tau = false;
+    {
+        std::mutex mu;
+        parallel_for(net->n_syn, [&](uint64_t lo, uint64_t hi) {
+            uint32_t mx = 1, mn = 0xffff, mt = 0;
+            bool tau = false;
+            for (uint64_t j = lo; j < hi; ++j) {
+                const uint32_t d = net->delay_steps[j];
+                mx = d > mx ? d : mx;
+                mn = d < mn ? d : mn;
+                mt = net->tgt[j] > mt ? net->tgt[j] : mt;
+            }
+            if (net->tau_ms)
+                for (uint64_t j = lo; j < hi; ++j) tau |= net->tau_ms[j] > 0.0f;
+            std::lock_guard<std::mutex> g(mu);
+            maxd = std::max(maxd, mx);
+            mind = std::min(mind, mn);
+            maxt = std::max(maxt, mt);
+            any_tau |= tau;
+        });
     }
+    if (net->n_syn && maxt >= n) {
+        for (uint64_t j = 0; j < net->n_syn; ++j)
+            if (net->tgt[j] >= n)
+                return set_error(NE2B_EINVAL, "synapse %llu targets %u >= n %u", (unsigned long long)j, net->tgt[j], n);
+    }
+    if (net->n_syn && mind < 1) return set_error(NE2B_EINVAL, "a synapse has delay 0 steps");
+    if (any_tau) return set_error(NE2B_UNSUPPORTED, "per-synapse tau is not supported by this backend");
     for (uint32_t i = 0; i < n; ++i)
         if (net->model[i] > 1) return set_error(NE2B_EINVAL, "neuron %u: unknown model id %u", i, net->model[i]);
     if (n > 0 && net->n_inputs > 0 && net->stim_ptr) {
@@ -396,7 +447,6 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
             u0[i] = row[1] * v0[i];
         }
     }
-    if (n > 0) pidx[n - 1] = pidx[n - 1];
     NET_TRY(upload_ptab());
     NET_TRY(up((void *)d.pidx, pidx.data(), sizeof(uint16_t) * np));
     NET_TRY(up((void *)d.v0, v0.data(), sizeof(float) * np));
@@ -405,18 +455,26 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     NET_TRY(up((void *)d.rowptr, net->src_ptr, sizeof(uint32_t) * ((size_t)n + 1)));
     NET_TRY(up((void *)d.tgt, net->tgt, sizeof(uint32_t) * h->e));
     if (int_ring_) {
-        std::vector<int32_t> wq(h->e);
-        for (uint64_t j = 0; j < h->e; ++j) wq[j] = (int32_t)lrintf(net->w[j] * 4096.0f);  // kernels.rs:61 rt_put
-        NET_TRY(up((void *)d.w, wq.data(), 4 * h->e));
+        // fixed-point weights, kernels.rs:61 rt_put: lrintf(w * 4096), written
+        // straight into pinned staging by several threads
+        int32_t *wq = nullptr;
+        NET_TRY(pin_reserve(4 * h->e, (void **)&wq));
+        parallel_for(h->e, [&](uint64_t lo, uint64_t hi) {
+            for (uint64_t j = lo; j < hi; ++j) wq[j] = (int32_t)lrintf(net->w[j] * 4096.0f);
+        });
+        NET_TRY(pin_issue((void *)d.w, wq, 4 * h->e));
     } else {
         NET_TRY(up((void *)d.w, net->w, 4 * h->e));
     }
     if (d16) {
         NET_TRY(up((void *)d.delay, net->delay_steps, 2 * h->e));
-    } else {
-        std::vector<uint8_t> d8(h->e);
-        for (uint64_t j = 0; j < h->e; ++j) d8[j] = (uint8_t)net->delay_steps[j];
-        NET_TRY(up((void *)d.delay, d8.data(), h->e));
+    } else if (h->e) {
+        uint8_t *d8 = nullptr;
+        NET_TRY(pin_reserve(h->e, (void **)&d8));
+        parallel_for(h->e, [&](uint64_t lo, uint64_t hi) {
+            for (uint64_t j = lo; j < hi; ++j) d8[j] = (uint8_t)net->delay_steps[j];
+        });
+        NET_TRY(pin_issue((void *)d.delay, d8, h->e));
     }
     // stimulus routing
     const bool has_stim = n > 0 && net->n_inputs > 0 && net->stim_ptr && net->stim_ptr[n] > 0;

@@ -92,6 +92,8 @@ class Engine {
                         uint32_t *slot, bool rebuild = true);
     ne2b_status remove_net(uint32_t slot, bool rebuild = true, const void *keep = nullptr);
     ne2b_status pin_copy(void *dst, const void *src, size_t bytes);
+    ne2b_status pin_reserve(size_t bytes, void **host);
+    ne2b_status pin_issue(void *dst, const void *host, size_t bytes);
     ne2b_status pin_close();
     ne2b_status run_steps(uint64_t steps);
     ne2b_status reset_net(uint32_t slot);

@@ -206,10 +206,11 @@ def run_profile(args):
     sim = nb.B200Sim(net, make_cfg(nb, args.active))
     if args.kernel:
         sim.set_kernel_mode({"stream": nb.KERNEL_STREAM, "resident": nb.KERNEL_RESIDENT}[args.kernel])
+    tiling = sim.autotune(128) if args.autotune else sim.tiling()
     scrub = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
     ms, spikes, launches = timed_trials(sim, 1, 3, args.trial_steps, 1, torch, scrub)
-    print(json.dumps({"profile_run": True, "trial_steps": args.trial_steps, "ms": ms, "spikes": spikes,
-                      "launches": launches}), flush=True)
+    print(json.dumps({"profile_run": True, "neurons": args.profile_neurons, "trial_steps": args.trial_steps,
+                      "ms": ms, "spikes": spikes, "launches": launches, "tiling": tiling}), flush=True)
 
 
 def run_ours(args):
@@ -586,6 +587,7 @@ def main():
     ap.add_argument("--active", action="store_true", help="--profile the active (Poisson-kick) regime")
     ap.add_argument("--profile-neurons", type=int, default=N, help="network size in --profile mode")
     ap.add_argument("--kernel", choices=["stream", "resident"], default=None, help="force the step kernel")
+    ap.add_argument("--autotune", action="store_true", help="--profile with the autotuned kernel and tiling")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

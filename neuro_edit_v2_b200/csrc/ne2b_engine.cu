@@ -207,13 +207,13 @@ ne2b_status Engine::param_index(uint32_t model, const float *p, uint32_t np, uin
         *idx = it->second;
         return NE2B_OK;
     }
-    if (h_ptab_.size() >= 65536)
-        return set_error(NE2B_UNSUPPORTED, "more than 65536 distinct parameter rows in one engine");
+    if (h_ptab_.size() >= kParamAdexBit)
+        return set_error(NE2B_UNSUPPORTED, "more than 32768 distinct parameter rows in one engine");
     ParamRow r;
     memset(&r, 0, sizeof r);
     for (uint32_t k = 0; k < np && k < kMaxParams; ++k) r.p[k] = p[k];
     r.model = model;
-    *idx = (uint16_t)h_ptab_.size();
+    *idx = (uint16_t)(h_ptab_.size() | (model == NE2B_MODEL_ADEX ? kParamAdexBit : 0u));
     h_ptab_.push_back(r);
     ptab_index_[key] = *idx;
     ptab_dirty_ = true;

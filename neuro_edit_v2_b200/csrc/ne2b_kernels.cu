@@ -115,31 +115,38 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             if (row)
                 for (uint32_t j = lo; j < hi; ++j) I = __fadd_rn(I, __fmul_rn(nd.stim_w[j], row[nd.stim_in[j]]));
         }
-        const ParamRow &pr = ptab[pi[q]];
+        // pidx bit 15 marks an AdEx row: an Izhikevich neuron reads only the
+        // first 16 bytes of its parameter row
+        const bool adex = (pi[q] & kParamAdexBit) != 0u;
+        const ParamRow &pr = ptab[pi[q] & ~kParamAdexBit];
         float p[10];
         const float4 p0 = *reinterpret_cast<const float4 *>(&pr.p[0]);
-        const float4 p1 = *reinterpret_cast<const float4 *>(&pr.p[4]);
-        const float4 p2 = *reinterpret_cast<const float4 *>(&pr.p[8]);
         p[0] = p0.x; p[1] = p0.y; p[2] = p0.z; p[3] = p0.w;
-        p[4] = p1.x; p[5] = p1.y; p[6] = p1.z; p[7] = p1.w;
-        p[8] = p2.x; p[9] = p2.y;
-        const uint32_t model = pr.model;
-        const float gain = model == 1u ? p[0] : 1.0f;  // model/mod.rs:104-106, adex.rs:189-191
+        if (adex) {
+            const float4 p1 = *reinterpret_cast<const float4 *>(&pr.p[4]);
+            const float4 p2 = *reinterpret_cast<const float4 *>(&pr.p[8]);
+            p[4] = p1.x; p[5] = p1.y; p[6] = p1.z; p[7] = p1.w;
+            p[8] = p2.x; p[9] = p2.y;
+        }
+        const float gain = adex ? p[0] : 1.0f;  // model/mod.rs:104-106, adex.rs:189-191
         if (pkick > 0.0f || gauss_k != 0.0f) {
             const uint64_t base = noise_base(i, t, seed);
             if (pkick > 0.0f && noise_fires(base, pkick)) I = __fadd_rn(I, __fmul_rn(kick, gain));
             if (gauss_k != 0.0f)
                 I = __fadd_rn(I, __fmul_rn(__int2float_rn(gauss_numer(base)), __fmul_rn(gauss_k, gain)));
         }
-        const bool sp = model == 1u ? adex_step(p, v[q], u[q], I, dt) : izh_step(p, v[q], u[q], I, dt);
+        const bool sp = adex ? adex_step(p, v[q], u[q], I, dt) : izh_step(p, v[q], u[q], I, dt);
         // trace: 1 on spike, else one more multiply by decay_t (saturating at
         // the table's last entry, 0 or the subnormal fixed point)
-        uint32_t k = tk[q];
-        k = sp ? 0u : (k == kTraceZero ? k : (k < tlast ? k + 1u : tlast));
+        const uint32_t k0 = tk[q];
+        const uint32_t k = sp ? 0u : (k0 == kTraceZero ? k0 : (k0 < tlast ? k0 + 1u : tlast));
+        const float snew = __fmul_rn(sv, decay_s);
         vs[off] = v[q];
         us[off] = u[q];
-        ss[off] = __fmul_rn(sv, decay_s);
-        tks[off] = (uint16_t)k;
+        // s and tk are written only when they change (quiet neurons keep s = 0
+        // and a zero trace step after step)
+        if (__float_as_uint(snew) != __float_as_uint(s[q])) ss[off] = snew;
+        if (k != k0) tks[off] = (uint16_t)k;
         if (sp) nd.pn_total[i] += 1ull;
         if (windows) {
             if (win_end) {

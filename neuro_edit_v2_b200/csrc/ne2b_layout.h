@@ -6,7 +6,8 @@
 //   neuron state, structure-of-arrays, n_pad = round_up(n, 64) entries:
 //     v, u (model state slots 0/1), s (merged synaptic current), tk (u16
 //     steps since the last spike: trace = trace_tab[tk], 0xFFFF = trace 0),
-//     ext, v0/u0 (reset rows), pidx (u16 index into the param table),
+//     ext, v0/u0 (reset rows), pidx (u16 index into the param table, bit 15
+//     set for AdEx rows),
 //     pn_total (u64 lifetime spike counts), wcount (u32 current-window counts)
 //   delay ring: D x n_pad words (int32 fixed point or f32), slot-major, so the
 //     neuron pass reads one contiguous slot row per step
@@ -51,6 +52,7 @@ struct alignas(16) Tile {
 };
 
 constexpr uint16_t kTraceZero = 0xFFFFu;  // tk value of a zero trace
+constexpr uint32_t kParamAdexBit = 0x8000u;  // pidx bit: the row is an AdEx row
 
 // Per-network descriptor.  Device copy read by the kernels; the host keeps a
 // mirror and rewrites the fields it changes.

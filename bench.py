@@ -206,6 +206,9 @@ def run_profile(args):
     sim = nb.B200Sim(net, make_cfg(nb, args.active))
     if args.kernel:
         sim.set_kernel_mode({"stream": nb.KERNEL_STREAM, "resident": nb.KERNEL_RESIDENT}[args.kernel])
+    if args.shape:
+        b, npt = (int(x) for x in args.shape.split("x"))
+        sim.set_tile_shape(b, npt)
     tiling = sim.autotune(128) if args.autotune else sim.tiling()
     scrub = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
     ms, spikes, launches = timed_trials(sim, 1, 3, args.trial_steps, 1, torch, scrub)
@@ -588,6 +591,7 @@ def main():
     ap.add_argument("--profile-neurons", type=int, default=N, help="network size in --profile mode")
     ap.add_argument("--kernel", choices=["stream", "resident"], default=None, help="force the step kernel")
     ap.add_argument("--autotune", action="store_true", help="--profile with the autotuned kernel and tiling")
+    ap.add_argument("--shape", default=None, help="--profile with tile shape BLOCKxNPT, e.g. 256x2")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

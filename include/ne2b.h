@@ -148,6 +148,8 @@ ne2b_status ne2b_kernel_mode(ne2b_sim *sim, int32_t *mode, int32_t *resident);
 ne2b_status ne2b_autotune(ne2b_sim *sim, uint32_t steps_per_trial);
 ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *neurons_per_thread,
                             uint32_t *blocks_per_sm);
+ne2b_status ne2b_set_tile_shape(ne2b_sim *sim, uint32_t block, uint32_t neurons_per_thread,
+                                uint32_t blocks_per_sm);
 
 /* Instrumentation (new): the CUDA stream the handle launches on (a
  * cudaStream_t, for timing with events on the launching stream) and the

@@ -337,6 +337,15 @@ ne2b_status ne2b_autotune(ne2b_sim *sim, uint32_t steps_per_trial) {
     GUARD(sim->eng.autotune(steps_per_trial));
 }
 
+ne2b_status ne2b_set_tile_shape(ne2b_sim *sim, uint32_t block, uint32_t npt, uint32_t bps) {
+    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
+    ne2b::TileShape sh;
+    sh.block = block;
+    sh.npt = npt;
+    sh.blocks_per_sm = bps;
+    GUARD(sim->eng.set_shape(sh));
+}
+
 ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *npt, uint32_t *bps) {
     if (!sim || !block || !npt || !bps) return set_error(NE2B_EINVAL, "null argument");
     *block = sim->eng.shape().block;

@@ -202,6 +202,9 @@ class B200Sim:
         check(lib.ne2b_autotune(self._h, steps_per_trial))
         return self.tiling()
 
+    def set_tile_shape(self, block: int, neurons_per_thread: int, blocks_per_sm: int = 0) -> None:
+        check(lib.ne2b_set_tile_shape(self._h, block, neurons_per_thread, blocks_per_sm))
+
     def tiling(self) -> dict:
         a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
         check(lib.ne2b_tile_shape(self._h, C.byref(a), C.byref(b), C.byref(c)))

@@ -445,6 +445,7 @@ def bench_serving(nb, count: int):
         done = 0
         refused = 0
         ready = []
+        tm = {"admit_s": 0.0, "step_s": 0.0, "take_s": 0.0}
         t0 = time.perf_counter()
         while done < count:
             now = time.perf_counter() - t0
@@ -453,7 +454,9 @@ def bench_serving(nb, count: int):
                 if time.perf_counter() > budget and srv.stats()["active"] > 0:
                     break
                 r = order[nxt]
+                ta = time.perf_counter()
                 rid = srv.submit(reqs[r].net, W.request_config(reqs[r], 11 + r), reqs[r].inputs, reqs[r].steps)
+                tm["admit_s"] += time.perf_counter() - ta
                 if rid is None:
                     refused += 1
                     break
@@ -463,14 +466,18 @@ def bench_serving(nb, count: int):
                 if nxt < count:
                     time.sleep(max(0.0, arrivals[order[nxt]] - (time.perf_counter() - t0)))
                 continue
+            ts = time.perf_counter()
             srv.step()
+            tm["step_s"] += time.perf_counter() - ts
             # results of requests retired by the previous launch are ready (or
             # nearly): taking them one launch late keeps the device busy
+            tt = time.perf_counter()
             for rid in ready:
                 counts, _ = srv.take(rid)
                 r = ids[rid]
                 lat[r] = time.perf_counter() - t0 - arrivals[r]
                 done += 1
+            tm["take_s"] += time.perf_counter() - tt
             ready = srv.finished()
             if srv.stats()["active"] == 0 and nxt >= count:
                 for rid in ready:
@@ -481,11 +488,15 @@ def bench_serving(nb, count: int):
                 ready = []
         span = time.perf_counter() - t0
         srv.close()
+        tm["span_s"] = span
+        serve.timing = tm
         return lat, span, refused
 
     arrivals = [q.arrival_s for q in reqs]
     lat, span, refused = serve(arrivals)
+    t_poisson = dict(serve.timing)
     sat_lat, sat_span, _ = serve([0.0] * count)
+    t_sat = dict(serve.timing)
     # one at a time: the same server and kernels, each request admitted only
     # after the previous one finished (sample of the stream)
     sample = min(24, count)
@@ -505,7 +516,8 @@ def bench_serving(nb, count: int):
     return {"requests": count, "offered_rate_hz": 200.0, "trials_per_s": count / span, "p50_ms": q[0] * 1e3,
             "p99_ms": q[1] * 1e3, "refused_admissions": refused,
             "saturated": {"trials_per_s": count / sat_span, "p50_ms": sq[0] * 1e3, "p99_ms": sq[1] * 1e3,
-                          "neuron_updates_per_s": neuron_steps / sat_span},
+                          "neuron_updates_per_s": neuron_steps / sat_span, "host_time": t_sat},
+            "host_time": t_poisson,
             "one_at_a_time_trials_per_s": one_tps, "one_at_a_time_sample": sample,
             "served_vs_one_at_a_time": (count / span) / one_tps,
             "saturated_vs_one_at_a_time": (count / sat_span) / one_tps,

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <mutex>
 #include <thread>
 
@@ -307,9 +308,15 @@ ne2b_status Engine::pin_close() {
     return NE2B_OK;
 }
 
+static double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
                             uint32_t *slot_out, bool rebuild) {
     if (!net || !cfg) return set_error(NE2B_EINVAL, "add_net: null net or config");
+    const bool dbg = getenv("NE2B_DEBUG") != nullptr;
+    double tp[8] = {now_ms()};
     const uint32_t n = net->n;
     if (!(cfg->dt_ms >= 0.001f && cfg->dt_ms <= 100.0f))  // lib.rs:35-39 valid_dt_ms
         return set_error(NE2B_EINVAL, "dt_ms %g outside [0.001, 100]", (double)cfg->dt_ms);
@@ -364,6 +371,7 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     if (cfg->window_steps > 0 && cfg->window_steps > 131070u)
         return set_error(NE2B_EINVAL, "window_steps %u would overflow the u16 window counts", cfg->window_steps);
     if (inputs && net->n_inputs == 0) inputs = nullptr;
+    tp[1] = now_ms();
 
     uint32_t slot = nets_cap_;
     for (uint32_t j = 0; j < nets_cap_; ++j)
@@ -428,6 +436,7 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     const bool d16 = h->D > 256;
     NET_TRY(alloc(&p, (d16 ? 2 : 1) * h->e)); d.delay = p;
 
+    tp[2] = now_ms();
     // host-side rows: params -> dictionary, x0
     std::vector<uint16_t> pidx(np, 0);
     std::vector<float> v0(np, 0.0f), u0(np, 0.0f);
@@ -448,6 +457,7 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
         }
     }
     NET_TRY(upload_ptab());
+    tp[3] = now_ms();
     NET_TRY(up((void *)d.pidx, pidx.data(), sizeof(uint16_t) * np));
     NET_TRY(up((void *)d.v0, v0.data(), sizeof(float) * np));
     NET_TRY(up((void *)d.u0, u0.data(), sizeof(float) * np));
@@ -476,6 +486,7 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
         });
         NET_TRY(pin_issue((void *)d.delay, d8, h->e));
     }
+    tp[4] = now_ms();
     // stimulus routing
     const bool has_stim = n > 0 && net->n_inputs > 0 && net->stim_ptr && net->stim_ptr[n] > 0;
     if (has_stim) {
@@ -547,8 +558,15 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
               (cfg->window_steps ? kNetWindows : 0u);
     nets_[slot] = h;
     NET_TRY(pin_close());
+    tp[5] = now_ms();
     NET_TRY(reset_net(slot));
+    tp[6] = now_ms();
     if (rebuild) NET_TRY(rebuild_tiles());
+    tp[7] = now_ms();
+    if (dbg)
+        fprintf(stderr, "ne2b add_net n=%u e=%llu: validate %.3f alloc %.3f params %.3f csr %.3f rest %.3f reset %.3f tiles %.3f ms\n",
+                n, (unsigned long long)h->e, tp[1] - tp[0], tp[2] - tp[1], tp[3] - tp[2], tp[4] - tp[3], tp[5] - tp[4],
+                tp[6] - tp[5], tp[7] - tp[6]);
 #undef NET_TRY
     *slot_out = slot;
     return NE2B_OK;

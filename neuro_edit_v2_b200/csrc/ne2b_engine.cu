@@ -258,11 +258,18 @@ static void fill_noise(NetDev &d, const ne2b_config &c) {
 // is copied into pinned memory and the DMA is issued asynchronously, so a
 // large upload never waits for the kernels in flight.  Small copies go
 // straight from pageable memory (the runtime stages them on the call).
+// Blocks used since the last pin_close stay "open": they are never handed
+// out again until pin_close has recorded, after every copy from them was
+// enqueued, the event that marks them reusable.
 ne2b_status Engine::pin_reserve(size_t bytes, void **host) {
     const size_t need = (bytes + 255) / 256 * 256;
-    if (pin_cur_ >= 0 && pin_[pin_cur_].used + need > pin_[pin_cur_].cap) NE2B_TRY(pin_close());
+    if (pin_cur_ >= 0 && pin_[pin_cur_].used + need > pin_[pin_cur_].cap) {
+        pin_open_.push_back(pin_cur_);
+        pin_cur_ = -1;
+    }
     if (pin_cur_ < 0) {
         for (size_t k = 0; k < pin_.size(); ++k) {
+            if (std::find(pin_open_.begin(), pin_open_.end(), (int)k) != pin_open_.end()) continue;
             if (pin_[k].cap >= need && cudaEventQuery(pin_[k].ev) == cudaSuccess) {
                 pin_cur_ = (int)k;
                 break;
@@ -302,8 +309,9 @@ ne2b_status Engine::pin_copy(void *dst, const void *src, size_t bytes) {
 }
 
 ne2b_status Engine::pin_close() {
-    if (pin_cur_ < 0) return NE2B_OK;
-    NE2B_CUDA(cudaEventRecord(pin_[pin_cur_].ev, stream_));
+    if (pin_cur_ >= 0) pin_open_.push_back(pin_cur_);
+    for (int k : pin_open_) NE2B_CUDA(cudaEventRecord(pin_[k].ev, stream_));
+    pin_open_.clear();
     pin_cur_ = -1;
     return NE2B_OK;
 }
@@ -463,28 +471,35 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     NET_TRY(up((void *)d.u0, u0.data(), sizeof(float) * np));
     NET_TRY(cuda_error(cudaMemsetAsync(d.ext, 0, sizeof(float) * np, stream_), "memset ext"));
     NET_TRY(up((void *)d.rowptr, net->src_ptr, sizeof(uint32_t) * ((size_t)n + 1)));
-    NET_TRY(up((void *)d.tgt, net->tgt, sizeof(uint32_t) * h->e));
-    if (int_ring_) {
-        // fixed-point weights, kernels.rs:61 rt_put: lrintf(w * 4096), written
-        // straight into pinned staging by several threads
-        int32_t *wq = nullptr;
-        NET_TRY(pin_reserve(4 * h->e, (void **)&wq));
+    if (h->e) {
+        // one parallel pass over the synapses into pinned staging: targets
+        // copied, weights quantised (kernels.rs:61 rt_put: lrintf(w * 4096))
+        // for the fixed-point ring, delays narrowed to u8 when D <= 256
+        uint32_t *tg = nullptr;
+        void *wst = nullptr;
+        void *dst8 = nullptr;
+        NET_TRY(pin_reserve(4 * h->e, (void **)&tg));
+        NET_TRY(pin_reserve(4 * h->e, &wst));
+        NET_TRY(pin_reserve((d16 ? 2 : 1) * h->e, &dst8));
+        const bool iq = int_ring_;
         parallel_for(h->e, [&](uint64_t lo, uint64_t hi) {
-            for (uint64_t j = lo; j < hi; ++j) wq[j] = (int32_t)lrintf(net->w[j] * 4096.0f);
+            memcpy(tg + lo, net->tgt + lo, 4 * (hi - lo));
+            if (iq) {
+                int32_t *wq = (int32_t *)wst;
+                for (uint64_t j = lo; j < hi; ++j) wq[j] = (int32_t)lrintf(net->w[j] * 4096.0f);
+            } else {
+                memcpy((float *)wst + lo, net->w + lo, 4 * (hi - lo));
+            }
+            if (d16) {
+                memcpy((uint16_t *)dst8 + lo, net->delay_steps + lo, 2 * (hi - lo));
+            } else {
+                uint8_t *d8 = (uint8_t *)dst8;
+                for (uint64_t j = lo; j < hi; ++j) d8[j] = (uint8_t)net->delay_steps[j];
+            }
         });
-        NET_TRY(pin_issue((void *)d.w, wq, 4 * h->e));
-    } else {
-        NET_TRY(up((void *)d.w, net->w, 4 * h->e));
-    }
-    if (d16) {
-        NET_TRY(up((void *)d.delay, net->delay_steps, 2 * h->e));
-    } else if (h->e) {
-        uint8_t *d8 = nullptr;
-        NET_TRY(pin_reserve(h->e, (void **)&d8));
-        parallel_for(h->e, [&](uint64_t lo, uint64_t hi) {
-            for (uint64_t j = lo; j < hi; ++j) d8[j] = (uint8_t)net->delay_steps[j];
-        });
-        NET_TRY(pin_issue((void *)d.delay, d8, h->e));
+        NET_TRY(pin_issue((void *)d.tgt, tg, 4 * h->e));
+        NET_TRY(pin_issue((void *)d.w, wst, 4 * h->e));
+        NET_TRY(pin_issue((void *)d.delay, dst8, (d16 ? 2 : 1) * h->e));
     }
     tp[4] = now_ms();
     // stimulus routing

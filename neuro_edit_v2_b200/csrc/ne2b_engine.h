@@ -182,6 +182,7 @@ class Engine {
     unsigned int *d_err_ = nullptr;
     std::vector<PinnedBlock> pin_;  // pinned staging pool for uploads
     int pin_cur_ = -1;
+    std::vector<int> pin_open_;  // blocks with copies enqueued since the last pin_close
     void *stage_ = nullptr;  // pinned staging for stimulus chunks and descriptors
     size_t stage_bytes_ = 0;
 };

@@ -116,6 +116,15 @@ ne2b_status ne2b_last_spikes(ne2b_sim *sim, uint32_t *out, uint32_t cap, uint32_
 ne2b_status ne2b_spike_counts(ne2b_sim *sim, uint64_t rows, uint32_t *out);
 /* Backend::spike_row: out holds ceil(n/64) words; NE2B_ENODATA outside the window */
 ne2b_status ne2b_spike_row(ne2b_sim *sim, uint32_t back, uint64_t *out);
+/* No counterpart in the reference.  ne2b_spike_counts without any device
+ * allocation, for callers that cannot allocate: a thread serving under a
+ * fixed device-memory budget (any allocation would fail), or one that must
+ * not stall on cudaMalloc/cudaFree, which synchronise the device.  Same
+ * window rules and results as ne2b_spike_counts; the scratch is a 4 MiB
+ * array compiled into the library (held by every GPU that loads it until
+ * exit), so n above 1,048,576 neurons is NE2B_EINVAL.  Calls share that
+ * array: calls whose work overlaps on the GPU race. */
+ne2b_status ne2b_spike_counts_noalloc(ne2b_sim *sim, uint64_t rows, uint32_t *out);
 ne2b_status ne2b_spikes_total(ne2b_sim *sim, uint64_t *total);             /* Backend::spikes_total */
 ne2b_status ne2b_mean_rate_hz(ne2b_sim *sim, double *hz);                  /* Backend::mean_rate_hz */
 /* On-device window counts (new): window w, n values */

@@ -129,6 +129,7 @@ _SIGS = {
     "ne2b_last_spikes": (C.c_int, [_p, _p, _u32, _pu32]),
     "ne2b_spike_counts": (C.c_int, [_p, _u64, _p]),
     "ne2b_spike_row": (C.c_int, [_p, _u32, _p]),
+    "ne2b_spike_counts_noalloc": (C.c_int, [_p, _u64, _p]),
     "ne2b_spikes_total": (C.c_int, [_p, _pu64]),
     "ne2b_mean_rate_hz": (C.c_int, [_p, _pf64]),
     "ne2b_window_counts": (C.c_int, [_p, _u32, _p]),

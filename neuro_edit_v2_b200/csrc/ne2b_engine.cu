@@ -133,6 +133,7 @@ ne2b_status Engine::init(int device, bool int_ring, uint32_t max_nets) {
     device_ = device;
     int_ring_ = int_ring;
     NE2B_CUDA(cudaSetDevice(device));
+    NE2B_TRY(noalloc_setup(device));  // scratch address of ne2b_spike_counts_noalloc
     cudaDeviceProp prop;
     NE2B_CUDA(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10)

@@ -21,6 +21,7 @@ namespace ne2b {
 
 ne2b_status set_error(ne2b_status st, const char *fmt, ...);
 ne2b_status cuda_error(cudaError_t e, const char *what);
+ne2b_status noalloc_setup(int device);  // ne2b_noalloc.cu
 
 // Host mirror of one network's stimulus program (sim/src/stim.rs:9-127).
 struct Stimulus {
@@ -124,6 +125,7 @@ class Engine {
     float last_ms() const { return last_ms_; }
     const TileShape &shape() const { return shape_; }
     cudaStream_t stream() const { return stream_; }
+    int device() const { return device_; }
     bool int_ring() const { return int_ring_; }
     uint64_t launches() const { return launches_; }
     bool resident() const { return resident_; }

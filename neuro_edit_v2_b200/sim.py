@@ -131,6 +131,16 @@ class B200Sim:
         check(st)
         return out
 
+    def spike_counts_noalloc(self, rows: int) -> np.ndarray:
+        """spike_counts that allocates no device memory (fixed 1,048,576-neuron
+        scratch compiled into the library; overlapping calls race)."""
+        out = np.empty(self._n, dtype=np.uint32)
+        st = lib.ne2b_spike_counts_noalloc(self._h, min(int(rows), 2**64 - 1), ptr(out))
+        if st == _abi.NE2B_EWINDOW:
+            raise SpikeWindowError(st, lib.ne2b_last_error().decode())
+        check(st)
+        return out
+
     def spike_row(self, back: int) -> np.ndarray | None:
         out = np.empty((self._n + 63) // 64, dtype=np.uint64)
         st = lib.ne2b_spike_row(self._h, int(back), ptr(out))

@@ -217,6 +217,13 @@ typedef struct {
     uint32_t max_requests;       /* concurrent request slots */
     uint32_t steps_per_launch;   /* steps per graph replay between admissions */
     int32_t int_weights;
+    /* 0: ne2b_server_submit builds the request's device arrays before it
+     * returns.  k > 0: k host threads build them while the device steps;
+     * submit only checks and reserves capacity, the request joins at a later
+     * ne2b_server_step, and the caller's net arrays and input matrix must
+     * stay valid until its result is taken.  A request that fails to build
+     * is reported finished; ne2b_server_take_result returns its error. */
+    uint32_t admission_threads;
 } ne2b_server_config;
 ne2b_status ne2b_server_create(const ne2b_server_config *cfg, int device, ne2b_server **out);
 ne2b_status ne2b_server_destroy(ne2b_server *s);
@@ -236,9 +243,16 @@ ne2b_status ne2b_server_step(ne2b_server *s, uint32_t *active, uint32_t *finishe
 ne2b_status ne2b_server_result_shape(ne2b_server *s, uint64_t request_id, uint32_t *n, uint32_t *windows);
 ne2b_status ne2b_server_take_result(ne2b_server *s, uint64_t request_id, uint16_t *counts,
                                     uint64_t *spikes_total);
+/* Ids of finished requests whose results are ready (taking them does not
+ * wait for the device); *count is the number ready, ids[0..min(cap,count))
+ * are filled.  A request retired by a launch still in flight appears once
+ * that launch completes. */
 ne2b_status ne2b_server_finished_ids(ne2b_server *s, uint64_t *ids, uint32_t cap, uint32_t *count);
 ne2b_status ne2b_server_stats(ne2b_server *s, uint64_t *admitted, uint64_t *retired, uint32_t *active,
                               uint64_t *neurons_used, uint64_t *synapses_used);
+/* Wait for every launch queued so far (no counterpart in the reference:
+ * the serving loop is new). */
+ne2b_status ne2b_server_synchronize(ne2b_server *s);
 ne2b_status ne2b_server_stream(ne2b_server *s, void **stream);
 ne2b_status ne2b_server_kernel_launches(ne2b_server *s, uint64_t *launches);
 

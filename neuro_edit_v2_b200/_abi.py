@@ -78,6 +78,7 @@ class ServerConfig(C.Structure):
         ("max_requests", C.c_uint32),
         ("steps_per_launch", C.c_uint32),
         ("int_weights", C.c_int32),
+        ("admission_threads", C.c_uint32),
     ]
 
 
@@ -155,6 +156,7 @@ _SIGS = {
     "ne2b_batch_stream": (C.c_int, [_p, C.POINTER(_p)]),
     "ne2b_batch_kernel_launches": (C.c_int, [_p, _pu64]),
     "ne2b_server_stream": (C.c_int, [_p, C.POINTER(_p)]),
+    "ne2b_server_synchronize": (C.c_int, [_p]),
     "ne2b_server_kernel_launches": (C.c_int, [_p, _pu64]),
     "ne2b_set_v_watch": (C.c_int, [_p, _p, _u32]),
     "ne2b_set_grid_watches": (C.c_int, [_p, _p, _p, _u32]),

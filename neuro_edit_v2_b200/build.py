@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libne2b.so")
 SOURCES = ["ne2b_kernels.cu", "ne2b_engine.cu", "ne2b_capi.cu", "ne2b_noalloc.cu", "ne2b_host.cpp"]
-HEADERS = ["ne2b_device.cuh", "ne2b_layout.h", "ne2b_kernels.h", "ne2b_engine.h", "ne2b_handles.h"]
+HEADERS = ["ne2b_device.cuh", "ne2b_layout.h", "ne2b_kernels.h", "ne2b_engine.h", "ne2b_handles.h", "ne2b_parallel.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -5,11 +5,13 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <new>
 #include <vector>
 
 #include "ne2b_engine.h"
+#include "ne2b_parallel.h"
 
 using ne2b::Engine;
 using ne2b::NetHost;
@@ -488,13 +490,64 @@ ne2b_status ne2b_request_footprint(const ne2b_net_desc *net, const ne2b_config *
                                    uint64_t *synapses, uint64_t *ring_words) {
     if (!net || !cfg) return set_error(NE2B_EINVAL, "null argument");
     const uint64_t np = (net->n + ne2b::kNeuronAlign - 1) / ne2b::kNeuronAlign * ne2b::kNeuronAlign;
-    uint32_t maxd = 1;
-    for (uint64_t j = 0; j < net->n_syn; ++j) maxd = std::max<uint32_t>(maxd, net->delay_steps[j]);
-    const uint64_t D = std::max<uint32_t>(2, maxd + 1);
+    std::atomic<uint32_t> maxd{1};
+    if (net->n_syn && !net->delay_steps) return set_error(NE2B_EINVAL, "net has synapses but no delays");
+    ne2b::parallel_for(net->n_syn, [&](uint64_t lo, uint64_t hi) {
+        uint16_t m = 1;
+        for (uint64_t j = lo; j < hi; ++j) m = std::max(m, net->delay_steps[j]);
+        uint32_t cur = maxd.load();
+        while (m > cur && !maxd.compare_exchange_weak(cur, m)) {
+        }
+    });
+    const uint64_t D = std::max<uint32_t>(2, maxd.load() + 1);
     if (neurons) *neurons = np;
     if (synapses) *synapses = net->n_syn;
     if (ring_words) *ring_words = D * np;
     return NE2B_OK;
+}
+
+// Admission thread: builds queued requests on its own stream (validation,
+// parameter rows, CSR staging, uploads, initial state) and hands them to
+// ne2b_server_step, which attaches them on the engine's stream.
+static void server_builder(ne2b_server *s, ne2b_server::Builder *b) {
+    cudaSetDevice(s->eng.device());
+    for (;;) {
+        ne2b_server::Job j;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_job.wait(lk, [&] { return s->stop || !s->jobs.empty(); });
+            if (s->stop) return;
+            j = s->jobs.front();
+            s->jobs.pop_front();
+        }
+        ne2b_server::Built r;
+        r.id = j.id;
+        try {
+            r.st = s->eng.build_net(&j.desc, &j.cfg, j.inputs, j.steps, b->sg, &r.h);
+        } catch (const std::bad_alloc &) {
+            r.st = set_error(NE2B_ENOMEM, "host allocation failed");
+        } catch (...) {
+            r.st = set_error(NE2B_ECUDA, "unexpected host exception while building a request");
+        }
+        if (r.st == NE2B_OK) {
+            cudaError_t e = cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventRecord(r.ev, b->st);
+            if (e != cudaSuccess) {
+                r.st = ne2b::cuda_error(e, "build event");
+                if (r.ev) cudaEventDestroy(r.ev);
+                r.ev = nullptr;
+                cudaStreamSynchronize(b->st);
+                s->eng.discard_net(r.h, b->st);
+                r.h = nullptr;
+            }
+        }
+        if (r.st != NE2B_OK) r.msg = ne2b::last_error_str();
+        {
+            std::lock_guard<std::mutex> g(s->mu);
+            s->built.push_back(std::move(r));
+        }
+        s->cv_built.notify_all();
+    }
 }
 
 ne2b_status ne2b_server_create(const ne2b_server_config *cfg, int device, ne2b_server **out) {
@@ -516,6 +569,18 @@ ne2b_status ne2b_server_create(const ne2b_server_config *cfg, int device, ne2b_s
         }
         s->eng.graph_steps = s->cfg.steps_per_launch;
         s->eng.fixed_grid = true;
+        for (uint32_t k = 0; k < std::min<uint32_t>(cfg->admission_threads, 16u); ++k) {
+            auto b = std::make_unique<ne2b_server::Builder>();
+            st = ne2b::cuda_error(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "admission stream");
+            if (st != NE2B_OK) {
+                delete s;
+                return st;
+            }
+            b->sg.set_stream(b->st);
+            ne2b_server::Builder *bp = b.get();
+            s->builders.push_back(std::move(b));
+            bp->th = std::thread(server_builder, s, bp);
+        }
         *out = s;
         return NE2B_OK;
     })());
@@ -547,8 +612,12 @@ ne2b_status ne2b_server_submit(ne2b_server *s, const ne2b_net_desc *net, const n
         ne2b_config cfg = *cfg_in;
         cfg.max_windows = (uint32_t)((steps + cfg.window_steps - 1) / cfg.window_steps);
         ne2b_server::Req r;
-        ne2b_status st2 = s->eng.add_net(net, &cfg, inputs, steps, &r.slot);
-        if (st2 != NE2B_OK) return st2;
+        if (!s->builders.empty()) {
+            r.queued = true;
+        } else {
+            ne2b_status st2 = s->eng.add_net(net, &cfg, inputs, steps, &r.slot);
+            if (st2 != NE2B_OK) return st2;
+        }
         r.n = net->n;
         r.n_pad = (uint32_t)fn;
         r.windows = (uint32_t)(steps / cfg.window_steps);
@@ -562,14 +631,83 @@ ne2b_status ne2b_server_submit(ne2b_server *s, const ne2b_net_desc *net, const n
         const uint64_t id = s->next_id++;
         s->reqs.emplace(id, std::move(r));
         s->admitted++;
+        if (!s->builders.empty()) {
+            {
+                std::lock_guard<std::mutex> g(s->mu);
+                s->jobs.push_back(ne2b_server::Job{id, *net, cfg, inputs, steps});
+            }
+            s->cv_job.notify_one();
+        }
         *request_id = id;
         return NE2B_OK;
     })());
 }
 
+// Attach the requests the admission threads have built: the engine's
+// stream waits for each build's stream work, then the net is published.  A
+// failed build finishes its request with the error.  When nothing runs on
+// the device yet, waits for the first build instead of stepping an empty
+// engine.
+static ne2b_status server_attach_built(ne2b_server *s) {
+    if (s->builders.empty()) return NE2B_OK;
+    std::vector<ne2b_server::Built> got;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        bool queued = false;
+        for (auto &kv : s->reqs) queued |= kv.second.queued;
+        if (queued && s->built.empty() && s->eng.active_nets() == 0)
+            s->cv_built.wait(lk, [&] { return !s->built.empty(); });
+        got.swap(s->built);
+    }
+    bool attached = false;
+    ne2b_status first_err = NE2B_OK;
+    for (ne2b_server::Built &r : got) {
+        auto it = s->reqs.find(r.id);
+        ne2b_status st = r.st;
+        std::string msg = r.msg;
+        if (st == NE2B_OK && it != s->reqs.end()) {
+            st = ne2b::cuda_error(cudaStreamWaitEvent(s->eng.stream(), r.ev, 0), "admission wait");
+            if (st == NE2B_OK) st = s->eng.attach_net(r.h, &it->second.slot, false);
+            if (st != NE2B_OK) {
+                msg = ne2b::last_error_str();
+                s->eng.discard_net(r.h, s->eng.stream());
+            }
+            r.h = nullptr;
+        } else if (r.h) {
+            s->eng.discard_net(r.h, s->eng.stream());
+            r.h = nullptr;
+        }
+        if (r.ev) cudaEventDestroy(r.ev);
+        if (it == s->reqs.end()) continue;
+        ne2b_server::Req &q = it->second;
+        q.queued = false;
+        if (st == NE2B_OK) {
+            attached = true;
+            continue;
+        }
+        if (st == NE2B_ECUDA && first_err == NE2B_OK) first_err = st;
+        q.done = true;
+        q.fail = st;
+        q.fail_msg = msg;
+        s->used_neurons -= q.fp_neurons;
+        s->used_syn -= q.fp_syn;
+        s->used_ring -= q.fp_ring;
+        s->retired++;
+        s->finished.push_back(r.id);
+    }
+    if (attached) {
+        ne2b_status st = s->eng.rebuild_tiles();
+        if (st != NE2B_OK) return st;
+    }
+    if (first_err != NE2B_OK) return set_error(first_err, "admission: %s", ne2b::last_error_str());
+    return NE2B_OK;
+}
+
 ne2b_status ne2b_server_step(ne2b_server *s, uint32_t *active_out, uint32_t *finished_out) {
     if (!s) return set_error(NE2B_EINVAL, "null server handle");
     GUARD(([&]() -> ne2b_status {
+        ne2b_status sa = server_attach_built(s);
+        if (sa != NE2B_OK) return sa;
         // at most two launch groups in flight: host admission and retirement
         // work overlaps the device without queueing unboundedly ahead of it
         cudaEvent_t &ev = s->step_ev[s->step_no & 1];
@@ -586,6 +724,10 @@ ne2b_status ne2b_server_step(ne2b_server *s, uint32_t *active_out, uint32_t *fin
         for (auto &kv : s->reqs) {
             ne2b_server::Req &r = kv.second;
             if (r.done) continue;
+            if (r.queued) {
+                ++act;
+                continue;
+            }
             NetHost *h = s->eng.net(r.slot);
             if (!(h && h->t >= h->t_end)) {
                 ++act;
@@ -637,6 +779,13 @@ ne2b_status ne2b_server_take_result(ne2b_server *s, uint64_t id, uint16_t *count
     if (it == s->reqs.end()) return set_error(NE2B_EINVAL, "unknown request %llu", (unsigned long long)id);
     ne2b_server::Req &r = it->second;
     if (!r.done) return set_error(NE2B_ENODATA, "request %llu is still running", (unsigned long long)id);
+    if (r.fail != NE2B_OK) {
+        const ne2b_status st = set_error(r.fail, "request %llu was not admitted: %s", (unsigned long long)id,
+                                         r.fail_msg.c_str());
+        s->reqs.erase(it);
+        s->finished.erase(std::remove(s->finished.begin(), s->finished.end(), id), s->finished.end());
+        return st;
+    }
     GUARD(([&]() -> ne2b_status {
         // the copies wait only for this request's retirement, not for the
         // launches queued after it
@@ -664,10 +813,21 @@ ne2b_status ne2b_server_take_result(ne2b_server *s, uint64_t id, uint16_t *count
     })());
 }
 
+// Finished requests whose results can be taken without waiting: the
+// device has completed the launch that retired them (or they failed to
+// build).  Requests retired by launches still in flight are listed once
+// those launches complete.
 ne2b_status ne2b_server_finished_ids(ne2b_server *s, uint64_t *ids, uint32_t cap, uint32_t *count) {
     if (!s || !count) return set_error(NE2B_EINVAL, "null argument");
-    const uint32_t c = (uint32_t)s->finished.size();
-    for (uint32_t k = 0; k < c && k < cap && ids; ++k) ids[k] = s->finished[k];
+    uint32_t c = 0;
+    for (uint64_t id : s->finished) {
+        auto it = s->reqs.find(id);
+        if (it == s->reqs.end()) continue;
+        const ne2b_server::Req &r = it->second;
+        if (r.ev && cudaEventQuery(r.ev) != cudaSuccess) continue;
+        if (ids && c < cap) ids[c] = id;
+        ++c;
+    }
     *count = c;
     return NE2B_OK;
 }
@@ -683,6 +843,11 @@ ne2b_status ne2b_server_stats(ne2b_server *s, uint64_t *admitted, uint64_t *reti
     if (neurons_used) *neurons_used = s->used_neurons;
     if (synapses_used) *synapses_used = s->used_syn;
     return NE2B_OK;
+}
+
+ne2b_status ne2b_server_synchronize(ne2b_server *s) {
+    if (!s) return set_error(NE2B_EINVAL, "null server handle");
+    GUARD(s->eng.sync());
 }
 
 ne2b_status ne2b_server_stream(ne2b_server *s, void **stream) {

@@ -15,27 +15,9 @@
 #include <thread>
 
 #include "ne2b_kernels.h"
+#include "ne2b_parallel.h"
 
 namespace ne2b {
-
-// Split [0, n) over up to 8 host threads when n is large (synapse-sized
-// loops of admission); small ranges run inline.
-template <class F>
-static void parallel_for(uint64_t n, F f) {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const unsigned T = std::min(8u, hw ? hw : 1u);
-    if (n < (1u << 20) || T <= 1) {
-        f((uint64_t)0, n);
-        return;
-    }
-    std::vector<std::thread> th;
-    const uint64_t chunk = (n + T - 1) / T;
-    for (unsigned k = 0; k < T; ++k) {
-        const uint64_t lo = k * chunk, hi = std::min(n, lo + chunk);
-        if (lo < hi) th.emplace_back(f, lo, hi);
-    }
-    for (auto &x : th) x.join();
-}
 
 static thread_local std::string g_err;
 
@@ -108,10 +90,6 @@ Engine::~Engine() {
     }
     if (stream_) cudaStreamSynchronize(stream_);
     if (stage_) cudaFreeHost(stage_);
-    for (PinnedBlock &b : pin_) {
-        cudaFreeHost(b.p);
-        cudaEventDestroy(b.ev);
-    }
     cudaFree(d_nets_);
     cudaFree(d_counters_);
     cudaFree(d_ptab_);
@@ -141,6 +119,7 @@ ne2b_status Engine::init(int device, bool int_ring, uint32_t max_nets) {
                          prop.major, prop.minor);
     sm_count_ = prop.multiProcessorCount;
     NE2B_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    stager_.set_stream(stream_);
     {
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -182,7 +161,7 @@ ne2b_status Engine::upload_eng() {
     e.counters = d_counters_;
     e.block_tiles = d_block_tiles_;
     e.block_neurons = res_neurons_;
-    e.pad0 = 0;
+    e.n_params = ptab_rows_dev_;
     e.barrier = d_barrier_;
     e.err = d_err_;
     // pageable source: the runtime copies it to staging before returning, so
@@ -240,6 +219,10 @@ ne2b_status Engine::upload_ptab() {
     NE2B_CUDA(cudaMemcpyAsync(d_ptab_, h_ptab_.data(), sizeof(ParamRow) * h_ptab_.size(), cudaMemcpyHostToDevice,
                               stream_));
     ptab_dirty_ = false;
+    if (ptab_rows_dev_ != (uint32_t)h_ptab_.size()) {
+        ptab_rows_dev_ = (uint32_t)h_ptab_.size();
+        NE2B_TRY(upload_eng());
+    }
     return NE2B_OK;
 }
 
@@ -255,65 +238,65 @@ static void fill_noise(NetDev &d, const ne2b_config &c) {
     d.gauss_k = c.gauss_sd != 0.0f ? (float)((double)c.gauss_sd * 1.7320508075688772 / 65536.0) : 0.0f;
 }
 
-// Host-to-device copy through a pool of pinned staging blocks: the source
-// is copied into pinned memory and the DMA is issued asynchronously, so a
-// large upload never waits for the kernels in flight.  Small copies go
-// straight from pageable memory (the runtime stages them on the call).
-// Blocks used since the last pin_close stay "open": they are never handed
-// out again until pin_close has recorded, after every copy from them was
-// enqueued, the event that marks them reusable.
-ne2b_status Engine::pin_reserve(size_t bytes, void **host) {
-    const size_t need = (bytes + 255) / 256 * 256;
-    if (pin_cur_ >= 0 && pin_[pin_cur_].used + need > pin_[pin_cur_].cap) {
-        pin_open_.push_back(pin_cur_);
-        pin_cur_ = -1;
+Stager::~Stager() {
+    for (PinnedBlock &b : pin_) {
+        cudaFreeHost(b.p);
+        cudaEventDestroy(b.ev);
     }
-    if (pin_cur_ < 0) {
+}
+
+ne2b_status Stager::reserve(size_t bytes, void **host) {
+    const size_t need = (bytes + 255) / 256 * 256;
+    if (cur_ >= 0 && pin_[cur_].used + need > pin_[cur_].cap) {
+        open_.push_back(cur_);
+        cur_ = -1;
+    }
+    if (cur_ < 0) {
         for (size_t k = 0; k < pin_.size(); ++k) {
-            if (std::find(pin_open_.begin(), pin_open_.end(), (int)k) != pin_open_.end()) continue;
+            if (std::find(open_.begin(), open_.end(), (int)k) != open_.end()) continue;
             if (pin_[k].cap >= need && cudaEventQuery(pin_[k].ev) == cudaSuccess) {
-                pin_cur_ = (int)k;
+                cur_ = (int)k;
                 break;
             }
         }
-        if (pin_cur_ < 0) {
+        if (cur_ < 0) {
             PinnedBlock b;
             b.cap = std::max<size_t>(need, (size_t)64 << 20);
             NE2B_CUDA(cudaMallocHost(&b.p, b.cap));
             NE2B_CUDA(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming));
             pin_.push_back(b);
-            pin_cur_ = (int)pin_.size() - 1;
+            cur_ = (int)pin_.size() - 1;
         }
-        pin_[pin_cur_].used = 0;
+        pin_[cur_].used = 0;
     }
-    PinnedBlock &b = pin_[pin_cur_];
+    PinnedBlock &b = pin_[cur_];
     *host = (uint8_t *)b.p + b.used;
     b.used += need;
     return NE2B_OK;
 }
 
-ne2b_status Engine::pin_issue(void *dst, const void *host, size_t bytes) {
-    NE2B_CUDA(cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, stream_));
+ne2b_status Stager::issue(void *dst, const void *host, size_t bytes) {
+    NE2B_CUDA(cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, st_));
     return NE2B_OK;
 }
 
-ne2b_status Engine::pin_copy(void *dst, const void *src, size_t bytes) {
+ne2b_status Stager::copy(void *dst, const void *src, size_t bytes) {
     if (!bytes) return NE2B_OK;
     if (bytes <= (64u << 10)) {
-        NE2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
+        NE2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st_));
         return NE2B_OK;
     }
     void *stage = nullptr;
-    NE2B_TRY(pin_reserve(bytes, &stage));
+    NE2B_TRY(reserve(bytes, &stage));
     parallel_for(bytes, [&](uint64_t lo, uint64_t hi) { memcpy((uint8_t *)stage + lo, (const uint8_t *)src + lo, hi - lo); });
-    return pin_issue(dst, stage, bytes);
+    return issue(dst, stage, bytes);
 }
 
-ne2b_status Engine::pin_close() {
-    if (pin_cur_ >= 0) pin_open_.push_back(pin_cur_);
-    for (int k : pin_open_) NE2B_CUDA(cudaEventRecord(pin_[k].ev, stream_));
-    pin_open_.clear();
-    pin_cur_ = -1;
+ne2b_status Stager::close() {
+    if (cur_ >= 0) open_.push_back(cur_);
+    for (int k : open_) NE2B_CUDA(cudaEventRecord(pin_[k].ev, st_));
+    open_.clear();
+    cur_ = -1;
     return NE2B_OK;
 }
 
@@ -323,7 +306,47 @@ static double now_ms() {
 
 ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
                             uint32_t *slot_out, bool rebuild) {
+    NetHost *h = nullptr;
+    NE2B_TRY(build_net(net, cfg, inputs, steps, stager_, &h));
+    const ne2b_status st = attach_net(h, slot_out, rebuild);
+    if (st != NE2B_OK) discard_net(h, stream_);
+    return st;
+}
+
+void Engine::discard_net(NetHost *h, cudaStream_t st) {
+    if (!h) return;
+    for (void *p : h->allocs) cudaFreeAsync(p, st);
+    delete h;
+}
+
+ne2b_status Engine::attach_net(NetHost *h, uint32_t *slot_out, bool rebuild) {
+    uint32_t slot = nets_cap_;
+    for (uint32_t j = 0; j < nets_cap_; ++j)
+        if (!nets_[j]) {
+            slot = j;
+            break;
+        }
+    if (slot == nets_cap_) return set_error(NE2B_EFULL, "all %u net slots are in use", nets_cap_);
+    {
+        std::lock_guard<std::mutex> g(ptab_mu_);
+        NE2B_TRY(upload_ptab());
+    }
+    NE2B_CUDA(cudaMemsetAsync(d_counters_ + slot, 0, sizeof(NetCounters), stream_));
+    h->slot = slot;
+    nets_[slot] = h;
+    launches_ += h->build_launches;
+    h->build_launches = 0;
+    NE2B_TRY(upload_net(*h));
+    if (rebuild) NE2B_TRY(rebuild_tiles());
+    *slot_out = slot;
+    return NE2B_OK;
+}
+
+ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
+                              Stager &sg, NetHost **out) {
+    *out = nullptr;
     if (!net || !cfg) return set_error(NE2B_EINVAL, "add_net: null net or config");
+    const cudaStream_t bst = sg.stream();
     const bool dbg = getenv("NE2B_DEBUG") != nullptr;
     double tp[8] = {now_ms()};
     const uint32_t n = net->n;
@@ -382,14 +405,8 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     if (inputs && net->n_inputs == 0) inputs = nullptr;
     tp[1] = now_ms();
 
-    uint32_t slot = nets_cap_;
-    for (uint32_t j = 0; j < nets_cap_; ++j)
-        if (!nets_[j]) { slot = j; break; }
-    if (slot == nets_cap_) return set_error(NE2B_EFULL, "all %u net slots are in use", nets_cap_);
-
     NetHost *h = new NetHost();
     h->cfg = *cfg;
-    h->slot = slot;
     h->n = n;
     h->n_pad = (n + kNeuronAlign - 1) / kNeuronAlign * kNeuronAlign;
     h->D = maxd + 1 < 2 ? 2 : maxd + 1;  // state.rs:221-224
@@ -406,19 +423,20 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     auto alloc = [&](void **p, size_t bytes) -> ne2b_status {
         *p = nullptr;
         if (bytes == 0) return NE2B_OK;
-        cudaError_t e = cudaMallocAsync(p, bytes, stream_);
+        cudaError_t e = cudaMallocAsync(p, bytes, bst);
         if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync (net arrays)");
         h->allocs.push_back(*p);
         h->dev_bytes += bytes;
         return NE2B_OK;
     };
     auto fail = [&](ne2b_status st) {
-        for (void *p : h->allocs) cudaFreeAsync(p, stream_);
-        cudaStreamSynchronize(stream_);
+        for (void *p : h->allocs) cudaFreeAsync(p, bst);
+        sg.close();
+        cudaStreamSynchronize(bst);
         delete h;
         return st;
     };
-    auto up = [&](void *dst, const void *src, size_t bytes) -> ne2b_status { return pin_copy(dst, src, bytes); };
+    auto up = [&](void *dst, const void *src, size_t bytes) -> ne2b_status { return sg.copy(dst, src, bytes); };
 #define NET_TRY(x)                          \
     do {                                    \
         ne2b_status _s = (x);               \
@@ -449,9 +467,12 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     // host-side rows: params -> dictionary, x0
     std::vector<uint16_t> pidx(np, 0);
     std::vector<float> v0(np, 0.0f), u0(np, 0.0f);
+    bool any_adex = false;
+    std::unique_lock<std::mutex> ptab_lock(ptab_mu_);
     for (uint32_t i = 0; i < n; ++i) {
         const float *row = net->params + (size_t)i * net->param_stride;
         const uint32_t m = net->model[i];
+        any_adex |= m == NE2B_MODEL_ADEX;
         const uint32_t width = std::min<uint32_t>(net->param_stride, 10);
         NET_TRY(param_index(m, row, width, &pidx[i]));
         if (net->x0) {
@@ -465,12 +486,12 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
             u0[i] = row[1] * v0[i];
         }
     }
-    NET_TRY(upload_ptab());
+    ptab_lock.unlock();  // the rows reach the device when the net is attached
     tp[3] = now_ms();
     NET_TRY(up((void *)d.pidx, pidx.data(), sizeof(uint16_t) * np));
     NET_TRY(up((void *)d.v0, v0.data(), sizeof(float) * np));
     NET_TRY(up((void *)d.u0, u0.data(), sizeof(float) * np));
-    NET_TRY(cuda_error(cudaMemsetAsync(d.ext, 0, sizeof(float) * np, stream_), "memset ext"));
+    NET_TRY(cuda_error(cudaMemsetAsync(d.ext, 0, sizeof(float) * np, bst), "memset ext"));
     NET_TRY(up((void *)d.rowptr, net->src_ptr, sizeof(uint32_t) * ((size_t)n + 1)));
     if (h->e) {
         // one parallel pass over the synapses into pinned staging: targets
@@ -479,9 +500,9 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
         uint32_t *tg = nullptr;
         void *wst = nullptr;
         void *dst8 = nullptr;
-        NET_TRY(pin_reserve(4 * h->e, (void **)&tg));
-        NET_TRY(pin_reserve(4 * h->e, &wst));
-        NET_TRY(pin_reserve((d16 ? 2 : 1) * h->e, &dst8));
+        NET_TRY(sg.reserve(4 * h->e, (void **)&tg));
+        NET_TRY(sg.reserve(4 * h->e, &wst));
+        NET_TRY(sg.reserve((d16 ? 2 : 1) * h->e, &dst8));
         const bool iq = int_ring_;
         parallel_for(h->e, [&](uint64_t lo, uint64_t hi) {
             memcpy(tg + lo, net->tgt + lo, 4 * (hi - lo));
@@ -498,9 +519,9 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
                 for (uint64_t j = lo; j < hi; ++j) d8[j] = (uint8_t)net->delay_steps[j];
             }
         });
-        NET_TRY(pin_issue((void *)d.tgt, tg, 4 * h->e));
-        NET_TRY(pin_issue((void *)d.w, wst, 4 * h->e));
-        NET_TRY(pin_issue((void *)d.delay, dst8, (d16 ? 2 : 1) * h->e));
+        NET_TRY(sg.issue((void *)d.tgt, tg, 4 * h->e));
+        NET_TRY(sg.issue((void *)d.w, wst, 4 * h->e));
+        NET_TRY(sg.issue((void *)d.delay, dst8, (d16 ? 2 : 1) * h->e));
     }
     tp[4] = now_ms();
     // stimulus routing
@@ -571,20 +592,26 @@ ne2b_status Engine::add_net(const ne2b_net_desc *net, const ne2b_config *cfg, co
     }
     fill_noise(d, *cfg);
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
-              (cfg->window_steps ? kNetWindows : 0u);
-    nets_[slot] = h;
-    NET_TRY(pin_close());
+              (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u);
     tp[5] = now_ms();
-    NET_TRY(reset_net(slot));
+    // initial state (cpu.rs:158-183), on the build stream
+    NET_TRY(cuda_error(launch_reset_neurons(d, bst), "reset kernel"));
+    h->build_launches += np ? 1 : 0;
+    NET_TRY(cuda_error(cudaMemsetAsync(d.ring, 0, sizeof(uint32_t) * (size_t)h->D * np, bst), "memset ring"));
+    if (d.rec_bits)
+        NET_TRY(cuda_error(cudaMemsetAsync(d.rec_bits, 0, sizeof(uint32_t) * (size_t)rec_rows * (np / 32), bst),
+                           "memset record"));
+    if (d.win_out)
+        NET_TRY(cuda_error(cudaMemsetAsync(d.win_out, 0, sizeof(uint16_t) * (size_t)d.max_windows * np, bst),
+                           "memset windows"));
+    NET_TRY(sg.close());
     tp[6] = now_ms();
-    if (rebuild) NET_TRY(rebuild_tiles());
-    tp[7] = now_ms();
     if (dbg)
-        fprintf(stderr, "ne2b add_net n=%u e=%llu: validate %.3f alloc %.3f params %.3f csr %.3f rest %.3f reset %.3f tiles %.3f ms\n",
+        fprintf(stderr, "ne2b build_net n=%u e=%llu: validate %.3f alloc %.3f params %.3f csr %.3f rest %.3f reset %.3f ms\n",
                 n, (unsigned long long)h->e, tp[1] - tp[0], tp[2] - tp[1], tp[3] - tp[2], tp[4] - tp[3], tp[5] - tp[4],
-                tp[6] - tp[5], tp[7] - tp[6]);
+                tp[6] - tp[5]);
 #undef NET_TRY
-    *slot_out = slot;
+    *out = h;
     return NE2B_OK;
 }
 
@@ -625,7 +652,7 @@ uint64_t Engine::dev_bytes() const {
 
 uint32_t Engine::grid() const {
     uint32_t bps = shape_.blocks_per_sm;
-    const int occ = step_occupancy(int_ring_, shape_.block, shape_.npt);
+    const int occ = step_occupancy(int_ring_, adex_, shape_.block, shape_.npt);
     if (bps == 0 || (int)bps > occ) bps = (uint32_t)(occ > 0 ? occ : 1);
     uint32_t g = (uint32_t)sm_count_ * bps;
     if (fixed_grid) return g;  // serving: graphs stay valid as nets come and go
@@ -668,7 +695,7 @@ bool Engine::plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &bloc
         uint64_t m = 0;
         for (uint64_t x : sum) m = std::max(m, x);
         const size_t smem = head + 16 * (size_t)((m + 3) / 4 * 4);
-        const int occ = smem > 227 * 1024 ? 0 : resident_occupancy(int_ring_, shape_.block, shape_.npt, smem);
+        const int occ = smem > 227 * 1024 ? 0 : resident_occupancy(int_ring_, adex_, shape_.block, shape_.npt, smem);
         const uint32_t blocks = (uint32_t)bt.size() - 1;
         if (getenv("NE2B_DEBUG"))
             fprintf(stderr, "ne2b plan: block %u npt %u bps %u -> %u blocks, %llu neurons/block, smem %zu, occ %d\n",
@@ -694,6 +721,13 @@ bool Engine::plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &bloc
 ne2b_status Engine::rebuild_tiles() {
     const uint32_t tile = shape_.block * shape_.npt;
     std::vector<Tile> tiles;
+    bool adex = false;
+    for (NetHost *h : nets_)
+        if (h) adex |= (h->dev.flags & kNetHasAdex) != 0u;
+    if (adex != adex_) {
+        adex_ = adex;
+        clear_graphs();
+    }
     for (NetHost *h : nets_) {
         if (!h) continue;
         for (uint32_t start = 0; start < h->n_pad; start += tile) {
@@ -882,7 +916,7 @@ ne2b_status Engine::launch_group(uint32_t steps) {
     if (n_tiles_ == 0 || steps == 0) return NE2B_OK;
     if (resident_) {
         NE2B_CUDA(cudaMemsetAsync(d_barrier_, 0, sizeof(unsigned int), stream_));
-        NE2B_CUDA(launch_resident(int_ring_, shape_.block, shape_.npt, d_eng_, 0, steps, res_grid_, res_smem_, stream_));
+        NE2B_CUDA(launch_resident(int_ring_, adex_, shape_.block, shape_.npt, d_eng_, 0, steps, res_grid_, res_smem_, stream_));
         NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
         launches_ += 2;
         return NE2B_OK;
@@ -895,7 +929,7 @@ ne2b_status Engine::launch_group(uint32_t steps) {
             NE2B_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
             cudaError_t err = cudaSuccess;
             for (uint32_t k = 0; k < steps && err == cudaSuccess; ++k)
-                err = launch_step(int_ring_, shape_.block, shape_.npt, d_eng_, k, g, stream_);
+                err = launch_step(int_ring_, adex_, shape_.block, shape_.npt, d_eng_, k, g, stream_);
             if (err == cudaSuccess) err = launch_advance(d_nets_, nets_cap_, steps, stream_);
             cudaError_t e2 = cudaStreamEndCapture(stream_, &gr);
             if (err != cudaSuccess) return cuda_error(err, "step launch during capture");
@@ -910,7 +944,7 @@ ne2b_status Engine::launch_group(uint32_t steps) {
         launches_ += steps + 1;
         return NE2B_OK;
     }
-    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, shape_.block, shape_.npt, d_eng_, k, g, stream_));
+    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, adex_, shape_.block, shape_.npt, d_eng_, k, g, stream_));
     NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
     launches_ += steps + 1;
     return NE2B_OK;
@@ -1119,8 +1153,9 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
     int best_mode = mode_ == kModeAuto ? (resident_ ? kModeResident : kModeStream) : mode_;
     float best_ms = 1e30f;
     for (int m : {(int)kModeStream, (int)kModeResident}) {
+        if (saved_mode != kModeAuto && m != saved_mode) continue;  // a forced kernel keeps its mode
         for (uint32_t c = 0; c < count; ++c) {
-            const int occ = step_occupancy(int_ring_, blocks[c], npts[c]);
+            const int occ = step_occupancy(int_ring_, adex_, blocks[c], npts[c]);
             for (int half = 0; half < 2; ++half) {
                 if (half && (m == kModeResident || occ < 2)) continue;
                 TileShape s;
@@ -1154,10 +1189,6 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
         }
     }
     mode_ = saved_mode == kModeAuto ? best_mode : saved_mode;
-    if (saved_mode != kModeAuto && best_mode != saved_mode) {
-        // a forced kernel keeps its mode; take its best shape instead
-        mode_ = saved_mode;
-    }
     shape_ = best;
     clear_graphs();
     NE2B_TRY(rebuild_tiles());

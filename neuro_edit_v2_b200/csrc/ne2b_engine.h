@@ -11,6 +11,7 @@
 
 #include <array>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -49,6 +50,7 @@ struct NetHost {
     std::vector<uint32_t> stim_ptr_host;  // for tile flags
     std::vector<void *> allocs;
     std::vector<float> pack_buf;
+    uint64_t build_launches = 0;  // kernels queued by build_net
 };
 
 enum KernelMode { kModeAuto = 0, kModeStream = 1, kModeResident = 2 };
@@ -75,6 +77,33 @@ struct PinnedBlock {
     cudaEvent_t ev = nullptr;
 };
 
+// Host-to-device copies on one stream through a pool of pinned staging
+// blocks: the source is copied into pinned memory and the DMA is issued
+// asynchronously, so a large upload never waits for kernels in flight.
+// Blocks used since the last close() stay "open": they are not handed out
+// again until close() has recorded, after every copy from them was enqueued,
+// the event that marks them reusable.  The owner synchronises the stream
+// before destroying a Stager.
+class Stager {
+  public:
+    Stager() = default;
+    Stager(const Stager &) = delete;
+    Stager &operator=(const Stager &) = delete;
+    ~Stager();
+    void set_stream(cudaStream_t st) { st_ = st; }
+    cudaStream_t stream() const { return st_; }
+    ne2b_status reserve(size_t bytes, void **host);
+    ne2b_status issue(void *dst, const void *host, size_t bytes);
+    ne2b_status copy(void *dst, const void *src, size_t bytes);  // small copies go from pageable memory
+    ne2b_status close();
+
+  private:
+    cudaStream_t st_ = nullptr;
+    std::vector<PinnedBlock> pin_;
+    int cur_ = -1;
+    std::vector<int> open_;
+};
+
 struct TileShape {
     uint32_t block = 256;
     uint32_t npt = 2;
@@ -91,11 +120,20 @@ class Engine {
     // input matrix (serving); NULL = host-packed stimulus program.
     ne2b_status add_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
                         uint32_t *slot, bool rebuild = true);
+    // add_net in two halves.  build_net validates the net and creates its
+    // device arrays (reset to the initial state) with copies and kernels on
+    // `sg`'s stream; it touches no other engine state than the parameter
+    // dictionary (under its lock), so it may run on another host thread
+    // while this engine steps.  attach_net publishes a built net (slot,
+    // descriptor, counters, parameter rows) on the engine's stream, which
+    // must already be ordered after the build's stream work.
+    ne2b_status build_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
+                          Stager &sg, NetHost **out);
+    ne2b_status attach_net(NetHost *h, uint32_t *slot, bool rebuild = true);
+    void discard_net(NetHost *h, cudaStream_t st);  // a built net that is never attached
     ne2b_status remove_net(uint32_t slot, bool rebuild = true, const void *keep = nullptr);
-    ne2b_status pin_copy(void *dst, const void *src, size_t bytes);
-    ne2b_status pin_reserve(size_t bytes, void **host);
-    ne2b_status pin_issue(void *dst, const void *host, size_t bytes);
-    ne2b_status pin_close();
+    ne2b_status pin_copy(void *dst, const void *src, size_t bytes) { return stager_.copy(dst, src, bytes); }
+    ne2b_status pin_close() { return stager_.close(); }
     ne2b_status run_steps(uint64_t steps);
     ne2b_status reset_net(uint32_t slot);
     ne2b_status sync();
@@ -163,6 +201,7 @@ class Engine {
     ParamRow *d_ptab_ = nullptr;
     uint32_t ptab_cap_ = 0;
     bool ptab_dirty_ = false;
+    uint32_t ptab_rows_dev_ = 0;  // rows copied to the device (EngineDev::n_params)
     Tile *d_tiles_ = nullptr;
     uint32_t tiles_cap_ = 0;
     uint32_t n_tiles_ = 0;
@@ -175,6 +214,7 @@ class Engine {
     // resident kernel
     int mode_ = kModeAuto;
     bool resident_ = false;
+    bool adex_ = false;  // some net holds AdEx rows: the kernels with the AdEx path run
     uint32_t *d_block_tiles_ = nullptr;
     uint32_t block_tiles_cap_ = 0;
     uint32_t res_neurons_ = 0;
@@ -182,9 +222,8 @@ class Engine {
     uint32_t res_grid_ = 0;
     unsigned int *d_barrier_ = nullptr;
     unsigned int *d_err_ = nullptr;
-    std::vector<PinnedBlock> pin_;  // pinned staging pool for uploads
-    int pin_cur_ = -1;
-    std::vector<int> pin_open_;  // blocks with copies enqueued since the last pin_close
+    Stager stager_;  // uploads on the engine's own stream
+    std::mutex ptab_mu_;  // the parameter dictionary (builds may run on other threads)
     void *stage_ = nullptr;  // pinned staging for stimulus chunks and descriptors
     size_t stage_bytes_ = 0;
 };

@@ -30,6 +30,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "ne2b_device.cuh"
 #include "ne2b_kernels.h"
 
@@ -41,21 +43,23 @@ struct SmemLists {
     uint32_t *total;  // [1]
 };
 
-template <bool INT, int BLOCK, int NPT, bool RES>
-__device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const Tile &tile, uint32_t k_step,
-                                             float *vs, float *us, float *ss, uint16_t *tks, const uint16_t *pis,
-                                             const SmemLists &sl) {
+// `nd` is the tile's net descriptor (global memory, or a shared-memory copy
+// staged before the launch's dependency wait); `t` is the absolute step and
+// `tmod` = t % D.  ADEX: the net holds AdEx rows (else the Izhikevich path is
+// the only one compiled into this instance).
+// `ptab` is the parameter table (a shared-memory copy when it is small).
+template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX>
+__device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
+                                             const Tile &tile, uint64_t t, uint32_t tmod, float *vs, float *us,
+                                             float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const NetDev &nd = eng->nets[tile.net];
     const uint32_t flags = nd.flags;
     if (!(flags & kNetActive)) return;  // uniform across the block
-    const uint64_t t = nd.t + k_step;
     if (t >= nd.t_end) return;  // uniform across the block
 
     const uint32_t n = nd.n, n_pad = nd.n_pad, D = nd.D;
-    const uint32_t tmod = (nd.tmod + k_step) % D;
     const size_t slot_off = (size_t)tmod * n_pad;
     const float dt = nd.dt, decay_s = nd.decay_s;
     const float pkick = nd.pkick, kick = nd.kick, gauss_k = nd.gauss_k;
@@ -71,7 +75,6 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         win_end = ((t + 1) % nd.win_steps) == 0;
         widx = (uint32_t)((t + 1) / nd.win_steps) - 1u;
     }
-    const ParamRow *__restrict__ ptab = eng->ptab;
 
     uint32_t li[NPT];
     bool valid[NPT];
@@ -117,25 +120,27 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         }
         // pidx bit 15 marks an AdEx row: an Izhikevich neuron reads only the
         // first 16 bytes of its parameter row
-        const bool adex = (pi[q] & kParamAdexBit) != 0u;
+        const bool adex = ADEX && (pi[q] & kParamAdexBit) != 0u;
         const ParamRow &pr = ptab[pi[q] & ~kParamAdexBit];
         float p[10];
         const float4 p0 = *reinterpret_cast<const float4 *>(&pr.p[0]);
         p[0] = p0.x; p[1] = p0.y; p[2] = p0.z; p[3] = p0.w;
-        if (adex) {
+        if (ADEX && adex) {
             const float4 p1 = *reinterpret_cast<const float4 *>(&pr.p[4]);
             const float4 p2 = *reinterpret_cast<const float4 *>(&pr.p[8]);
             p[4] = p1.x; p[5] = p1.y; p[6] = p1.z; p[7] = p1.w;
             p[8] = p2.x; p[9] = p2.y;
         }
-        const float gain = adex ? p[0] : 1.0f;  // model/mod.rs:104-106, adex.rs:189-191
+        const float gain = (ADEX && adex) ? p[0] : 1.0f;  // model/mod.rs:104-106, adex.rs:189-191
         if (pkick > 0.0f || gauss_k != 0.0f) {
             const uint64_t base = noise_base(i, t, seed);
             if (pkick > 0.0f && noise_fires(base, pkick)) I = __fadd_rn(I, __fmul_rn(kick, gain));
             if (gauss_k != 0.0f)
                 I = __fadd_rn(I, __fmul_rn(__int2float_rn(gauss_numer(base)), __fmul_rn(gauss_k, gain)));
         }
-        const bool sp = adex ? adex_step(p, v[q], u[q], I, dt) : izh_step(p, v[q], u[q], I, dt);
+        bool sp;
+        if (ADEX && adex) sp = adex_step(p, v[q], u[q], I, dt);
+        else sp = izh_step(p, v[q], u[q], I, dt);
         // trace: 1 on spike, else one more multiply by decay_t (saturating at
         // the table's last entry, 0 or the subnormal fixed point)
         const uint32_t k0 = tk[q];
@@ -232,28 +237,81 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
 }
 
 // Programmatic dependent launch: let the next kernel of the stream be
-// scheduled now, then wait until the previous one has completed and its
-// memory is visible (griddepcontrol.wait).  Both are no-ops for a kernel
-// launched without the programmatic-serialization attribute.
+// scheduled now (griddepcontrol.launch_dependents), and wait until the
+// previous one has completed and its memory is visible (griddepcontrol.wait).
+// Both are no-ops for a kernel launched without the programmatic-serialization
+// attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_enter() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
+    pdl_trigger();
+    pdl_wait();
+}
+
+// Copy the parameter table into shared memory when it has at most
+// kSmemParamRows rows; returns the table the block reads from.
+template <int BLOCK>
+__device__ __forceinline__ const ParamRow *stage_params(const EngineDev *__restrict__ eng, ParamRow *s_ptab) {
+    const uint32_t np = eng->n_params;
+    if (np > kSmemParamRows) return eng->ptab;
+    constexpr uint32_t kWords = sizeof(ParamRow) / 16;
+    for (uint32_t w = threadIdx.x; w < np * kWords; w += BLOCK)
+        reinterpret_cast<uint4 *>(s_ptab)[w] = reinterpret_cast<const uint4 *>(eng->ptab)[w];
+    return s_ptab;
+}
+
+// Copy net descriptor `net` into shared memory (16-byte words, one per
+// thread).
+__device__ __forceinline__ void stage_net(const EngineDev *__restrict__ eng, uint32_t net, NetDev *s_nd) {
+    constexpr uint32_t kNetWords = sizeof(NetDev) / 16;
+    if (threadIdx.x < kNetWords)
+        reinterpret_cast<uint4 *>(s_nd)[threadIdx.x] = reinterpret_cast<const uint4 *>(eng->nets + net)[threadIdx.x];
 }
 
 // ------------------------------------------------------ streaming kernel
-template <bool INT, int BLOCK, int NPT>
+// The tile list and the net descriptors are written by host copies, which
+// a launch always follows in full, and by advance_kernel (`t`, `tmod`),
+// after which the next step launch is never programmatic (launch_step
+// gives k_step = 0 a plain stream dependency).  So every block reads its
+// first tile and stages the net descriptor, t included, before the
+// dependency wait, overlapping the previous step's tail; after the wait
+// only the step's own data is read.  The descriptor is restaged only when
+// the net changes from one tile to the next.
+template <bool INT, int BLOCK, int NPT, bool ADEX>
 __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
-    pdl_enter();
+    pdl_trigger();
     __shared__ uint32_t s_list[BLOCK * NPT];
     __shared__ uint32_t s_woff[BLOCK / 32];
     __shared__ uint32_t s_total;
+    __shared__ __align__(16) NetDev s_nd;
+    __shared__ __align__(16) ParamRow s_ptab[kSmemParamRows];
+    static_assert(sizeof(NetDev) % 16 == 0 && sizeof(ParamRow) % 16 == 0, "16-byte staging");
+    static_assert(sizeof(NetDev) / 16 <= BLOCK, "one 16-byte word per thread");
     const SmemLists sl{s_list, s_woff, &s_total};
     const uint32_t n_tiles = eng->n_tiles;
-    for (uint32_t tix = blockIdx.x; tix < n_tiles; tix += gridDim.x) {
-        const Tile tile = eng->tiles[tix];
-        const NetDev &nd = eng->nets[tile.net];
-        process_tile<INT, BLOCK, NPT, false>(eng, tile, k_step, nd.v + tile.start, nd.u + tile.start,
-                                             nd.s + tile.start, nd.tk + tile.start, nd.pidx + tile.start, sl);
+    uint32_t tix = blockIdx.x;
+    if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
+    Tile tile = eng->tiles[tix];
+    stage_net(eng, tile.net, &s_nd);
+    const ParamRow *ptab = stage_params<BLOCK>(eng, s_ptab);
+    __syncthreads();
+    pdl_wait();
+    for (;;) {
+        const uint32_t nx = tix + gridDim.x;
+        const uint64_t t = s_nd.t + k_step;
+        const uint32_t tmod = (uint32_t)((s_nd.tmod + k_step) % s_nd.D);
+        process_tile<INT, BLOCK, NPT, false, ADEX>(eng, ptab, s_nd, tile, t, tmod, s_nd.v + tile.start,
+                                                  s_nd.u + tile.start, s_nd.s + tile.start, s_nd.tk + tile.start,
+                                                  s_nd.pidx + tile.start, sl);
+        if (nx >= n_tiles) break;
+        const Tile next = eng->tiles[nx];
+        if (next.net != tile.net) {
+            __syncthreads();  // every thread is done with the staged descriptor
+            stage_net(eng, next.net, &s_nd);
+            __syncthreads();
+        }
+        tix = nx;
+        tile = next;
     }
 }
 
@@ -322,7 +380,7 @@ __host__ __device__ constexpr uint32_t resident_head_bytes() {
     return (uint32_t)((BLOCK * NPT + BLOCK / 32 + 2) * 4 + 15) / 16 * 16;
 }
 
-template <bool INT, int BLOCK, int NPT>
+template <bool INT, int BLOCK, int NPT, bool ADEX>
 __global__ void __launch_bounds__(BLOCK) resident_kernel(const EngineDev *__restrict__ eng, uint32_t k0,
                                                          uint32_t nsteps) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -336,6 +394,8 @@ __global__ void __launch_bounds__(BLOCK) resident_kernel(const EngineDev *__rest
     float *ss = su + M;
     uint16_t *stk = reinterpret_cast<uint16_t *>(ss + M);
     uint16_t *spi = stk + M;
+    __shared__ __align__(16) ParamRow s_ptab[kSmemParamRows];
+    const ParamRow *ptab = stage_params<BLOCK>(eng, s_ptab);
     const uint32_t t_lo = eng->block_tiles[blockIdx.x], t_hi = eng->block_tiles[blockIdx.x + 1];
 
     for (uint32_t tix = t_lo; tix < t_hi; ++tix) {
@@ -356,7 +416,11 @@ __global__ void __launch_bounds__(BLOCK) resident_kernel(const EngineDev *__rest
         for (uint32_t tix = t_lo; tix < t_hi; ++tix) {
             const Tile tile = eng->tiles[tix];
             const uint32_t o = tile.smem_off;
-            process_tile<INT, BLOCK, NPT, true>(eng, tile, k0 + k, sv + o, su + o, ss + o, stk + o, spi + o, sl);
+            const NetDev &nd = eng->nets[tile.net];
+            const uint64_t t = nd.t + k0 + k;
+            const uint32_t tmod = (uint32_t)((nd.tmod + k0 + k) % nd.D);
+            process_tile<INT, BLOCK, NPT, true, ADEX>(eng, ptab, nd, tile, t, tmod, sv + o, su + o, ss + o,
+                                                      stk + o, spi + o, sl);
         }
         if (k + 1 < nsteps && !grid_barrier(eng->barrier, (k + 1) * gridDim.x, eng->err, s_flag)) break;
     }
@@ -450,16 +514,25 @@ void shape_list(uint32_t *blocks, uint32_t *npts, uint32_t *count) {
     *count = c;
 }
 
-template <bool INT, int BLOCK, int NPT>
-static int occupancy_t() {
-    int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, BLOCK, NPT>, BLOCK, 0);
-    return b;
+// Kernel variants: INT (int32 fixed-point ring) x ADEX (AdEx rows present;
+// an all-Izhikevich engine runs the instance without the AdEx path).
+template <typename F>
+static auto with_kind(bool int_ring, bool adex, F f) {
+    using T = std::true_type;
+    using N = std::false_type;
+    if (int_ring) return adex ? f(T{}, T{}) : f(T{}, N{});
+    return adex ? f(N{}, T{}) : f(N{}, N{});
 }
 
-int step_occupancy(bool int_ring, uint32_t block, uint32_t npt) {
-#define X(B, P) \
-    if (block == B && npt == P) return int_ring ? occupancy_t<true, B, P>() : occupancy_t<false, B, P>();
+int step_occupancy(bool int_ring, bool adex, uint32_t block, uint32_t npt) {
+#define X(B, P)                                                                                         \
+    if (block == B && npt == P)                                                                         \
+        return with_kind(int_ring, adex, [&](auto I, auto A) {                                          \
+            int b = 0;                                                                                  \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<decltype(I)::value, B, P,     \
+                                                                          decltype(A)::value>, B, 0);   \
+            return b;                                                                                   \
+        });
     NE2B_SHAPES(X)
 #undef X
     return 0;
@@ -469,7 +542,7 @@ static bool g_pdl = true;
 void set_pdl(bool on) { g_pdl = on; }
 
 template <typename... Args>
-static cudaError_t launch_ex(void (*kernel)(Args...), uint32_t grid, uint32_t block, cudaStream_t st,
+static cudaError_t launch_ex(void (*kernel)(Args...), uint32_t grid, uint32_t block, cudaStream_t st, bool pdl,
                              Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -480,16 +553,18 @@ static cudaError_t launch_ex(void (*kernel)(Args...), uint32_t grid, uint32_t bl
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = g_pdl ? 1 : 0;
+    cfg.numAttrs = (g_pdl && pdl) ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-cudaError_t launch_step(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,
-                        uint32_t grid, cudaStream_t st) {
-#define X(B, P)                                                                            \
-    if (block == B && npt == P)                                                            \
-        return int_ring ? launch_ex(step_kernel<true, B, P>, grid, B, st, eng, k_step)     \
-                        : launch_ex(step_kernel<false, B, P>, grid, B, st, eng, k_step);
+cudaError_t launch_step(bool int_ring, bool adex, uint32_t block, uint32_t npt, const EngineDev *eng,
+                        uint32_t k_step, uint32_t grid, cudaStream_t st) {
+#define X(B, P)                                                                                          \
+    if (block == B && npt == P)                                                                          \
+        return with_kind(int_ring, adex, [&](auto I, auto A) {                                           \
+            return launch_ex(step_kernel<decltype(I)::value, B, P, decltype(A)::value>, grid, B, st,      \
+                             k_step > 0, eng, k_step);                                                   \
+        });
     NE2B_SHAPES(X)
 #undef X
     return cudaErrorInvalidValue;
@@ -502,44 +577,34 @@ uint32_t resident_head(uint32_t block, uint32_t npt) {
     return 0;
 }
 
-template <bool INT, int BLOCK, int NPT>
-static int resident_occupancy_t(size_t smem) {
-    if (cudaFuncSetAttribute(resident_kernel<INT, BLOCK, NPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-        return 0;
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, resident_kernel<INT, BLOCK, NPT>, BLOCK, smem) !=
-        cudaSuccess)
-        return 0;
-    return b;
-}
-
-int resident_occupancy(bool int_ring, uint32_t block, uint32_t npt, size_t smem) {
-#define X(B, P)                                                                                              \
-    if (block == B && npt == P)                                                                              \
-        return int_ring ? resident_occupancy_t<true, B, P>(smem) : resident_occupancy_t<false, B, P>(smem);
+int resident_occupancy(bool int_ring, bool adex, uint32_t block, uint32_t npt, size_t smem) {
+#define X(B, P)                                                                                             \
+    if (block == B && npt == P)                                                                             \
+        return with_kind(int_ring, adex, [&](auto I, auto A) {                                              \
+            auto *k = resident_kernel<decltype(I)::value, B, P, decltype(A)::value>;                        \
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=          \
+                cudaSuccess)                                                                                \
+                return 0;                                                                                   \
+            int b = 0;                                                                                      \
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, B, smem) != cudaSuccess) return 0;     \
+            return b;                                                                                       \
+        });
     NE2B_SHAPES(X)
 #undef X
     return 0;
 }
 
-template <bool INT, int BLOCK, int NPT>
-static cudaError_t launch_resident_t(const EngineDev *eng, uint32_t k0, uint32_t nsteps, uint32_t grid, size_t smem,
-                                     cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(resident_kernel<INT, BLOCK, NPT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    void *args[] = {(void *)&eng, (void *)&k0, (void *)&nsteps};
-    return cudaLaunchCooperativeKernel((const void *)resident_kernel<INT, BLOCK, NPT>, dim3(grid), dim3(BLOCK), args,
-                                       smem, st);
-}
-
-cudaError_t launch_resident(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k0,
-                            uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st) {
-#define X(B, P)                                                                               \
-    if (block == B && npt == P)                                                               \
-        return int_ring ? launch_resident_t<true, B, P>(eng, k0, nsteps, grid, smem, st)       \
-                        : launch_resident_t<false, B, P>(eng, k0, nsteps, grid, smem, st);
+cudaError_t launch_resident(bool int_ring, bool adex, uint32_t block, uint32_t npt, const EngineDev *eng,
+                            uint32_t k0, uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st) {
+#define X(B, P)                                                                                             \
+    if (block == B && npt == P)                                                                             \
+        return with_kind(int_ring, adex, [&](auto I, auto A) {                                              \
+            auto *k = resident_kernel<decltype(I)::value, B, P, decltype(A)::value>;                        \
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+            if (e != cudaSuccess) return e;                                                                 \
+            void *args[] = {(void *)&eng, (void *)&k0, (void *)&nsteps};                                    \
+            return cudaLaunchCooperativeKernel((const void *)k, dim3(grid), dim3(B), args, smem, st);       \
+        });
     NE2B_SHAPES(X)
 #undef X
     return cudaErrorInvalidValue;
@@ -547,7 +612,7 @@ cudaError_t launch_resident(bool int_ring, uint32_t block, uint32_t npt, const E
 
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st) {
     if (n_nets == 0) return cudaSuccess;
-    return launch_ex(advance_kernel, (n_nets + 127) / 128, 128, st, nets, n_nets, steps);
+    return launch_ex(advance_kernel, (n_nets + 127) / 128, 128, st, true, nets, n_nets, steps);
 }
 
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st) {

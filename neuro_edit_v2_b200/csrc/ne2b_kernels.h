@@ -10,13 +10,18 @@ namespace ne2b {
 bool shape_supported(uint32_t block, uint32_t npt);
 void set_pdl(bool on);  // programmatic dependent launch of the streaming kernels (default on)
 void shape_list(uint32_t *blocks, uint32_t *npts, uint32_t *count);
-int step_occupancy(bool int_ring, uint32_t block, uint32_t npt);
-cudaError_t launch_step(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,
-                        uint32_t grid, cudaStream_t st);
+// `adex`: an AdEx row is present in some net (else the Izhikevich-only
+// instance of the step kernels runs).
+int step_occupancy(bool int_ring, bool adex, uint32_t block, uint32_t npt);
+// k_step > 0 launches are programmatic (they follow step k_step - 1 of the
+// same launch group); k_step = 0 follows advance_kernel or host copies and
+// waits for them in full.
+cudaError_t launch_step(bool int_ring, bool adex, uint32_t block, uint32_t npt, const EngineDev *eng,
+                        uint32_t k_step, uint32_t grid, cudaStream_t st);
 uint32_t resident_head(uint32_t block, uint32_t npt);
-int resident_occupancy(bool int_ring, uint32_t block, uint32_t npt, size_t smem);
-cudaError_t launch_resident(bool int_ring, uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k0,
-                            uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st);
+int resident_occupancy(bool int_ring, bool adex, uint32_t block, uint32_t npt, size_t smem);
+cudaError_t launch_resident(bool int_ring, bool adex, uint32_t block, uint32_t npt, const EngineDev *eng,
+                            uint32_t k0, uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st);
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st);
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st);
 cudaError_t launch_trace(const uint16_t *tk, const float *tab, uint32_t n, float *out, cudaStream_t st);

@@ -30,6 +30,7 @@ enum NetFlags : uint32_t {
     kNetRecord = 1u << 2,
     kNetWindows = 1u << 3,
     kNetActive = 1u << 4,
+    kNetHasAdex = 1u << 5,  // at least one AdEx neuron
 };
 
 enum TileFlags : uint32_t {
@@ -53,6 +54,7 @@ struct alignas(16) Tile {
 
 constexpr uint16_t kTraceZero = 0xFFFFu;  // tk value of a zero trace
 constexpr uint32_t kParamAdexBit = 0x8000u;  // pidx bit: the row is an AdEx row
+constexpr uint32_t kSmemParamRows = 32;      // param tables up to this size are staged in shared memory
 
 // Per-network descriptor.  Device copy read by the kernels; the host keeps a
 // mirror and rewrites the fields it changes.
@@ -110,7 +112,7 @@ struct EngineDev {
     // resident kernel: block b owns tiles [block_tiles[b], block_tiles[b+1])
     const uint32_t *block_tiles;
     uint32_t block_neurons;  // shared-memory state capacity per block
-    uint32_t pad0;
+    uint32_t n_params;       // rows of ptab on the device
     unsigned int *barrier;   // grid-barrier arrival counter (zeroed before each launch)
     unsigned int *err;       // nonzero: a grid barrier timed out
 };

@@ -335,16 +335,23 @@ class Batch:
 
 
 class Server:
-    """Continuous-batching trial server (admission by device footprint)."""
+    """Continuous-batching trial server (admission by device footprint).
+
+    admission_threads = 0: `submit` builds the request on the device before
+    it returns.  k > 0: k library threads build requests while the device
+    steps; the request joins at a later `step`, and the server keeps the
+    net and the input matrix alive until the result is taken."""
 
     def __init__(self, neuron_capacity: int, synapse_capacity: int, ring_capacity: int, max_requests: int = 256,
-                 steps_per_launch: int = 100, int_weights: bool = True, device: int = 0):
+                 steps_per_launch: int = 100, int_weights: bool = True, device: int = 0,
+                 admission_threads: int = 0):
         c = _abi.ServerConfig(neuron_capacity, synapse_capacity, ring_capacity, max_requests, steps_per_launch,
-                              1 if int_weights else 0)
+                              1 if int_weights else 0, admission_threads)
         h = C.c_void_p()
         check(lib.ne2b_server_create(C.byref(c), device, C.byref(h)))
         self._h = h
         self.int_weights = int_weights
+        self._keep = {}  # request id -> arrays a builder thread may still read
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -362,6 +369,7 @@ class Server:
         if st == _abi.NE2B_EFULL:
             return None
         check(st)
+        self._keep[int(rid.value)] = (net, x)
         return int(rid.value)
 
     def step(self) -> tuple[int, int]:
@@ -369,7 +377,11 @@ class Server:
         check(lib.ne2b_server_step(self._h, C.byref(a), C.byref(f)))
         return int(a.value), int(f.value)
 
+    def synchronize(self) -> None:
+        check(lib.ne2b_server_synchronize(self._h))
+
     def finished(self) -> list[int]:
+        """Finished requests whose results are ready to take."""
         cnt = C.c_uint32()
         check(lib.ne2b_server_finished_ids(self._h, None, 0, C.byref(cnt)))
         ids = np.zeros(max(cnt.value, 1), dtype=np.uint64)
@@ -381,7 +393,10 @@ class Server:
         check(lib.ne2b_server_result_shape(self._h, rid, C.byref(n), C.byref(w)))
         out = np.zeros((w.value, n.value), dtype=np.uint16)
         tot = C.c_uint64()
-        check(lib.ne2b_server_take_result(self._h, rid, ptr(out), C.byref(tot)))
+        st = lib.ne2b_server_take_result(self._h, rid, ptr(out), C.byref(tot))
+        if st != _abi.NE2B_ENODATA:
+            self._keep.pop(rid, None)
+        check(st)
         return out, int(tot.value)
 
     def stream_handle(self) -> int:

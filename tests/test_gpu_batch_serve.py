@@ -80,11 +80,14 @@ def test_batch_autotune_keeps_results():
             assert np.array_equal(a.window_counts(k, w), b.window_counts(k, w))
 
 
-def test_server_results_equal_alone_and_admission():
+@pytest.mark.parametrize("threads", [0, 2])
+def test_server_results_equal_alone_and_admission(threads):
+    """Served requests equal the same nets run alone, with admission inside
+    submit (threads = 0) or on admission threads while the device steps."""
     nets = liquids()
     steps = [500, 800, 300, 700, 400, 600]
     srv = nb.Server(neuron_capacity=3 * 2048, synapse_capacity=10**7, ring_capacity=10**8, max_requests=3,
-                    steps_per_launch=50)
+                    steps_per_launch=50, admission_threads=threads)
     pending = list(range(len(nets)))
     ids = {}
     refused = 0
@@ -101,6 +104,7 @@ def test_server_results_equal_alone_and_admission():
         if not pending and srv.stats()["active"] == 0:
             break
     assert refused > 0  # capacity forced queueing
+    srv.synchronize()
     results = {}
     for rid in srv.finished():
         counts, tot = srv.take(rid)
@@ -116,6 +120,40 @@ def test_server_results_equal_alone_and_admission():
         assert tot == alone.spikes_total()
         for w in range(steps[k] // WIN):
             assert np.array_equal(counts[w], alone.window_counts(w)), (k, w)
+
+
+@pytest.mark.parametrize("threads", [0, 2])
+def test_server_invalid_request_is_an_error(threads):
+    """A net that fails validation (a target out of range) is refused by
+    submit, or, with admission threads, finishes with the error that take
+    reports; the server keeps serving."""
+    one = O.ONet()
+    one.add_neuron(0, 0, 0, O.EXC)
+    bad = one.flat()
+    bad.src_ptr = np.array([0, 1], np.uint32)
+    bad.tgt = np.array([5], np.uint32)
+    bad.w = np.array([1.0], np.float32)
+    bad.delay_steps = np.array([1], np.uint16)
+    good = liquids()[0]
+    srv = nb.Server(neuron_capacity=4096, synapse_capacity=10**6, ring_capacity=10**7, max_requests=4,
+                    steps_per_launch=50, admission_threads=threads)
+    x = np.zeros((200, 0), np.float32)
+    if threads == 0:
+        with pytest.raises(nb.Ne2bError, match="EINVAL"):
+            srv.submit(bad, cfg(1), x, 200)
+    else:
+        rid = srv.submit(bad, cfg(1), x, 200)
+        gid = srv.submit(good, cfg(2), streams(2, 200), 200)
+        for _ in range(100):
+            srv.step()
+            if srv.stats()["active"] == 0:
+                break
+        srv.synchronize()
+        assert sorted(srv.finished()) == sorted([rid, gid])
+        with pytest.raises(nb.Ne2bError, match="EINVAL"):
+            srv.take(rid)
+        counts, tot = srv.take(gid)
+        assert counts.shape == (2, good.n)
 
 
 def test_server_rejects_oversized_request():

@@ -37,11 +37,24 @@
 
 namespace ne2b {
 
+// Shared memory of the delivery phase.  The tile's spiking neurons are
+// listed by their CSR rows: lo[k] is row k's first synapse and off[k] the
+// number of synapses in rows 0..k-1 (off[total] = all of them), so the
+// block can stride one flat range of synapse indices.
 struct SmemLists {
-    uint32_t *list;   // [tile size] spiking local ids
-    uint32_t *woff;   // [warps] prefix offsets
-    uint32_t *total;  // [1]
+    uint32_t *lo;     // [tile size]
+    uint32_t *off;    // [tile size + 1]
+    uint32_t *woff;   // [warps] spike prefix per warp
+    uint32_t *wsyn;   // [warps] synapse prefix per warp
+    uint32_t *total;  // [2] spikes, synapses
 };
+template <int BLOCK, int NPT>
+__host__ __device__ constexpr uint32_t smem_lists_words() {
+    return 2 * BLOCK * NPT + 1 + 2 * (BLOCK / 32) + 2;
+}
+__device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, uint32_t nw) {
+    return SmemLists{base, base + tile, base + 2 * tile + 1, base + 2 * tile + 1 + nw, base + 2 * tile + 1 + 2 * nw};
+}
 
 // `nd` is the tile's net descriptor (global memory, or a shared-memory copy
 // staged before the launch's dependency wait); `t` is the absolute step and
@@ -97,9 +110,12 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     }
 
     bool spk[NPT];
+    uint32_t rlo[NPT], rhi[NPT];  // CSR row of a spiking neuron, loaded as soon as it spikes
+    const uint32_t *__restrict__ rowptr = nd.rowptr;
 #pragma unroll
     for (int q = 0; q < NPT; ++q) {
         spk[q] = false;
+        rlo[q] = rhi[q] = 0u;
         if (!valid[q]) continue;
         const uint32_t i = li[q];
         const uint32_t off = q * BLOCK + threadIdx.x;
@@ -152,7 +168,11 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         // and a zero trace step after step)
         if (__float_as_uint(snew) != __float_as_uint(s[q])) ss[off] = snew;
         if (k != k0) tks[off] = (uint16_t)k;
-        if (sp) nd.pn_total[i] += 1ull;
+        if (sp) {
+            rlo[q] = rowptr[i];
+            rhi[q] = rowptr[i + 1];
+            nd.pn_total[i] += 1ull;
+        }
         if (windows) {
             if (win_end) {
                 const uint32_t c = nd.wcount[i] + (sp ? 1u : 0u);
@@ -165,74 +185,105 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         spk[q] = sp;
     }
 
-    // ---- compaction: warp ballots -> record words + block prefix sum
-    uint32_t mask[NPT];
-    uint32_t wcnt = 0;
-#pragma unroll
-    for (int q = 0; q < NPT; ++q) {
-        mask[q] = __ballot_sync(0xffffffffu, spk[q]);
-        wcnt += __popc(mask[q]);
-    }
+    // ---- spike record: one ballot word per warp and q
     if (flags & kNetRecord) {
         const uint32_t row = (uint32_t)(t % nd.rec_rows);
         const uint32_t words32 = n_pad >> 5;
-        if (lane == 0) {
 #pragma unroll
-            for (int q = 0; q < NPT; ++q) {
-                const uint32_t off = q * BLOCK + warp * 32;
-                if (off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask[q];
-            }
+        for (int q = 0; q < NPT; ++q) {
+            const uint32_t mask = __ballot_sync(0xffffffffu, spk[q]);
+            const uint32_t off = q * BLOCK + warp * 32;
+            if (lane == 0 && off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask;
         }
     }
+    // ---- compaction: per-thread (spikes, synapses), block prefix sums
+    uint32_t cnt = 0, syn = 0;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+        if (spk[q]) {
+            ++cnt;
+            syn += rhi[q] - rlo[q];
+        }
     // quiet tile: one block barrier, no scan, no delivery
-    if (!__syncthreads_or(wcnt != 0u)) return;
-    if (lane == 0) sl.woff[warp] = wcnt;
+    if (!__syncthreads_or(cnt != 0u)) return;
+    uint32_t ic = cnt, is = syn;  // inclusive warp scans
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t yc = __shfl_up_sync(0xffffffffu, ic, o);
+        const uint32_t ys = __shfl_up_sync(0xffffffffu, is, o);
+        if (lane >= o) {
+            ic += yc;
+            is += ys;
+        }
+    }
+    if (lane == 31) {
+        sl.woff[warp] = ic;
+        sl.wsyn[warp] = is;
+    }
     __syncthreads();
     if (warp == 0) {
-        const uint32_t c = lane < NW ? sl.woff[lane] : 0u;
-        uint32_t incl = c;
+        uint32_t c = lane < NW ? sl.woff[lane] : 0u, y = lane < NW ? sl.wsyn[lane] : 0u;
+        uint32_t jc = c, js = y;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+            const uint32_t a = __shfl_up_sync(0xffffffffu, jc, o);
+            const uint32_t b = __shfl_up_sync(0xffffffffu, js, o);
+            if (lane >= o) {
+                jc += a;
+                js += b;
+            }
         }
-        if (lane < NW) sl.woff[lane] = incl - c;
-        if (lane == 31) *sl.total = incl;
+        if (lane < NW) {
+            sl.woff[lane] = jc - c;
+            sl.wsyn[lane] = js - y;
+        }
+        if (lane == 31) {
+            sl.total[0] = jc;
+            sl.total[1] = js;
+        }
     }
     __syncthreads();
     {
-        uint32_t pos = sl.woff[warp];
-        const uint32_t lt = (1u << lane) - 1u;
+        uint32_t pos = sl.woff[warp] + ic - cnt;
+        uint32_t so = sl.wsyn[warp] + is - syn;
 #pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-            if (spk[q]) sl.list[pos + __popc(mask[q] & lt)] = li[q];
-            pos += __popc(mask[q]);
-        }
+        for (int q = 0; q < NPT; ++q)
+            if (spk[q]) {
+                sl.lo[pos] = rlo[q];
+                sl.off[pos] = so;
+                ++pos;
+                so += rhi[q] - rlo[q];
+            }
     }
+    const uint32_t total = sl.total[0], nsyn = sl.total[1];
+    if (threadIdx.x == 0) sl.off[total] = nsyn;
     __syncthreads();
-    const uint32_t total = *sl.total;
     if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
-    const uint32_t *__restrict__ rowptr = nd.rowptr;
+    // ---- delivery: the block strides the flat synapse range; a thread
+    // finds its row by binary search over off[], then adds the weight into
+    // ring[(t + d) % D][tgt] with a no-return atomic
     const uint32_t *__restrict__ tgt = nd.tgt;
     const bool d16 = flags & kNetDelay16;
-    for (uint32_t si = warp; si < total; si += NW) {
-        const uint32_t i = sl.list[si];
-        const uint32_t lo = rowptr[i], hi = rowptr[i + 1];
-        for (uint32_t j = lo + lane; j < hi; j += 32) {
-            const uint32_t tg = tgt[j];
-            const uint32_t d =
-                d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
-            uint32_t slot = tmod + d;
-            if (slot >= D) slot -= D;
-            const size_t idx = (size_t)slot * n_pad + tg;
-            if (INT) {
-                atomicAdd((int *)ringw + idx, ((const int *)nd.w)[j]);
-            } else {
-                atomicAdd((float *)ringw + idx, ((const float *)nd.w)[j]);
-            }
+    for (uint32_t f = threadIdx.x; f < nsyn; f += BLOCK) {
+        uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sl.off[mid] <= f) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t j = sl.lo[lo] + (f - sl.off[lo]);
+        const uint32_t tg = tgt[j];
+        const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
+        uint32_t slot = tmod + d;
+        if (slot >= D) slot -= D;
+        const size_t idx = (size_t)slot * n_pad + tg;
+        if (INT) {
+            atomicAdd((int *)ringw + idx, ((const int *)nd.w)[j]);
+        } else {
+            atomicAdd((float *)ringw + idx, ((const float *)nd.w)[j]);
         }
     }
-    // the next tile reuses the shared spike list
+    // the next tile reuses the shared lists
     __syncthreads();
 }
 
@@ -280,14 +331,12 @@ __device__ __forceinline__ void stage_net(const EngineDev *__restrict__ eng, uin
 template <bool INT, int BLOCK, int NPT, bool ADEX>
 __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
     pdl_trigger();
-    __shared__ uint32_t s_list[BLOCK * NPT];
-    __shared__ uint32_t s_woff[BLOCK / 32];
-    __shared__ uint32_t s_total;
+    __shared__ uint32_t s_lists[smem_lists_words<BLOCK, NPT>()];
     __shared__ __align__(16) NetDev s_nd;
     __shared__ __align__(16) ParamRow s_ptab[kSmemParamRows];
     static_assert(sizeof(NetDev) % 16 == 0 && sizeof(ParamRow) % 16 == 0, "16-byte staging");
     static_assert(sizeof(NetDev) / 16 <= BLOCK, "one 16-byte word per thread");
-    const SmemLists sl{s_list, s_woff, &s_total};
+    const SmemLists sl = smem_lists(s_lists, BLOCK * NPT, BLOCK / 32);
     const uint32_t n_tiles = eng->n_tiles;
     uint32_t tix = blockIdx.x;
     if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
@@ -373,11 +422,11 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int
     return *s_flag != 0u;
 }
 
-// Shared memory: [spike list TILE u32][woff NW u32][total, flag u32]
+// Shared memory: [delivery lists][flag u32]
 //                [v M f32][u M f32][s M f32][tk M u16][pidx M u16]
 template <int BLOCK, int NPT>
 __host__ __device__ constexpr uint32_t resident_head_bytes() {
-    return (uint32_t)((BLOCK * NPT + BLOCK / 32 + 2) * 4 + 15) / 16 * 16;
+    return (uint32_t)((smem_lists_words<BLOCK, NPT>() + 1) * 4 + 15) / 16 * 16;
 }
 
 template <bool INT, int BLOCK, int NPT, bool ADEX>
@@ -386,8 +435,8 @@ __global__ void __launch_bounds__(BLOCK) resident_kernel(const EngineDev *__rest
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int TILE = BLOCK * NPT;
     uint32_t *head = reinterpret_cast<uint32_t *>(smem);
-    const SmemLists sl{head, head + TILE, head + TILE + BLOCK / 32};
-    unsigned int *s_flag = head + TILE + BLOCK / 32 + 1;
+    const SmemLists sl = smem_lists(head, TILE, BLOCK / 32);
+    unsigned int *s_flag = head + smem_lists_words<BLOCK, NPT>();
     const uint32_t M = eng->block_neurons;
     float *sv = reinterpret_cast<float *>(smem + resident_head_bytes<BLOCK, NPT>());
     float *su = sv + M;

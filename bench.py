@@ -229,7 +229,16 @@ def run_ours(args):
     dev = local
     net = nb.random_kout(N, K_OUT, SEED + rank)
     sim = nb.B200Sim(net, make_cfg(nb, False), device=dev)
-    tiling = sim.autotune(256)
+
+    def tune(s):
+        if args.shape and args.kernel:
+            s.set_kernel_mode({"stream": nb.KERNEL_STREAM, "resident": nb.KERNEL_RESIDENT}[args.kernel])
+            b, npt = (int(x) for x in args.shape.split("x"))
+            s.set_tile_shape(b, npt)
+            return s.tiling()
+        return s.autotune(256)
+
+    tiling = tune(sim)
     scrub = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
 
     with Clocks(dev) as clk:
@@ -247,7 +256,7 @@ def run_ours(args):
 
     # active companion regime (same net, Poisson kicks on top)
     act = nb.B200Sim(net, make_cfg(nb, True), device=dev)
-    a_tiling = act.autotune(256)
+    a_tiling = tune(act)
     a_ms, a_spikes, _ = timed_trials(act, max(1, args.steps // 2), 1, TRIAL_STEPS, ws, torch, scrub)
     a_ms = max_over_ranks(a_ms, ws)
     a_trials = max(1, args.steps // 2)
@@ -608,8 +617,18 @@ def main():
     ap.add_argument("--profile-neurons", type=int, default=N, help="network size in --profile mode")
     ap.add_argument("--kernel", choices=["stream", "resident"], default=None, help="force the step kernel")
     ap.add_argument("--autotune", action="store_true", help="--profile with the autotuned kernel and tiling")
-    ap.add_argument("--shape", default=None, help="--profile with tile shape BLOCKxNPT, e.g. 256x2")
+    ap.add_argument("--shape", default=None,
+                    help="tile shape BLOCKxNPT, e.g. 256x2 (with --kernel: fixes the headline tiling instead of "
+                         "autotuning it, e.g. for an ncu launch list)")
+    ap.add_argument("--floors", action="store_true",
+                    help="print the measured launch / streaming / atomic floors (neuro_edit_v2_b200/_lib/probe_floors)")
     args = ap.parse_args()
+    if args.floors:
+        sys.path.insert(0, ROOT)
+        from neuro_edit_v2_b200 import build as B
+
+        B.build()
+        sys.exit(subprocess.run([B.PROBE]).returncode)
     if args.warmup < 3:
         args.warmup = 3
     if args.profile:

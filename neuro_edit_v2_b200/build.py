@@ -4,7 +4,9 @@ Compiles the CUDA kernels ahead of time for sm_100a only
 (`-gencode arch=compute_100a,code=sm_100a`) with `-fmad=false`, so no float
 operation of the step is contracted into an FMA, and the host sources with
 `-ffp-contract=off`.  The library is built in-tree so it travels with the
-repository; nothing is installed.
+repository; nothing is installed.  `_lib/probe_floors` (csrc/probe_floors.cu)
+is a standalone program that measures the launch, streaming and atomic floors
+that bound the step kernel (`python bench.py --floors`).
 """
 from __future__ import annotations
 
@@ -16,8 +18,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libne2b.so")
-SOURCES = ["ne2b_kernels.cu", "ne2b_engine.cu", "ne2b_capi.cu", "ne2b_noalloc.cu", "ne2b_host.cpp"]
-HEADERS = ["ne2b_device.cuh", "ne2b_layout.h", "ne2b_kernels.h", "ne2b_engine.h", "ne2b_handles.h", "ne2b_parallel.h"]
+SOURCES = ["ne2b_step_k00.cu", "ne2b_step_k01.cu", "ne2b_step_k10.cu", "ne2b_step_k11.cu", "ne2b_kernels.cu",
+           "ne2b_engine.cu", "ne2b_capi.cu", "ne2b_noalloc.cu", "ne2b_host.cpp"]
+HEADERS = ["ne2b_device.cuh", "ne2b_layout.h", "ne2b_kernels.h", "ne2b_engine.h", "ne2b_handles.h", "ne2b_parallel.h",
+           "ne2b_step.cuh", "ne2b_step_kind.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -44,27 +48,48 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+PROBE = os.path.join(OUT_DIR, "probe_floors")
+
+
+def _run_all(cmds, verbose: bool) -> None:
+    """Run the compiler commands concurrently; raise on the first failure."""
+    procs = []
+    for cmd in cmds:
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
+    probe_src = os.path.join(CSRC, "probe_floors.cu")
+    probe_stale = not os.path.exists(PROBE) or os.path.getmtime(probe_src) > os.path.getmtime(PROBE)
+    if not force and not _stale() and not probe_stale:
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
+    cmds = []
     objs = []
-    for src in SOURCES:
-        obj = os.path.join(OUT_DIR, src + ".o")
-        cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+    if force or _stale():
+        for src in SOURCES:
+            obj = os.path.join(OUT_DIR, src + ".o")
+            cmds.append([nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj])
+            objs.append(obj)
+    if force or probe_stale:
+        cmds.append([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", probe_src, "-o",
+                     PROBE])
+    _run_all(cmds, verbose)
+    if objs:
+        tmp = LIB + ".tmp"
+        cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp, "-lcudart",
+               "-Xcompiler", "-pthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
-    tmp = LIB + ".tmp"
-    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp, "-lcudart",
-           "-Xcompiler", "-pthread"]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
-    for o in objs:
-        os.remove(o)
+        os.replace(tmp, LIB)
+        for o in objs:
+            os.remove(o)
     return LIB
 
 

@@ -14,6 +14,23 @@ namespace ne2b {
 __device__ __forceinline__ uint64_t noise_base(uint32_t i, uint64_t t, uint64_t seed) {
     return (uint64_t)i * 0x9E3779B97F4A7C15ull + t * 0xBF58476D1CE4E5B9ull + seed * 0x94D049BB133111EBull;
 }
+// The same base split into its step part (one per tile) and its neuron part:
+// the sum is taken mod 2^64, so the grouping does not change the value.
+__device__ __forceinline__ uint64_t noise_base_step(uint64_t t, uint64_t seed) {
+    return t * 0xBF58476D1CE4E5B9ull + seed * 0x94D049BB133111EBull;
+}
+__device__ __forceinline__ uint64_t noise_base_at(uint32_t i, uint64_t step_part) {
+    return (uint64_t)i * 0x9E3779B97F4A7C15ull + step_part;
+}
+
+// x mod m for the step counters: x < 2^32 in every run shorter than 5 days
+// of 0.1 ms steps, where 32-bit division is used.
+__device__ __forceinline__ uint32_t mod_steps(uint64_t x, uint32_t m) {
+    return x <= 0xffffffffull ? (uint32_t)x % m : (uint32_t)(x % m);
+}
+__device__ __forceinline__ uint64_t div_steps(uint64_t x, uint32_t m) {
+    return x <= 0xffffffffull ? (uint64_t)((uint32_t)x / m) : x / m;
+}
 
 // splitmix64 finaliser: sim/src/state.rs:289-293.
 __device__ __forceinline__ uint64_t mix64(uint64_t h) {

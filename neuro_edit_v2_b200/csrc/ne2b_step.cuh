@@ -1,0 +1,567 @@
+// ne2b_step.cuh — the step kernels (streaming and resident), included by the
+// four translation units that instantiate them, one per kernel kind.
+//
+// A tile is `count` consecutive neurons of one network.  Processing one tile
+// for one dt step (process_tile):
+//
+//   1. read the tile's state and its ring slot for this step, zeroing the slot
+//      words that held arrivals (sim/src/cpu.rs:218-222, kernels.rs:104-107);
+//   2. assemble the input current s + ext (+ stimulus) (+ noise) in the
+//      reference order and run the model step (cpu.rs:223-250);
+//   3. update s and the trace with the host-computed decays (cpu.rs:252-260);
+//      the trace is kept as "steps since the last spike" into a table of the
+//      exact f32 products 1.0 * decay_t * decay_t ..., which reproduces the
+//      reference's repeated multiply bit-for-bit at 2 bytes per neuron;
+//   4. write the spike-record words straight from warp ballots, and compact
+//      the tile's spikes by their CSR rows with block prefix sums over
+//      (spikes, synapses) into shared memory (replaces the global atomicAdd
+//      slot of kernels.rs:150-156);
+//   5. deliver its own spikes: the block strides the flat range of all its
+//      spikes' synapses, a no-return atomic add into
+//      ring[(t + delay) % D][tgt] per synapse (cpu.rs:264-278,
+//      kernels.rs:174-204).
+//
+// Within a step no cross-block ordering is needed: step t reads slot t % D and
+// every delivery of step t lands in slot (t + d) % D, 1 <= d < D.  Between
+// steps, step t's deliveries must land before step t+1 reads:
+//   * step_kernel (streaming): one launch per step, the kernel boundary orders
+//     the steps; state is streamed from HBM every step.
+//   * resident_kernel (persistent, cooperative): each block owns a fixed set
+//     of tiles whose state stays in shared memory for the whole launch; steps
+//     are separated by a grid barrier whose wait is bounded by %globaltimer
+//     (2 s, then the launch stops and reports an error flag).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ne2b_device.cuh"
+#include "ne2b_step_kind.h"
+
+namespace ne2b {
+
+// Shared memory of the delivery phase.  The tile's spiking neurons are
+// listed by their CSR rows: lo[k] is row k's first synapse and off[k] the
+// number of synapses in rows 0..k-1 (off[total] = all of them), so the
+// block can stride one flat range of synapse indices.
+struct SmemLists {
+    uint32_t *lo;     // [tile size]
+    uint32_t *off;    // [tile size + 1]
+    uint32_t *woff;   // [warps] spike prefix per warp
+    uint32_t *wsyn;   // [warps] synapse prefix per warp
+    uint32_t *total;  // [2] spikes, synapses
+};
+__device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, uint32_t nw) {
+    return SmemLists{base, base + tile, base + 2 * tile + 1, base + 2 * tile + 1 + nw, base + 2 * tile + 1 + 2 * nw};
+}
+
+// `nd` is the tile's net descriptor (global memory, or a shared-memory copy
+// staged before the launch's dependency wait); `t` is the absolute step and
+// `tmod` = t % D.  ADEX: the net holds AdEx rows (else the Izhikevich path is
+// the only one compiled into this instance).
+// `ptab` is the parameter table (a shared-memory copy when it is small).
+template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX>
+__device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
+                                             const Tile &tile, uint64_t t, uint32_t tmod, float *vs, float *us,
+                                             float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const uint32_t flags = nd.flags;
+    if (!(flags & kNetActive)) return;  // uniform across the block
+    if (t >= nd.t_end) return;  // uniform across the block
+
+    const uint32_t n = nd.n, n_pad = nd.n_pad, D = nd.D;
+    const size_t slot_off = (size_t)tmod * n_pad;
+    const float dt = nd.dt, decay_s = nd.decay_s;
+    const float pkick = nd.pkick, kick = nd.kick, gauss_k = nd.gauss_k;
+    const uint64_t nbase = noise_base_step(t, nd.seed);
+    const uint32_t tlast = nd.trace_last;
+    uint32_t *__restrict__ ringw = (uint32_t *)nd.ring;
+    const bool has_ext = flags & kNetHasExt;
+    const bool has_stim = tile.flags & kTileHasStim;
+    const bool windows = flags & kNetWindows;
+    bool win_end = false;
+    uint32_t widx = 0;
+    if (windows) {
+        win_end = mod_steps(t + 1, nd.win_steps) == 0u;
+        widx = (uint32_t)div_steps(t + 1, nd.win_steps) - 1u;
+    }
+
+    uint32_t li[NPT];
+    bool valid[NPT];
+    float v[NPT], u[NPT], s[NPT], ex[NPT];
+    uint32_t rw[NPT], tk[NPT], pi[NPT];
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) {
+        const uint32_t off = q * BLOCK + threadIdx.x;
+        li[q] = tile.start + off;
+        valid[q] = off < tile.count && li[q] < n;
+        if (valid[q]) {
+            rw[q] = RES ? __ldcg(ringw + slot_off + li[q]) : ringw[slot_off + li[q]];
+            v[q] = vs[off];
+            u[q] = us[off];
+            s[q] = ss[off];
+            tk[q] = tks[off];
+            pi[q] = pis[off];
+            ex[q] = has_ext ? nd.ext[li[q]] : 0.0f;
+        }
+    }
+    // warm L2 with the next step's ring slot (one prefetch per 32-byte
+    // sector): in a quiet net that slot was last touched D steps ago and
+    // would otherwise come from DRAM on the next step's critical path
+    {
+        const uint32_t nslot = tmod + 1u == D ? 0u : tmod + 1u;
+        const uint32_t *nrow = ringw + (size_t)nslot * n_pad;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q)
+            if (valid[q] && (lane & 7) == 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(nrow + li[q]));
+    }
+
+    bool spk[NPT];
+    uint32_t rlo[NPT], rhi[NPT];  // CSR row of a spiking neuron, loaded as soon as it spikes
+    const uint32_t *__restrict__ rowptr = nd.rowptr;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) {
+        spk[q] = false;
+        rlo[q] = rhi[q] = 0u;
+        if (!valid[q]) continue;
+        const uint32_t i = li[q];
+        const uint32_t off = q * BLOCK + threadIdx.x;
+        const float arr = INT ? __fmul_rn(__int2float_rn((int)rw[q]), 0x1p-12f)  // rt_get, kernels.rs:60
+                              : __uint_as_float(rw[q]);
+        if (rw[q] != 0u) ringw[slot_off + i] = 0u;
+        const float sv = __fadd_rn(s[q], arr);
+        float I = __fadd_rn(sv, ex[q]);
+        if (has_stim) {
+            // the host provides the [steps x inputs] values covering every
+            // launched step; the range check only guards the read
+            const long long rel = (long long)t - nd.stim_t0;
+            const float *row = (rel >= 0 && rel < (long long)nd.stim_len) ? nd.stim_buf + (size_t)rel * nd.n_inputs
+                                                                          : nullptr;
+            const uint32_t lo = nd.stim_ptr[i], hi = nd.stim_ptr[i + 1];
+            if (row)
+                for (uint32_t j = lo; j < hi; ++j) I = __fadd_rn(I, __fmul_rn(nd.stim_w[j], row[nd.stim_in[j]]));
+        }
+        // pidx bit 15 marks an AdEx row: an Izhikevich neuron reads only the
+        // first 16 bytes of its parameter row
+        const bool adex = ADEX && (pi[q] & kParamAdexBit) != 0u;
+        const ParamRow &pr = ptab[pi[q] & ~kParamAdexBit];
+        float p[10];
+        const float4 p0 = *reinterpret_cast<const float4 *>(&pr.p[0]);
+        p[0] = p0.x; p[1] = p0.y; p[2] = p0.z; p[3] = p0.w;
+        if (ADEX && adex) {
+            const float4 p1 = *reinterpret_cast<const float4 *>(&pr.p[4]);
+            const float4 p2 = *reinterpret_cast<const float4 *>(&pr.p[8]);
+            p[4] = p1.x; p[5] = p1.y; p[6] = p1.z; p[7] = p1.w;
+            p[8] = p2.x; p[9] = p2.y;
+        }
+        const float gain = (ADEX && adex) ? p[0] : 1.0f;  // model/mod.rs:104-106, adex.rs:189-191
+        if (pkick > 0.0f || gauss_k != 0.0f) {
+            const uint64_t base = noise_base_at(i, nbase);
+            if (pkick > 0.0f && noise_fires(base, pkick)) I = __fadd_rn(I, __fmul_rn(kick, gain));
+            if (gauss_k != 0.0f)
+                I = __fadd_rn(I, __fmul_rn(__int2float_rn(gauss_numer(base)), __fmul_rn(gauss_k, gain)));
+        }
+        bool sp;
+        if (ADEX && adex) sp = adex_step(p, v[q], u[q], I, dt);
+        else sp = izh_step(p, v[q], u[q], I, dt);
+        // trace: 1 on spike, else one more multiply by decay_t (saturating at
+        // the table's last entry, 0 or the subnormal fixed point)
+        const uint32_t k0 = tk[q];
+        const uint32_t k = sp ? 0u : (k0 == kTraceZero ? k0 : (k0 < tlast ? k0 + 1u : tlast));
+        const float snew = __fmul_rn(sv, decay_s);
+        vs[off] = v[q];
+        us[off] = u[q];
+        // s and tk are written only when they change (quiet neurons keep s = 0
+        // and a zero trace step after step)
+        if (__float_as_uint(snew) != __float_as_uint(s[q])) ss[off] = snew;
+        if (k != k0) tks[off] = (uint16_t)k;
+        if (sp) {
+            rlo[q] = rowptr[i];
+            rhi[q] = rowptr[i + 1];
+            nd.pn_total[i] += 1ull;
+        }
+        if (windows) {
+            if (win_end) {
+                const uint32_t c = nd.wcount[i] + (sp ? 1u : 0u);
+                if (widx < nd.max_windows) nd.win_out[(size_t)widx * n_pad + i] = (uint16_t)(c > 65535u ? 65535u : c);
+                nd.wcount[i] = 0u;
+            } else if (sp) {
+                nd.wcount[i] += 1u;
+            }
+        }
+        spk[q] = sp;
+    }
+
+    // ---- spike record: one ballot word per warp and q
+    if (flags & kNetRecord) {
+        const uint32_t row = mod_steps(t, nd.rec_rows);
+        const uint32_t words32 = n_pad >> 5;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+            const uint32_t mask = __ballot_sync(0xffffffffu, spk[q]);
+            const uint32_t off = q * BLOCK + warp * 32;
+            if (lane == 0 && off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask;
+        }
+    }
+    // ---- compaction: per-thread (spikes, synapses), block prefix sums
+    uint32_t cnt = 0, syn = 0;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+        if (spk[q]) {
+            ++cnt;
+            syn += rhi[q] - rlo[q];
+        }
+    // quiet tile: one block barrier, no scan, no delivery
+    if (!__syncthreads_or(cnt != 0u)) return;
+    uint32_t ic = cnt, is = syn;  // inclusive warp scans
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t yc = __shfl_up_sync(0xffffffffu, ic, o);
+        const uint32_t ys = __shfl_up_sync(0xffffffffu, is, o);
+        if (lane >= o) {
+            ic += yc;
+            is += ys;
+        }
+    }
+    if (lane == 31) {
+        sl.woff[warp] = ic;
+        sl.wsyn[warp] = is;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t c = lane < NW ? sl.woff[lane] : 0u, y = lane < NW ? sl.wsyn[lane] : 0u;
+        uint32_t jc = c, js = y;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t a = __shfl_up_sync(0xffffffffu, jc, o);
+            const uint32_t b = __shfl_up_sync(0xffffffffu, js, o);
+            if (lane >= o) {
+                jc += a;
+                js += b;
+            }
+        }
+        if (lane < NW) {
+            sl.woff[lane] = jc - c;
+            sl.wsyn[lane] = js - y;
+        }
+        if (lane == 31) {
+            sl.total[0] = jc;
+            sl.total[1] = js;
+        }
+    }
+    __syncthreads();
+    {
+        uint32_t pos = sl.woff[warp] + ic - cnt;
+        uint32_t so = sl.wsyn[warp] + is - syn;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q)
+            if (spk[q]) {
+                sl.lo[pos] = rlo[q];
+                sl.off[pos] = so;
+                ++pos;
+                so += rhi[q] - rlo[q];
+            }
+    }
+    const uint32_t total = sl.total[0], nsyn = sl.total[1];
+    if (threadIdx.x == 0) sl.off[total] = nsyn;
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
+    // ---- delivery: the block strides the flat synapse range; a thread
+    // finds its row by binary search over off[], then adds the weight into
+    // ring[(t + d) % D][tgt] with a no-return atomic
+    const uint32_t *__restrict__ tgt = nd.tgt;
+    const bool d16 = flags & kNetDelay16;
+    for (uint32_t f = threadIdx.x; f < nsyn; f += BLOCK) {
+        uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sl.off[mid] <= f) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t j = sl.lo[lo] + (f - sl.off[lo]);
+        const uint32_t tg = tgt[j];
+        const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
+        uint32_t slot = tmod + d;
+        if (slot >= D) slot -= D;
+        const size_t idx = (size_t)slot * n_pad + tg;
+        if (INT) {
+            atomicAdd((int *)ringw + idx, ((const int *)nd.w)[j]);
+        } else {
+            atomicAdd((float *)ringw + idx, ((const float *)nd.w)[j]);
+        }
+    }
+    // the next tile reuses the shared lists
+    __syncthreads();
+}
+
+// Programmatic dependent launch: let the next kernel of the stream be
+// scheduled now (griddepcontrol.launch_dependents), and wait until the
+// previous one has completed and its memory is visible (griddepcontrol.wait).
+// Both are no-ops for a kernel launched without the programmatic-serialization
+// attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_enter() {
+    pdl_trigger();
+    pdl_wait();
+}
+
+// Copy the parameter table into shared memory when it has at most
+// kSmemParamRows rows; returns the table the block reads from.
+template <int BLOCK>
+__device__ __forceinline__ const ParamRow *stage_params(const EngineDev *__restrict__ eng, ParamRow *s_ptab) {
+    const uint32_t np = eng->n_params;
+    if (np > kSmemParamRows) return eng->ptab;
+    constexpr uint32_t kWords = sizeof(ParamRow) / 16;
+    for (uint32_t w = threadIdx.x; w < np * kWords; w += BLOCK)
+        reinterpret_cast<uint4 *>(s_ptab)[w] = reinterpret_cast<const uint4 *>(eng->ptab)[w];
+    return s_ptab;
+}
+
+// Copy net descriptor `net` into shared memory (16-byte words, one per
+// thread).
+__device__ __forceinline__ void stage_net(const EngineDev *__restrict__ eng, uint32_t net, NetDev *s_nd) {
+    constexpr uint32_t kNetWords = sizeof(NetDev) / 16;
+    if (threadIdx.x < kNetWords)
+        reinterpret_cast<uint4 *>(s_nd)[threadIdx.x] = reinterpret_cast<const uint4 *>(eng->nets + net)[threadIdx.x];
+}
+
+// ------------------------------------------------------ streaming kernel
+// The tile list and the net descriptors are written by host copies, which
+// a launch always follows in full, and by advance_kernel (`t`, `tmod`),
+// after which the next step launch is never programmatic (launch_step
+// gives k_step = 0 a plain stream dependency).  So every block reads its
+// first tile and stages the net descriptor, t included, before the
+// dependency wait, overlapping the previous step's tail; after the wait
+// only the step's own data is read.  The descriptor is restaged only when
+// the net changes from one tile to the next.
+template <bool INT, int BLOCK, int NPT, bool ADEX>
+__global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
+    pdl_trigger();
+    __shared__ uint32_t s_lists[smem_lists_words<BLOCK, NPT>()];
+    __shared__ __align__(16) NetDev s_nd;
+    __shared__ __align__(16) ParamRow s_ptab[kSmemParamRows];
+    static_assert(sizeof(NetDev) % 16 == 0 && sizeof(ParamRow) % 16 == 0, "16-byte staging");
+    static_assert(sizeof(NetDev) / 16 <= BLOCK, "one 16-byte word per thread");
+    const SmemLists sl = smem_lists(s_lists, BLOCK * NPT, BLOCK / 32);
+    const uint32_t n_tiles = eng->n_tiles;
+    uint32_t tix = blockIdx.x;
+    if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
+    Tile tile = eng->tiles[tix];
+    stage_net(eng, tile.net, &s_nd);
+    const ParamRow *ptab = stage_params<BLOCK>(eng, s_ptab);
+    __syncthreads();
+    pdl_wait();
+    for (;;) {
+        const uint32_t nx = tix + gridDim.x;
+        const uint64_t t = s_nd.t + k_step;
+        uint32_t tmod = s_nd.tmod + k_step;
+        if (tmod >= s_nd.D) tmod %= s_nd.D;
+        process_tile<INT, BLOCK, NPT, false, ADEX>(eng, ptab, s_nd, tile, t, tmod, s_nd.v + tile.start,
+                                                  s_nd.u + tile.start, s_nd.s + tile.start, s_nd.tk + tile.start,
+                                                  s_nd.pidx + tile.start, sl);
+        if (nx >= n_tiles) break;
+        const Tile next = eng->tiles[nx];
+        if (next.net != tile.net) {
+            __syncthreads();  // every thread is done with the staged descriptor
+            stage_net(eng, next.net, &s_nd);
+            __syncthreads();
+        }
+        tix = nx;
+        tile = next;
+    }
+}
+
+// ------------------------------------------------------- resident kernel
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ unsigned int atom_add_release_gpu(unsigned int *p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// Grid barrier for a cooperative launch.  Arrival: block-wide barrier, then
+// thread 0 publishes the block's ring deliveries (gpu-scope fence) and
+// increments the counter with a release atomic; the last block to arrive
+// sees target - 1 and does not wait.  The others poll the counter with
+// acquire loads; every 64 polls they check the error flag (another block
+// gave up) and the %globaltimer limit, after which they flag the error and
+// stop.  Returns false (for every thread of the block) when the launch must
+// stop.
+__device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int target, unsigned int *err,
+                                             unsigned int *s_flag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned int ok = 1u;
+        if (atom_add_release_gpu(counter, 1u) + 1u < target) {
+            const unsigned long long t0 = globaltimer_ns();
+            for (uint32_t polls = 1;; ++polls) {
+                if (ld_acquire_gpu(counter) >= target) break;
+                if ((polls & 63u) == 0u) {
+                    if (ld_acquire_gpu(err) != 0u) {
+                        ok = 0u;
+                        break;
+                    }
+                    if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+                        atomicExch(err, 1u);
+                        ok = 0u;
+                        break;
+                    }
+                }
+            }
+        }
+        *s_flag = ok;
+    }
+    __syncthreads();
+    return *s_flag != 0u;
+}
+
+
+template <bool INT, int BLOCK, int NPT, bool ADEX>
+__global__ void __launch_bounds__(BLOCK) resident_kernel(const EngineDev *__restrict__ eng, uint32_t k0,
+                                                         uint32_t nsteps) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int TILE = BLOCK * NPT;
+    uint32_t *head = reinterpret_cast<uint32_t *>(smem);
+    const SmemLists sl = smem_lists(head, TILE, BLOCK / 32);
+    unsigned int *s_flag = head + smem_lists_words<BLOCK, NPT>();
+    const uint32_t M = eng->block_neurons;
+    float *sv = reinterpret_cast<float *>(smem + resident_head_bytes<BLOCK, NPT>());
+    float *su = sv + M;
+    float *ss = su + M;
+    uint16_t *stk = reinterpret_cast<uint16_t *>(ss + M);
+    uint16_t *spi = stk + M;
+    __shared__ __align__(16) ParamRow s_ptab[kSmemParamRows];
+    const ParamRow *ptab = stage_params<BLOCK>(eng, s_ptab);
+    const uint32_t t_lo = eng->block_tiles[blockIdx.x], t_hi = eng->block_tiles[blockIdx.x + 1];
+
+    for (uint32_t tix = t_lo; tix < t_hi; ++tix) {
+        const Tile tile = eng->tiles[tix];
+        const NetDev &nd = eng->nets[tile.net];
+        for (uint32_t j = threadIdx.x; j < tile.count; j += BLOCK) {
+            const uint32_t i = tile.start + j, o = tile.smem_off + j;
+            sv[o] = nd.v[i];
+            su[o] = nd.u[i];
+            ss[o] = nd.s[i];
+            stk[o] = nd.tk[i];
+            spi[o] = nd.pidx[i];
+        }
+    }
+    __syncthreads();
+
+    for (uint32_t k = 0; k < nsteps; ++k) {
+        for (uint32_t tix = t_lo; tix < t_hi; ++tix) {
+            const Tile tile = eng->tiles[tix];
+            const uint32_t o = tile.smem_off;
+            const NetDev &nd = eng->nets[tile.net];
+            const uint64_t t = nd.t + k0 + k;
+            uint32_t tmod = nd.tmod + k0 + k;
+            if (tmod >= nd.D) tmod %= nd.D;
+            process_tile<INT, BLOCK, NPT, true, ADEX>(eng, ptab, nd, tile, t, tmod, sv + o, su + o, ss + o,
+                                                      stk + o, spi + o, sl);
+        }
+        if (k + 1 < nsteps && !grid_barrier(eng->barrier, (k + 1) * gridDim.x, eng->err, s_flag)) break;
+    }
+    __syncthreads();
+
+    for (uint32_t tix = t_lo; tix < t_hi; ++tix) {
+        const Tile tile = eng->tiles[tix];
+        const NetDev &nd = eng->nets[tile.net];
+        for (uint32_t j = threadIdx.x; j < tile.count; j += BLOCK) {
+            const uint32_t i = tile.start + j, o = tile.smem_off + j;
+            nd.v[i] = sv[o];
+            nd.u[i] = su[o];
+            nd.s[i] = ss[o];
+            nd.tk[i] = stk[o];
+        }
+    }
+}
+
+// ------------------------------------------------ per-kind launchers
+template <typename... Args>
+static cudaError_t launch_pdl(void (*kernel)(Args...), uint32_t grid, uint32_t block, cudaStream_t st, bool pdl,
+                              Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = (pdl_enabled() && pdl) ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+template <bool INT, bool ADEX>
+int StepKind<INT, ADEX>::occupancy(uint32_t block, uint32_t npt) {
+#define X(B, P)                                                                                    \
+    if (block == B && npt == P) {                                                                  \
+        int b = 0;                                                                                 \
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX>, B, 0);     \
+        return b;                                                                                  \
+    }
+    NE2B_SHAPES(X)
+#undef X
+    return 0;
+}
+
+template <bool INT, bool ADEX>
+cudaError_t StepKind<INT, ADEX>::launch(uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,
+                                        uint32_t grid, cudaStream_t st) {
+#define X(B, P) \
+    if (block == B && npt == P) return launch_pdl(step_kernel<INT, B, P, ADEX>, grid, B, st, k_step > 0, eng, k_step);
+    NE2B_SHAPES(X)
+#undef X
+    return cudaErrorInvalidValue;
+}
+
+template <bool INT, bool ADEX>
+int StepKind<INT, ADEX>::resident_occupancy(uint32_t block, uint32_t npt, size_t smem) {
+#define X(B, P)                                                                                            \
+    if (block == B && npt == P) {                                                                          \
+        auto *k = resident_kernel<INT, B, P, ADEX>;                                                        \
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) \
+            return 0;                                                                                      \
+        int b = 0;                                                                                         \
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, B, smem) != cudaSuccess) return 0;        \
+        return b;                                                                                          \
+    }
+    NE2B_SHAPES(X)
+#undef X
+    return 0;
+}
+
+template <bool INT, bool ADEX>
+cudaError_t StepKind<INT, ADEX>::launch_resident(uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k0,
+                                                 uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st) {
+#define X(B, P)                                                                                              \
+    if (block == B && npt == P) {                                                                            \
+        auto *k = resident_kernel<INT, B, P, ADEX>;                                                          \
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+        if (e != cudaSuccess) return e;                                                                      \
+        void *args[] = {(void *)&eng, (void *)&k0, (void *)&nsteps};                                         \
+        return cudaLaunchCooperativeKernel((const void *)k, dim3(grid), dim3(B), args, smem, st);            \
+    }
+    NE2B_SHAPES(X)
+#undef X
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace ne2b

@@ -204,6 +204,8 @@ def run_profile(args):
 
     import neuro_edit_v2_b200 as nb
 
+    if args.served_mix:
+        return run_profile_served(args, nb, torch)
     net = nb.random_kout(args.profile_neurons, K_OUT, SEED)
     sim = nb.B200Sim(net, make_cfg(nb, args.active))
     if args.kernel:
@@ -216,6 +218,39 @@ def run_profile(args):
     ms, spikes, launches = timed_trials(sim, 1, 3, args.trial_steps, 1, torch, scrub)
     print(json.dumps({"profile_run": True, "neurons": args.profile_neurons, "trial_steps": args.trial_steps,
                       "ms": ms, "spikes": spikes, "launches": launches, "tiling": tiling}), flush=True)
+
+
+def run_profile_served(args, nb, torch):
+    """The first --served-mix requests of the serving stream stepped together
+    in one batch (the serving kernels without the admission loop): 3 warm-up
+    trials + 1 trial of --trial-steps steps, for ncu."""
+    from neuro_edit_v2_b200 import workloads as W
+
+    reqs = W.request_stream(args.served_mix)
+    b = nb.Batch([q.net for q in reqs], [W.request_config(q, 11 + k) for k, q in enumerate(reqs)])
+    for k, q in enumerate(reqs):
+        b.set_input_matrix(k, q.inputs)
+    if args.kernel:
+        b.set_kernel_mode({"stream": nb.KERNEL_STREAM, "resident": nb.KERNEL_RESIDENT}[args.kernel])
+    if args.shape:
+        bl, npt = (int(x) for x in args.shape.split("x"))
+        b.set_tile_shape(bl, npt)
+    stream = torch.cuda.ExternalStream(b.stream_handle())
+    for _ in range(3):
+        b.reset_state()
+        b.run_steps(args.trial_steps)
+    b.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.reset_state()
+    b.run_steps(args.trial_steps)
+    e1.record(stream)
+    e1.synchronize()
+    spikes = sum(b.spikes_total(k) for k in range(len(reqs)))
+    print(json.dumps({"profile_run": True, "served_mix": args.served_mix, "neurons": sum(q.n for q in reqs),
+                      "trial_steps": args.trial_steps, "ms": e0.elapsed_time(e1), "spikes": spikes,
+                      "tile_shape": b.tile_shape()}), flush=True)
 
 
 def run_ours(args):
@@ -620,6 +655,8 @@ def main():
     ap.add_argument("--shape", default=None,
                     help="tile shape BLOCKxNPT, e.g. 256x2 (with --kernel: fixes the headline tiling instead of "
                          "autotuning it, e.g. for an ncu launch list)")
+    ap.add_argument("--served-mix", type=int, default=0,
+                    help="--profile the first N requests of the serving stream stepped as one batch")
     ap.add_argument("--floors", action="store_true",
                     help="print the measured launch / streaming / atomic floors (neuro_edit_v2_b200/_lib/probe_floors)")
     args = ap.parse_args()

@@ -57,7 +57,8 @@ typedef struct {
     const uint32_t *tgt;         /* [n_syn] target neuron */
     const float *w;              /* [n_syn] weight, Dale's-law signed */
     const uint16_t *delay_steps; /* [n_syn] delay in steps, >= 1 */
-    const float *tau_ms;         /* [n_syn] per-synapse tau or NULL (0 = merged path) */
+    const float *tau_ms;         /* [n_syn] per-synapse tau in ms or NULL: tau > 0 gives the synapse its own
+                                    current (XSyn, sim/src/state.rs:231-275), 0 the merged ring */
     uint32_t n_inputs;           /* stimulus inputs (Network::inputs) */
     const uint32_t *stim_ptr;    /* [n + 1] neuron-major (input, weight) rows, or NULL */
     const uint32_t *stim_input;  /* [stim_ptr[n]] */
@@ -253,6 +254,9 @@ ne2b_status ne2b_server_stats(ne2b_server *s, uint64_t *admitted, uint64_t *reti
 /* Wait for every launch queued so far (no counterpart in the reference:
  * the serving loop is new). */
 ne2b_status ne2b_server_synchronize(ne2b_server *s);
+/* Tile shape of the server's step kernel (default 128 threads x 1 neuron);
+ * same shapes as ne2b_set_tile_shape.  Waits for queued launches. */
+ne2b_status ne2b_server_set_tile_shape(ne2b_server *s, uint32_t block, uint32_t npt, uint32_t blocks_per_sm);
 ne2b_status ne2b_server_stream(ne2b_server *s, void **stream);
 ne2b_status ne2b_server_kernel_launches(ne2b_server *s, uint64_t *launches);
 

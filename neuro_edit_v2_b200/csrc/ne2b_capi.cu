@@ -569,6 +569,19 @@ ne2b_status ne2b_server_create(const ne2b_server_config *cfg, int device, ne2b_s
         }
         s->eng.graph_steps = s->cfg.steps_per_launch;
         s->eng.fixed_grid = true;
+        {
+            // small tiles: the most blocks per SM, so the latency chains of
+            // active tiles (state loads, scans, CSR loads) overlap; measured
+            // 1.6x faster than 256x2 on the served request mix
+            ne2b::TileShape sh;
+            sh.block = 128;
+            sh.npt = 1;
+            st = s->eng.set_shape(sh);
+            if (st != NE2B_OK) {
+                delete s;
+                return st;
+            }
+        }
         for (uint32_t k = 0; k < std::min<uint32_t>(cfg->admission_threads, 16u); ++k) {
             auto b = std::make_unique<ne2b_server::Builder>();
             st = ne2b::cuda_error(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "admission stream");
@@ -843,6 +856,15 @@ ne2b_status ne2b_server_stats(ne2b_server *s, uint64_t *admitted, uint64_t *reti
     if (neurons_used) *neurons_used = s->used_neurons;
     if (synapses_used) *synapses_used = s->used_syn;
     return NE2B_OK;
+}
+
+ne2b_status ne2b_server_set_tile_shape(ne2b_server *s, uint32_t block, uint32_t npt, uint32_t bps) {
+    if (!s) return set_error(NE2B_EINVAL, "null server handle");
+    ne2b::TileShape sh;
+    sh.block = block;
+    sh.npt = npt;
+    sh.blocks_per_sm = bps;
+    GUARD(s->eng.set_shape(sh));
 }
 
 ne2b_status ne2b_server_synchronize(ne2b_server *s) {

@@ -390,7 +390,6 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
                 return set_error(NE2B_EINVAL, "synapse %llu targets %u >= n %u", (unsigned long long)j, net->tgt[j], n);
     }
     if (net->n_syn && mind < 1) return set_error(NE2B_EINVAL, "a synapse has delay 0 steps");
-    if (any_tau) return set_error(NE2B_UNSUPPORTED, "per-synapse tau is not supported by this backend");
     for (uint32_t i = 0; i < n; ++i)
         if (net->model[i] > 1) return set_error(NE2B_EINVAL, "neuron %u: unknown model id %u", i, net->model[i]);
     if (n > 0 && net->n_inputs > 0 && net->stim_ptr) {
@@ -523,6 +522,45 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         NET_TRY(sg.issue((void *)d.w, wst, 4 * h->e));
         NET_TRY(sg.issue((void *)d.delay, dst8, (d16 ? 2 : 1) * h->e));
     }
+    if (any_tau) {
+        // XSyn::build (sim/src/state.rs:245-274): synapses with tau > 0 get
+        // their own current, numbered in CSR order; the neuron pass reads
+        // them grouped by target (CSR order within a target)
+        std::vector<uint32_t> xmap(h->e), xt_ptr((size_t)n + 1, 0);
+        uint32_t nx = 0;
+        for (uint64_t j = 0; j < h->e; ++j) xmap[j] = net->tau_ms[j] > 0.0f ? nx++ : kNoXsyn;
+        std::vector<float> xdecay(nx), xw(nx);
+        std::vector<uint32_t> xt_idx(nx);
+        for (uint64_t j = 0; j < h->e; ++j) {
+            const uint32_t k = xmap[j];
+            if (k == kNoXsyn) continue;
+            xdecay[k] = host_decay(cfg->dt_ms, net->tau_ms[j]);  // state.rs:262-264
+            // the arrival adds w; with the int ring it is rt_get(rt_put(w)),
+            // the value the fixed-point path delivers (kernels.rs:57-66)
+            xw[k] = int_ring_ ? (float)(int32_t)lrintf(net->w[j] * 4096.0f) / 4096.0f : net->w[j];
+            xt_ptr[net->tgt[j] + 1]++;
+        }
+        for (uint32_t i = 0; i < n; ++i) xt_ptr[i + 1] += xt_ptr[i];
+        {
+            std::vector<uint32_t> fill(xt_ptr.begin(), xt_ptr.end() - 1);
+            for (uint64_t j = 0; j < h->e; ++j)
+                if (xmap[j] != kNoXsyn) xt_idx[fill[net->tgt[j]]++] = xmap[j];
+        }
+        h->nx = nx;
+        d.xwords = (nx + 31) / 32;
+        NET_TRY(alloc(&p, sizeof(uint32_t) * h->e)); d.xmap = (const uint32_t *)p;
+        NET_TRY(up(p, xmap.data(), sizeof(uint32_t) * h->e));
+        NET_TRY(alloc(&p, sizeof(uint32_t) * ((size_t)n + 1))); d.xt_ptr = (const uint32_t *)p;
+        NET_TRY(up(p, xt_ptr.data(), sizeof(uint32_t) * ((size_t)n + 1)));
+        NET_TRY(alloc(&p, sizeof(uint32_t) * nx)); d.xt_idx = (const uint32_t *)p;
+        NET_TRY(up(p, xt_idx.data(), sizeof(uint32_t) * nx));
+        NET_TRY(alloc(&p, sizeof(float) * nx)); d.xdecay = (const float *)p;
+        NET_TRY(up(p, xdecay.data(), sizeof(float) * nx));
+        NET_TRY(alloc(&p, sizeof(float) * nx)); d.xw = (const float *)p;
+        NET_TRY(up(p, xw.data(), sizeof(float) * nx));
+        NET_TRY(alloc(&p, sizeof(float) * nx)); d.xsyn = (float *)p;
+        NET_TRY(alloc(&p, sizeof(uint32_t) * (size_t)h->D * d.xwords)); d.xpend = (uint32_t *)p;
+    }
     tp[4] = now_ms();
     // stimulus routing
     const bool has_stim = n > 0 && net->n_inputs > 0 && net->stim_ptr && net->stim_ptr[n] > 0;
@@ -592,7 +630,7 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     }
     fill_noise(d, *cfg);
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
-              (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u);
+              (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u) | (h->nx ? kNetXsyn : 0u);
     tp[5] = now_ms();
     // initial state (cpu.rs:158-183), on the build stream
     NET_TRY(cuda_error(launch_reset_neurons(d, bst), "reset kernel"));
@@ -604,6 +642,11 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     if (d.win_out)
         NET_TRY(cuda_error(cudaMemsetAsync(d.win_out, 0, sizeof(uint16_t) * (size_t)d.max_windows * np, bst),
                            "memset windows"));
+    if (h->nx) {
+        NET_TRY(cuda_error(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h->nx, bst), "memset xsyn"));
+        NET_TRY(cuda_error(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h->D * d.xwords, bst),
+                           "memset xsyn arrivals"));
+    }
     NET_TRY(sg.close());
     tp[6] = now_ms();
     if (dbg)
@@ -809,6 +852,10 @@ ne2b_status Engine::reset_net(uint32_t slot) {
     NE2B_CUDA(cudaMemsetAsync(d.ring, 0, sizeof(uint32_t) * (size_t)h.D * h.n_pad, stream_));
     if (d.rec_bits) NE2B_CUDA(cudaMemsetAsync(d.rec_bits, 0, sizeof(uint32_t) * (size_t)d.rec_rows * (h.n_pad / 32), stream_));
     if (d.win_out) NE2B_CUDA(cudaMemsetAsync(d.win_out, 0, sizeof(uint16_t) * (size_t)d.max_windows * h.n_pad, stream_));
+    if (h.nx) {
+        NE2B_CUDA(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h.nx, stream_));
+        NE2B_CUDA(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h.D * d.xwords, stream_));
+    }
     NE2B_CUDA(cudaMemsetAsync(d_counters_ + slot, 0, sizeof(NetCounters), stream_));
     h.t = 0;
     d.t = 0;
@@ -1099,6 +1146,8 @@ ne2b_status Engine::snapshot(EngineSnapshot &snap) {
         NE2B_TRY(grab(d.rec_bits, d.rec_bits ? 4 * (size_t)d.rec_rows * (np / 32) : 0));
         NE2B_TRY(grab(d.wcount, d.wcount ? 4 * np : 0));
         NE2B_TRY(grab(d.win_out, d.win_out ? 2 * (size_t)d.max_windows * np : 0));
+        NE2B_TRY(grab(d.xsyn, 4 * (size_t)h->nx));
+        NE2B_TRY(grab(d.xpend, 4 * (size_t)h->D * d.xwords));
         snap.hosts.push_back({h->slot, h->t, h->dev});
     }
     return NE2B_OK;

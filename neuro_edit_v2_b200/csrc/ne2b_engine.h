@@ -40,6 +40,7 @@ struct NetHost {
     uint32_t slot = 0;        // index in the engine's net array
     uint32_t n = 0, n_pad = 0, D = 0, n_inputs = 0;
     uint64_t e = 0;
+    uint32_t nx = 0;          // synapses with their own tau (XSyn)
     uint64_t t = 0;           // host mirror of dev.t
     uint64_t t_end = ~0ull;
     uint64_t dev_bytes = 0;

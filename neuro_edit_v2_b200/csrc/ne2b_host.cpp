@@ -23,6 +23,7 @@ struct ne2b_net {
     std::vector<uint32_t> src_ptr, tgt;
     std::vector<float> w;
     std::vector<uint16_t> delay;
+    std::vector<float> tau;  // per-synapse tau in ms (empty: none is custom)
     uint32_t n_inputs = 0;
     std::vector<uint32_t> stim_ptr, stim_input;
     std::vector<float> stim_w;
@@ -172,12 +173,12 @@ ne2b_status ne2b_net_from_synapses(uint32_t n, const uint8_t *model, const float
         net->tgt.resize(n_syn);
         net->w.resize(n_syn);
         net->delay.resize(n_syn);
+        bool any_tau = false;
+        for (uint64_t j = 0; tau_ms && j < n_syn && !any_tau; ++j) any_tau = tau_ms[j] > 0.0f;
+        if (any_tau) net->tau.resize(n_syn);
         for (uint64_t j = 0; j < n_syn; ++j) {
-            if (tau_ms && tau_ms[j] > 0.0f) {
-                delete net;
-                return set_error(NE2B_UNSUPPORTED, "per-synapse tau is not supported by this backend");
-            }
             const uint32_t p = fill[src[j]]++;
+            if (any_tau) net->tau[p] = tau_ms[j];  // network.rs:673 (tau travels with its synapse)
             net->tgt[p] = tgt[j];
             const float m = fabsf(w[j]);
             net->w[p] = kind[src[j]] == 1 ? -m : m;  // Dale's law, network.rs:668-672
@@ -371,7 +372,7 @@ ne2b_status ne2b_net_desc_of(const ne2b_net *net, ne2b_net_desc *d) {
     d->tgt = net->tgt.data();
     d->w = net->w.data();
     d->delay_steps = net->delay.data();
-    d->tau_ms = nullptr;
+    d->tau_ms = net->tau.empty() ? nullptr : net->tau.data();
     d->n_inputs = net->n_inputs;
     d->stim_ptr = net->n_inputs ? net->stim_ptr.data() : nullptr;
     d->stim_input = net->stim_input.data();

@@ -31,6 +31,7 @@ enum NetFlags : uint32_t {
     kNetWindows = 1u << 3,
     kNetActive = 1u << 4,
     kNetHasAdex = 1u << 5,  // at least one AdEx neuron
+    kNetXsyn = 1u << 6,     // some synapses have their own tau (XSyn)
 };
 
 enum TileFlags : uint32_t {
@@ -53,6 +54,7 @@ struct alignas(16) Tile {
 };
 
 constexpr uint16_t kTraceZero = 0xFFFFu;  // tk value of a zero trace
+constexpr uint32_t kNoXsyn = 0xFFFFFFFFu;  // xmap value of a synapse on the merged ring
 constexpr uint32_t kParamAdexBit = 0x8000u;  // pidx bit: the row is an AdEx row
 constexpr uint32_t kSmemParamRows = 32;      // param tables up to this size are staged in shared memory
 
@@ -82,6 +84,14 @@ struct alignas(16) NetDev {
     // spike record + windows
     uint32_t *rec_bits;     // [rec_rows x n_pad/32]
     uint16_t *win_out;      // [max_windows x n_pad]
+    // synapses with their own tau (sim/src/state.rs:231-275), kNetXsyn only
+    const uint32_t *xmap;   // [E] custom-synapse id of CSR synapse j, or kNoXsyn
+    const uint32_t *xt_ptr; // [n+1] each target's range in xt_idx
+    const uint32_t *xt_idx; // [nx] custom-synapse ids grouped by target, CSR order within
+    float *xsyn;            // [nx] each custom synapse's current
+    const float *xdecay;    // [nx] exp(-dt / tau)
+    const float *xw;        // [nx] arrival weight (rt_get(rt_put(w)) with the int ring)
+    uint32_t *xpend;        // [D x xwords] arrival bits: bit k of slot s = synapse k arrives at s
     // scalars
     unsigned long long t;       // step index of the next launch group's k = 0
     unsigned long long t_end;   // steps at or beyond this are skipped (serving)
@@ -92,7 +102,7 @@ struct alignas(16) NetDev {
     uint32_t rec_rows, win_steps, max_windows, flags;
     float dt, pkick, kick, decay_s, decay_t, gauss_k;
     uint32_t trace_last;  // last index of trace_tab (saturation)
-    uint32_t pad[1];
+    uint32_t xwords;      // ceil(nx / 32)
 };
 
 // Mutable per-net counters, kept apart from the read-mostly descriptor.

@@ -80,6 +80,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     const bool has_ext = flags & kNetHasExt;
     const bool has_stim = tile.flags & kTileHasStim;
     const bool windows = flags & kNetWindows;
+    const bool xsyn_on = flags & kNetXsyn;
     bool win_end = false;
     uint32_t widx = 0;
     if (windows) {
@@ -132,6 +133,25 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         if (rw[q] != 0u) ringw[slot_off + i] = 0u;
         const float sv = __fadd_rn(s[q], arr);
         float I = __fadd_rn(sv, ex[q]);
+        if (xsyn_on) {
+            // synapses with their own tau (cpu.rs:206-228): an arrival due
+            // this step (its bit in this slot's words) adds w, then the
+            // current joins the input and decays; a synapse arrives at most
+            // once per step, so arrivals commute and fold into this loop
+            uint32_t *pend = nd.xpend + (size_t)tmod * nd.xwords;
+            for (uint32_t j = nd.xt_ptr[i], je = nd.xt_ptr[i + 1]; j < je; ++j) {
+                const uint32_t k = nd.xt_idx[j];
+                const uint32_t bit = 1u << (k & 31u);
+                float x = nd.xsyn[k];
+                const uint32_t word = RES ? __ldcg(pend + (k >> 5)) : pend[k >> 5];
+                if (word & bit) {
+                    x = __fadd_rn(x, nd.xw[k]);
+                    atomicAnd(pend + (k >> 5), ~bit);  // other bits of the word belong to other targets
+                }
+                I = __fadd_rn(I, x);
+                nd.xsyn[k] = __fmul_rn(x, nd.xdecay[k]);
+            }
+        }
         if (has_stim) {
             // the host provides the [steps x inputs] values covering every
             // launched step; the range check only guards the read
@@ -284,6 +304,13 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
         uint32_t slot = tmod + d;
         if (slot >= D) slot -= D;
+        if (xsyn_on) {
+            const uint32_t k = nd.xmap[j];
+            if (k != kNoXsyn) {  // its own current: mark the arrival (cpu.rs:270-273)
+                atomicOr(nd.xpend + (size_t)slot * nd.xwords + (k >> 5), 1u << (k & 31u));
+                continue;
+            }
+        }
         const size_t idx = (size_t)slot * n_pad + tg;
         if (INT) {
             atomicAdd((int *)ringw + idx, ((const int *)nd.w)[j]);

@@ -35,6 +35,7 @@ class FlatNet:
     stim_w: np.ndarray | None = None       # f32[entries]
     x0: np.ndarray | None = None           # f32[n, 2]
     kind: np.ndarray | None = None         # u8[n] (0 exc, 1 inh, 2 regular)
+    tau_ms: np.ndarray | None = None       # f32[E]: > 0 gives the synapse its own current (XSyn)
     _desc: _abi.NetDesc | None = field(default=None, repr=False)
 
     def __post_init__(self):
@@ -47,7 +48,7 @@ class FlatNet:
         self.w = np.ascontiguousarray(self.w, dtype=np.float32)
         self.delay_steps = np.ascontiguousarray(self.delay_steps, dtype=np.uint16)
         for name, dt in (("stim_ptr", np.uint32), ("stim_input", np.uint32), ("stim_w", np.float32),
-                         ("x0", np.float32), ("kind", np.uint8)):
+                         ("x0", np.float32), ("kind", np.uint8), ("tau_ms", np.float32)):
             v = getattr(self, name)
             if v is not None:
                 setattr(self, name, np.ascontiguousarray(v, dtype=dt))
@@ -72,7 +73,7 @@ class FlatNet:
         d.tgt = ptr(self.tgt)
         d.w = ptr(self.w)
         d.delay_steps = ptr(self.delay_steps)
-        d.tau_ms = None
+        d.tau_ms = ptr(self.tau_ms) if self.tau_ms is not None else None
         d.n_inputs = self.n_inputs
         d.stim_ptr = ptr(self.stim_ptr) if self.n_inputs else None
         d.stim_input = ptr(self.stim_input) if self.n_inputs else None
@@ -141,6 +142,7 @@ class NativeNet:
             tgt=arr(d.tgt, e, C.c_uint32, np.uint32),
             w=arr(d.w, e, C.c_float, np.float32),
             delay_steps=arr(d.delay_steps, e, C.c_uint16, np.uint16),
+            tau_ms=arr(d.tau_ms, e, C.c_float, np.float32) if d.tau_ms else None,
             n_inputs=ni,
             stim_ptr=sp,
             stim_input=arr(d.stim_input, ne, C.c_uint32, np.uint32) if ni else None,

@@ -380,6 +380,9 @@ class Server:
     def synchronize(self) -> None:
         check(lib.ne2b_server_synchronize(self._h))
 
+    def set_tile_shape(self, block: int, npt: int, blocks_per_sm: int = 0) -> None:
+        check(lib.ne2b_server_set_tile_shape(self._h, block, npt, blocks_per_sm))
+
     def finished(self) -> list[int]:
         """Finished requests whose results are ready to take."""
         cnt = C.c_uint32()

@@ -273,9 +273,10 @@ class ONet:
         c = self.csr(dt_ms)
         model, params = self.models()
         ni, ptr, inp, w = self.stim_map()
+        tau = c["tau"] if c["tau"] is not None and np.any(c["tau"] > 0) else None
         return FlatNet(model=model, params=params, src_ptr=c["src_ptr"], tgt=c["tgt"], w=c["w"],
                        delay_steps=c["delay"], n_inputs=ni, stim_ptr=ptr if ni else None,
-                       stim_input=inp if ni else None, stim_w=w if ni else None, kind=self.kinds())
+                       stim_input=inp if ni else None, stim_w=w if ni else None, kind=self.kinds(), tau_ms=tau)
 
 
 class OSim:

@@ -49,6 +49,9 @@ def _same_flat(a, b):
     assert np.array_equal(a.model, b.model)
     assert np.array_equal(a.params[:, :10].view(np.uint32), b.params[:, :10].view(np.uint32))
     assert a.n_inputs == b.n_inputs
+    assert (a.tau_ms is None) == (b.tau_ms is None)
+    if a.tau_ms is not None:
+        assert np.array_equal(a.tau_ms.view(np.uint32), b.tau_ms.view(np.uint32))
     if a.n_inputs:
         assert np.array_equal(a.stim_ptr, b.stim_ptr)
         assert np.array_equal(a.stim_input, b.stim_input)
@@ -82,6 +85,25 @@ def test_csr_build_matches_oracle():
     model, params = net.models()
     prod = nb.from_synapses(model, params, net.kinds(), src, tgt, w, d, 0.1).arrays()
     _same_flat(prod, net.flat())
+
+
+def test_csr_build_keeps_per_synapse_tau_in_csr_order():
+    """tau travels with its synapse through the stable sort (network.rs:673)."""
+    net = O.ONet()
+    r = O.rng(5)
+    m = net.create_2d_grid(6, 6, 30.0)
+    net.set_exc_inh(m, 0.3, r)
+    net.create_connections(m, 0.35, 80.0, 6.0, r)
+    rng = np.random.default_rng(1)
+    for _ in range(200):
+        net.push_synapse(int(rng.integers(36)), int(rng.integers(36)), 2.0, float(rng.uniform(0.1, 5.0)),
+                         float(rng.uniform(1.0, 20.0)))
+    src, tgt, w, d, tau = net.synapses()
+    model, params = net.models()
+    prod = nb.from_synapses(model, params, net.kinds(), src, tgt, w, d, 0.1, tau_ms=tau).arrays()
+    flat = net.flat()
+    assert flat.tau_ms is not None
+    _same_flat(prod, flat)
 
 
 def test_csr_build_rejects_delay_overflow():

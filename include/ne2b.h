@@ -272,6 +272,28 @@ ne2b_status ne2b_net_from_synapses(uint32_t n, const uint8_t *model, const float
                                    const uint32_t *src, const uint32_t *tgt, const float *w,
                                    const float *delay_ms, const float *tau_ms, float dt_ms,
                                    ne2b_net **out);
+/* The reference's `.ne2` network files (net-format/src/io.rs:427-467 load):
+ * format versions 1-7, checked by the rules of Network::validate
+ * (network.rs:1007-1236), then built as Sim::new sees the network: model
+ * rows by NeuronParams::from_network (sim/src/state.rs:98-153; models "izh"
+ * and "adex", others NE2B_UNSUPPORTED), the CSR of Network::synapse_csr at
+ * the file's dt, per-synapse tau kept, stimulus routing by
+ * StimMap::from_network (stim.rs:26-48).  `meta` (may be NULL) receives the
+ * file's Meta (network.rs:381-392) for the sim config.  A malformed file is
+ * NE2B_EINVAL with the decoder's message. */
+typedef struct {
+    uint32_t version;
+    float dt_ms;
+    uint64_t seed;
+    float conduction_speed;
+    float synapse_tau_ms;
+    float readout_tau_ms;
+    float noise_rate_hz;
+    float noise_kick_mv;
+    uint32_t n_types, n_groups, n_samples, n_readouts, n_scripts;
+} ne2b_ne2_meta;
+ne2b_status ne2b_net_load_ne2(const char *path, ne2b_net **out, ne2b_ne2_meta *meta);
+ne2b_status ne2b_net_from_ne2(const uint8_t *bytes, uint64_t len, ne2b_net **out, ne2b_ne2_meta *meta);
 /* Random K-out workload net (10k/100k/1M configurations). */
 ne2b_status ne2b_gen_random_kout(uint32_t n, uint32_t k, uint64_t seed, float w_scale, float exc_hi,
                                  float inh_hi, float delay_cap_ms, float dt_ms, ne2b_net **out);

@@ -10,12 +10,13 @@ fails loudly if it is missing.
 from . import _abi
 from ._abi import (KERNEL_AUTO, KERNEL_RESIDENT, KERNEL_STREAM, MODEL_ADEX, MODEL_IZH, Config, Ne2bError,
                    default_config)
-from .net import FlatNet, NativeNet, from_synapses, liquid, random_kout, to_adex
+from .net import (FlatNet, NativeNet, config_from_meta, from_ne2_bytes, from_synapses, liquid, load_ne2, random_kout,
+                  to_adex)
 from .sim import B200Sim, Batch, Server, SpikeWindowError, footprint
 
 __all__ = [
     "B200Sim", "Batch", "Server", "SpikeWindowError", "footprint", "FlatNet", "NativeNet", "from_synapses",
-    "liquid", "random_kout", "to_adex", "Config", "default_config", "Ne2bError", "MODEL_IZH", "MODEL_ADEX",
+    "liquid", "random_kout", "to_adex", "load_ne2", "from_ne2_bytes", "config_from_meta", "Config", "default_config", "Ne2bError", "MODEL_IZH", "MODEL_ADEX",
     "KERNEL_AUTO", "KERNEL_STREAM", "KERNEL_RESIDENT",
     "expf",
 ]

@@ -33,6 +33,25 @@ KERNEL_STREAM = 1
 KERNEL_RESIDENT = 2
 
 
+class Ne2Meta(C.Structure):
+    """ne2b_ne2_meta: a .ne2 file's version and Meta (network.rs:381-392)."""
+    _fields_ = [
+        ("version", C.c_uint32),
+        ("dt_ms", C.c_float),
+        ("seed", C.c_uint64),
+        ("conduction_speed", C.c_float),
+        ("synapse_tau_ms", C.c_float),
+        ("readout_tau_ms", C.c_float),
+        ("noise_rate_hz", C.c_float),
+        ("noise_kick_mv", C.c_float),
+        ("n_types", C.c_uint32),
+        ("n_groups", C.c_uint32),
+        ("n_samples", C.c_uint32),
+        ("n_readouts", C.c_uint32),
+        ("n_scripts", C.c_uint32),
+    ]
+
+
 class NetDesc(C.Structure):
     _fields_ = [
         ("n", C.c_uint32),
@@ -187,6 +206,8 @@ _SIGS = {
     "ne2b_server_stats": (C.c_int, [_p, _pu64, _pu64, _pu32, _pu64, _pu64]),
     "ne2b_net_from_synapses": (C.c_int, [_u32, _p, _p, _u32, _p, _u64, _p, _p, _p, _p, _p, _f32, C.POINTER(_p)]),
     "ne2b_gen_random_kout": (C.c_int, [_u32, _u32, _u64, _f32, _f32, _f32, _f32, _f32, C.POINTER(_p)]),
+    "ne2b_net_load_ne2": (C.c_int, [C.c_char_p, C.POINTER(_p), _p]),
+    "ne2b_net_from_ne2": (C.c_int, [_p, _u64, C.POINTER(_p), _p]),
     "ne2b_gen_liquid": (C.c_int, [_u32, _u64, _f64, _i32, _f32, _u32, _u32, _f32, _i32, _f32, C.POINTER(_p)]),
     "ne2b_net_set_model_all": (C.c_int, [_p, _i32, _p, _p, _u32]),
     "ne2b_net_desc_of": (C.c_int, [_p, C.POINTER(NetDesc)]),

@@ -9,25 +9,12 @@
 #include <vector>
 
 #include "../../include/ne2b.h"
+#include "ne2b_net.h"
 
 namespace ne2b {
 ne2b_status set_error(ne2b_status st, const char *fmt, ...);
 }
 using ne2b::set_error;
-
-struct ne2b_net {
-    uint32_t n = 0;
-    std::vector<uint8_t> model, kind;
-    std::vector<float> params;  // n * 10
-    std::vector<float> pos;     // n * 3
-    std::vector<uint32_t> src_ptr, tgt;
-    std::vector<float> w;
-    std::vector<uint16_t> delay;
-    std::vector<float> tau;  // per-synapse tau in ms (empty: none is custom)
-    uint32_t n_inputs = 0;
-    std::vector<uint32_t> stim_ptr, stim_input;
-    std::vector<float> stim_w;
-};
 
 namespace {
 
@@ -106,6 +93,10 @@ float delay_ms(const ne2b_net &net, uint32_t a, uint32_t b, float speed) {
 }
 
 // network.rs:674-685: steps = max(1, round(delay/dt)); > u16 is an error
+}  // namespace
+
+namespace ne2b_hostnet {
+
 bool delay_steps(float ms, float dt, uint16_t *out) {
     float st = roundf(ms / dt);
     if (st < 1.0f) st = 1.0f;
@@ -134,6 +125,12 @@ void build_stim(ne2b_net &net, const std::vector<std::vector<std::pair<uint32_t,
             net.stim_w[p] = tw.second;
         }
 }
+
+}  // namespace ne2b_hostnet
+
+namespace {
+using ne2b_hostnet::build_stim;
+using ne2b_hostnet::delay_steps;
 
 }  // namespace
 

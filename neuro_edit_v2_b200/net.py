@@ -13,6 +13,7 @@ generators and the CSR build).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -185,6 +186,37 @@ def liquid(side: int, seed: int = 1, lambda_units: float = 2.0, radius_units: in
     check(lib.ne2b_gen_liquid(side, seed, lambda_units, radius_units, w_rec, n_inputs, targets_per_input, w_in,
                               model, dt_ms, C.byref(h)))
     return NativeNet(h)
+
+
+def _meta_dict(m: _abi.Ne2Meta) -> dict:
+    return {f: getattr(m, f) for f, _ in m._fields_}
+
+
+def load_ne2(path) -> tuple[NativeNet, dict]:
+    """A reference `.ne2` network file (versions 1-7) as a library net, and
+    the file's version and Meta (dt_ms, seed, conduction_speed,
+    synapse_tau_ms, readout_tau_ms, noise_rate_hz, noise_kick_mv)."""
+    h = C.c_void_p()
+    m = _abi.Ne2Meta()
+    check(lib.ne2b_net_load_ne2(os.fsencode(path), C.byref(h), C.byref(m)))
+    return NativeNet(h), _meta_dict(m)
+
+
+def from_ne2_bytes(data: bytes) -> tuple[NativeNet, dict]:
+    """`load_ne2` from the file's bytes."""
+    buf = (C.c_uint8 * len(data)).from_buffer_copy(data) if data else None
+    h = C.c_void_p()
+    m = _abi.Ne2Meta()
+    check(lib.ne2b_net_from_ne2(buf, len(data), C.byref(h), C.byref(m)))
+    return NativeNet(h), _meta_dict(m)
+
+
+def config_from_meta(meta: dict, **overrides) -> _abi.Config:
+    """The sim config a `.ne2` file asks for (its Meta), as Sim::new builds it."""
+    kw = dict(dt_ms=meta["dt_ms"], synapse_tau_ms=meta["synapse_tau_ms"], readout_tau_ms=meta["readout_tau_ms"],
+              noise_rate_hz=meta["noise_rate_hz"], noise_kick_mv=meta["noise_kick_mv"], seed=meta["seed"])
+    kw.update(overrides)
+    return _abi.default_config(**kw)
 
 
 ADEX_TONIC = np.array([281.0, 30.0, -70.6, -50.4, 2.0, 4.0, 144.0, 80.5, -70.6, 20.0], dtype=np.float32)

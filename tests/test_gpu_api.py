@@ -183,3 +183,39 @@ def test_sim_autotune_restores_state_and_keeps_results():
     assert np.array_equal(a.v().view(np.uint32), b.v().view(np.uint32))
     assert np.array_equal(a.trace().view(np.uint32), b.trace().view(np.uint32))
     assert np.array_equal(a.spike_counts(512), b.spike_counts(512))
+
+
+def test_ne2_file_runs_bit_exact_against_oracle():
+    """A `.ne2` file (written by tests/ne2_writer.py from an oracle net, v7)
+    loaded by the library and run on the GPU equals the oracle run of the
+    same net, with the file's Meta as the config."""
+    import ne2_writer as W
+    from helpers import assert_state_bits_equal, lockstep
+
+    onet = O.ONet()
+    r = O.rng(8)
+    m = onet.create_3d_grid(8, 8, 8, 60.0)
+    onet.set_exc_inh(m, 0.2, r)
+    onet.create_connections(m, 1.0, 120.0, 3.0, r)
+    rng = np.random.default_rng(2)
+    for _ in range(300):
+        onet.push_synapse(int(rng.integers(512)), int(rng.integers(512)), 3.0, float(rng.uniform(0.1, 9.0)),
+                          float(rng.uniform(1.0, 25.0)))
+    inputs = [("in0", [(int(t), 12.0) for t in rng.integers(0, 512, 24)])]
+    for _, tw in inputs:
+        onet.add_input(tw)
+    desc = W.from_onet(onet, inputs)
+    desc["meta"].update(noise_rate_hz=200.0, noise_kick_mv=15.0, seed=21)
+    net, meta = nb.from_ne2_bytes(W.encode(desc, 7))
+    cfg = nb.config_from_meta(meta)
+    series = (rng.random(1200) < 0.05).astype(np.float32)
+
+    def drive(s):
+        s.play_input(0, series)
+
+    g, o, first = lockstep(onet, 1200, int_weights=True, chunk=100, flat=net.arrays(), drive=drive,
+                           noise_rate_hz=cfg.noise_rate_hz, noise_kick_mv=cfg.noise_kick_mv, seed=cfg.seed,
+                           synapse_tau_ms=cfg.synapse_tau_ms, readout_tau_ms=cfg.readout_tau_ms)
+    assert first < 0, f"raster diverged at step {first}"
+    assert o.spikes_total() > 0
+    assert_state_bits_equal(g, o)

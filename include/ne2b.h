@@ -167,10 +167,22 @@ ne2b_status ne2b_set_tile_shape(ne2b_sim *sim, uint32_t block, uint32_t neurons_
 ne2b_status ne2b_stream(ne2b_sim *sim, void **stream);
 ne2b_status ne2b_kernel_launches(ne2b_sim *sim, uint64_t *launches);
 
-/* Editor observability (lib.rs:164-176): not provided by this backend. */
+/* Editor observability (lib.rs:164-176; cpu.rs:308-407).
+ * set_v_watch: the neurons whose state slots 0 and 1 are recorded after
+ * every step (an id beyond n records 0); a new list starts an empty
+ * history, the same list keeps it; the last 4096 samples are kept.
+ * watch_count: the watch count and the samples drain_watch would return.
+ * drain_watch: out = [slot 0..1][watch][samples], oldest first, sized by
+ * watch_count; empties the history.  set_grid_watches: member lists in
+ * texel order (members[group_ptr[g] .. group_ptr[g+1]]); grid_traces: one
+ * value per texel, groups concatenated, exp(-(t - last spike) * dt / tau)
+ * and 0 for a texel that never spiked.  reset_state clears both. */
 ne2b_status ne2b_set_v_watch(ne2b_sim *sim, const uint32_t *ids, uint32_t count);
+ne2b_status ne2b_watch_count(ne2b_sim *sim, uint32_t *watches, uint32_t *samples);
+ne2b_status ne2b_drain_watch(ne2b_sim *sim, float *out, uint32_t *samples);
 ne2b_status ne2b_set_grid_watches(ne2b_sim *sim, const uint32_t *members, const uint32_t *group_ptr,
                                   uint32_t groups);
+ne2b_status ne2b_grid_traces(ne2b_sim *sim, float tau_ms, float *out);
 
 /* ---------------------------------------------------------------- batch */
 /* Many independent networks of uneven size stepped together: one

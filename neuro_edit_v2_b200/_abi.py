@@ -180,6 +180,9 @@ _SIGS = {
     "ne2b_server_kernel_launches": (C.c_int, [_p, _pu64]),
     "ne2b_set_v_watch": (C.c_int, [_p, _p, _u32]),
     "ne2b_set_grid_watches": (C.c_int, [_p, _p, _p, _u32]),
+    "ne2b_watch_count": (C.c_int, [_p, C.POINTER(_u32), C.POINTER(_u32)]),
+    "ne2b_drain_watch": (C.c_int, [_p, _p, C.POINTER(_u32)]),
+    "ne2b_grid_traces": (C.c_int, [_p, _f32, _p]),
     "ne2b_batch_create": (C.c_int, [C.POINTER(NetDesc), C.POINTER(Config), _u32, C.c_int, C.POINTER(_p)]),
     "ne2b_batch_destroy": (C.c_int, [_p]),
     "ne2b_batch_play_input": (C.c_int, [_p, _u32, _u32, _p, _u64]),

@@ -330,14 +330,33 @@ ne2b_status ne2b_kernel_launches(ne2b_sim *sim, uint64_t *launches) {
 }
 
 ne2b_status ne2b_set_v_watch(ne2b_sim *sim, const uint32_t *ids, uint32_t count) {
-    (void)sim; (void)ids; (void)count;
-    return set_error(NE2B_UNSUPPORTED, "v-watch recording is not provided by the B200 backend");
+    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
+    GUARD(sim->eng.set_v_watch(*sim->eng.net(sim->slot), ids, count));
+}
+
+ne2b_status ne2b_watch_count(ne2b_sim *sim, uint32_t *watches, uint32_t *samples) {
+    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
+    NetHost &h = *sim->eng.net(sim->slot);
+    const uint64_t span = h.t - std::min(h.watch_t0, h.t);
+    if (watches) *watches = (uint32_t)h.watch_ids.size();
+    if (samples) *samples = (uint32_t)std::min<uint64_t>(span, ne2b::kWatchCap);
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_drain_watch(ne2b_sim *sim, float *out, uint32_t *samples) {
+    if (!sim || !samples) return set_error(NE2B_EINVAL, "null argument");
+    GUARD(sim->eng.drain_watch(*sim->eng.net(sim->slot), out, samples));
 }
 
 ne2b_status ne2b_set_grid_watches(ne2b_sim *sim, const uint32_t *members, const uint32_t *group_ptr,
                                   uint32_t groups) {
-    (void)sim; (void)members; (void)group_ptr; (void)groups;
-    return set_error(NE2B_UNSUPPORTED, "grid traces are not provided by the B200 backend");
+    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
+    GUARD(sim->eng.set_grid_watches(*sim->eng.net(sim->slot), members, group_ptr, groups));
+}
+
+ne2b_status ne2b_grid_traces(ne2b_sim *sim, float tau_ms, float *out) {
+    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
+    GUARD(sim->eng.grid_traces(*sim->eng.net(sim->slot), tau_ms, out));
 }
 
 // ----------------------------------------------------------------- batch

@@ -86,6 +86,8 @@ Engine::~Engine() {
     for (NetHost *h : nets_) {
         if (!h) continue;
         for (void *p : h->allocs) cudaFreeAsync(p, stream_);
+        for (void *p : h->watch_allocs) cudaFreeAsync(p, stream_);
+        for (void *p : h->gw_allocs) cudaFreeAsync(p, stream_);
         delete h;
     }
     if (stream_) cudaStreamSynchronize(stream_);
@@ -669,6 +671,8 @@ ne2b_status Engine::remove_net(uint32_t slot, bool rebuild, const void *keep) {
     NE2B_CUDA(cudaMemcpyAsync(d_nets_ + slot, &z, sizeof z, cudaMemcpyHostToDevice, stream_));
     for (void *p : h->allocs)
         if (p != keep) NE2B_CUDA(cudaFreeAsync(p, stream_));
+    for (void *p : h->watch_allocs) NE2B_CUDA(cudaFreeAsync(p, stream_));
+    for (void *p : h->gw_allocs) NE2B_CUDA(cudaFreeAsync(p, stream_));
     nets_[slot] = nullptr;
     delete h;
     return rebuild ? rebuild_tiles() : NE2B_OK;
@@ -856,6 +860,9 @@ ne2b_status Engine::reset_net(uint32_t slot) {
         NE2B_CUDA(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h.nx, stream_));
         NE2B_CUDA(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h.D * d.xwords, stream_));
     }
+    // cpu.rs:176-183: the watch history and the grid marks start over
+    h.watch_t0 = 0;
+    if (d.gw_ls) NE2B_CUDA(cudaMemsetAsync(d.gw_ls, 0xFF, sizeof(uint32_t) * std::max<uint32_t>(h.gw_ptr.back(), 1), stream_));
     NE2B_CUDA(cudaMemsetAsync(d_counters_ + slot, 0, sizeof(NetCounters), stream_));
     h.t = 0;
     d.t = 0;
@@ -1118,6 +1125,138 @@ ne2b_status Engine::refresh_noise(NetHost &h) {
     return upload_net(h);
 }
 
+// cpu.rs:330-338: a new list starts an empty history; the same list keeps it.
+// Each distinct id below n gets a ring row; an id beyond n records 0.
+ne2b_status Engine::set_v_watch(NetHost &h, const uint32_t *ids, uint32_t count) {
+    if (count && !ids) return set_error(NE2B_EINVAL, "null ids");
+    if (count == h.watch_ids.size() && std::equal(h.watch_ids.begin(), h.watch_ids.end(), ids)) return NE2B_OK;
+    NE2B_CUDA(cudaStreamSynchronize(stream_));  // no launch in flight writes the old ring
+    for (void *p : h.watch_allocs) NE2B_CUDA(cudaFreeAsync(p, stream_));
+    h.watch_allocs.clear();
+    h.watch_ids.assign(ids, ids + count);
+    h.watch_row.assign(count, -1);
+    std::vector<uint32_t> idx(h.n_pad, kNoWatch);
+    uint32_t rows = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t i = ids[k];
+        if (i >= h.n) continue;
+        if (idx[i] == kNoWatch) idx[i] = rows++;
+        h.watch_row[k] = (int32_t)idx[i];
+    }
+    h.watch_t0 = h.t;
+    h.dev.watch_idx = nullptr;
+    h.dev.watch_ring = nullptr;
+    h.dev.watch_n = rows;
+    h.dev.flags &= ~kNetWatch;
+    if (rows) {
+        void *p = nullptr;
+        NE2B_CUDA(cudaMallocAsync(&p, sizeof(uint32_t) * h.n_pad, stream_));
+        h.watch_allocs.push_back(p);
+        NE2B_TRY(pin_copy(p, idx.data(), sizeof(uint32_t) * h.n_pad));
+        h.dev.watch_idx = (const uint32_t *)p;
+        NE2B_CUDA(cudaMallocAsync(&p, sizeof(float) * 2 * (size_t)rows * kWatchCap, stream_));
+        h.watch_allocs.push_back(p);
+        h.dev.watch_ring = (float *)p;
+        NE2B_TRY(pin_close());
+        h.dev.flags |= kNetWatch;
+    }
+    return upload_net(h);
+}
+
+// drain_state for both slots (cpu.rs:350-357): the samples of steps
+// [max(t0, t - kWatchCap), t), oldest first, then an empty history.
+ne2b_status Engine::drain_watch(NetHost &h, float *out, uint32_t *count) {
+    const uint64_t span = h.t - std::min(h.watch_t0, h.t);
+    const uint32_t c = (uint32_t)std::min<uint64_t>(span, kWatchCap);
+    const uint32_t w = (uint32_t)h.watch_ids.size();
+    *count = c;
+    if (c && w && out) {
+        std::vector<float> ring(2 * (size_t)h.dev.watch_n * kWatchCap);
+        if (h.dev.watch_n) {
+            NE2B_CUDA(cudaMemcpyAsync(ring.data(), h.dev.watch_ring, sizeof(float) * ring.size(),
+                                      cudaMemcpyDeviceToHost, stream_));
+            NE2B_CUDA(cudaStreamSynchronize(stream_));
+        }
+        const uint64_t first = h.t - c;
+        for (uint32_t slot = 0; slot < 2; ++slot)
+            for (uint32_t k = 0; k < w; ++k) {
+                float *o = out + ((size_t)slot * w + k) * c;
+                const int32_t row = h.watch_row[k];
+                for (uint32_t j = 0; j < c; ++j)
+                    o[j] = row < 0 ? 0.0f
+                                   : ring[((size_t)slot * h.dev.watch_n + (uint32_t)row) * kWatchCap +
+                                          ((first + j) & (kWatchCap - 1u))];
+            }
+    }
+    h.watch_t0 = h.t;
+    return NE2B_OK;
+}
+
+// cpu.rs:361-387: member lists in texel order (a neuron's texel is its
+// last position in the list); the same lists keep their marks.
+ne2b_status Engine::set_grid_watches(NetHost &h, const uint32_t *members, const uint32_t *group_ptr,
+                                     uint32_t ngroups) {
+    if (ngroups && !group_ptr) return set_error(NE2B_EINVAL, "null group_ptr");
+    const uint32_t total = ngroups ? group_ptr[ngroups] : 0;
+    if (total && !members) return set_error(NE2B_EINVAL, "null members");
+    for (uint32_t g = 0; g < ngroups; ++g)
+        if (group_ptr[g] > group_ptr[g + 1]) return set_error(NE2B_EINVAL, "group_ptr not monotone");
+    if (ngroups && group_ptr[0] != 0) return set_error(NE2B_EINVAL, "group_ptr[0] != 0");
+    const bool same = ngroups == 0 ? h.gw_ptr.empty()
+                                   : (h.gw_ptr.size() == (size_t)ngroups + 1 &&
+                                      std::equal(h.gw_ptr.begin(), h.gw_ptr.end(), group_ptr) &&
+                                      h.gw_members.size() == total &&
+                                      std::equal(h.gw_members.begin(), h.gw_members.end(), members));
+    if (same) return NE2B_OK;
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    for (void *p : h.gw_allocs) NE2B_CUDA(cudaFreeAsync(p, stream_));
+    h.gw_allocs.clear();
+    h.gw_ptr.assign(group_ptr, group_ptr + (ngroups ? ngroups + 1 : 0));
+    h.gw_members.assign(members, members + total);
+    h.dev.gw_map = nullptr;
+    h.dev.gw_off = nullptr;
+    h.dev.gw_ls = nullptr;
+    h.dev.gw_n = ngroups;
+    h.dev.flags &= ~kNetGridWatch;
+    if (ngroups) {
+        std::vector<int32_t> map((size_t)ngroups * h.n_pad, -1);
+        for (uint32_t g = 0; g < ngroups; ++g)
+            for (uint32_t k = group_ptr[g]; k < group_ptr[g + 1]; ++k)
+                if (members[k] < h.n) map[(size_t)g * h.n_pad + members[k]] = (int32_t)(k - group_ptr[g]);
+        void *p = nullptr;
+        NE2B_CUDA(cudaMallocAsync(&p, sizeof(int32_t) * map.size(), stream_));
+        h.gw_allocs.push_back(p);
+        NE2B_TRY(pin_copy(p, map.data(), sizeof(int32_t) * map.size()));
+        h.dev.gw_map = (const int32_t *)p;
+        NE2B_CUDA(cudaMallocAsync(&p, sizeof(uint32_t) * ((size_t)ngroups + 1), stream_));
+        h.gw_allocs.push_back(p);
+        NE2B_TRY(pin_copy(p, group_ptr, sizeof(uint32_t) * ((size_t)ngroups + 1)));
+        h.dev.gw_off = (const uint32_t *)p;
+        NE2B_CUDA(cudaMallocAsync(&p, sizeof(uint32_t) * std::max<uint32_t>(total, 1), stream_));
+        h.gw_allocs.push_back(p);
+        NE2B_CUDA(cudaMemsetAsync(p, 0xFF, sizeof(uint32_t) * std::max<uint32_t>(total, 1), stream_));
+        h.dev.gw_ls = (uint32_t *)p;
+        NE2B_TRY(pin_close());
+        h.dev.flags |= kNetGridWatch;
+    }
+    return upload_net(h);
+}
+
+// cpu.rs:391-407: exp(-(t - last) * dt / tau) per texel (f32, libm expf),
+// 0 for a texel that never spiked; groups concatenated in order.
+ne2b_status Engine::grid_traces(NetHost &h, float tau_ms, float *out) {
+    const uint32_t ng = h.gw_ptr.empty() ? 0 : (uint32_t)h.gw_ptr.size() - 1;
+    const uint32_t total = ng ? h.gw_ptr[ng] : 0;
+    if (!total) return NE2B_OK;
+    std::vector<uint32_t> ls(total);
+    NE2B_CUDA(cudaMemcpyAsync(ls.data(), h.dev.gw_ls, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, stream_));
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
+    const float k = h.cfg.dt_ms / (tau_ms > 1e-6f ? tau_ms : 1e-6f);
+    for (uint32_t j = 0; j < total; ++j)
+        out[j] = ls[j] == kNeverSpiked ? 0.0f : expf(-(float)(h.t > ls[j] ? h.t - ls[j] : 0) * k);
+    return NE2B_OK;
+}
+
 // Snapshot of every mutable device array (state, ring, record, windows,
 // descriptors, counters) in device memory, for the autotuner's trials.
 ne2b_status Engine::snapshot(EngineSnapshot &snap) {
@@ -1147,6 +1286,8 @@ ne2b_status Engine::snapshot(EngineSnapshot &snap) {
         NE2B_TRY(grab(d.wcount, d.wcount ? 4 * np : 0));
         NE2B_TRY(grab(d.win_out, d.win_out ? 2 * (size_t)d.max_windows * np : 0));
         NE2B_TRY(grab(d.xsyn, 4 * (size_t)h->nx));
+        NE2B_TRY(grab(d.watch_ring, d.watch_ring ? 8 * (size_t)d.watch_n * kWatchCap : 0));
+        NE2B_TRY(grab(d.gw_ls, d.gw_ls ? 4 * (size_t)std::max<uint32_t>(h->gw_ptr.back(), 1) : 0));
         NE2B_TRY(grab(d.xpend, 4 * (size_t)h->D * d.xwords));
         snap.hosts.push_back({h->slot, h->t, h->dev});
     }

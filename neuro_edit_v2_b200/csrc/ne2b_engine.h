@@ -51,6 +51,13 @@ struct NetHost {
     std::vector<uint32_t> stim_ptr_host;  // for tile flags
     std::vector<void *> allocs;
     std::vector<float> pack_buf;
+    // editor watches (cpu.rs:63-95)
+    std::vector<uint32_t> watch_ids;   // as set
+    std::vector<int32_t> watch_row;    // watch k -> ring row, -1 for an id beyond n (records 0)
+    uint64_t watch_t0 = 0;             // first step of the undrained history
+    std::vector<void *> watch_allocs;
+    std::vector<uint32_t> gw_ptr, gw_members;
+    std::vector<void *> gw_allocs;
     uint64_t build_launches = 0;  // kernels queued by build_net
 };
 
@@ -153,6 +160,11 @@ class Engine {
     ne2b_status set_ext(NetHost &h, const float *ext, uint32_t len);
     ne2b_status set_input_matrix(NetHost &h, const float *x, uint64_t steps);
     ne2b_status refresh_noise(NetHost &h);
+    // editor watches (lib.rs:164-176, cpu.rs:308-407)
+    ne2b_status set_v_watch(NetHost &h, const uint32_t *ids, uint32_t count);
+    ne2b_status drain_watch(NetHost &h, float *out, uint32_t *count);  // out: [2][nwatch][count]
+    ne2b_status set_grid_watches(NetHost &h, const uint32_t *members, const uint32_t *group_ptr, uint32_t ngroups);
+    ne2b_status grid_traces(NetHost &h, float tau_ms, float *out);
     ne2b_status snapshot(EngineSnapshot &snap);
     ne2b_status restore(const EngineSnapshot &snap);
     void drop(EngineSnapshot &snap);

@@ -32,6 +32,8 @@ enum NetFlags : uint32_t {
     kNetActive = 1u << 4,
     kNetHasAdex = 1u << 5,  // at least one AdEx neuron
     kNetXsyn = 1u << 6,     // some synapses have their own tau (XSyn)
+    kNetWatch = 1u << 7,    // watched neurons record their state every step
+    kNetGridWatch = 1u << 8,  // grid groups record each member's last spike step
 };
 
 enum TileFlags : uint32_t {
@@ -55,6 +57,9 @@ struct alignas(16) Tile {
 
 constexpr uint16_t kTraceZero = 0xFFFFu;  // tk value of a zero trace
 constexpr uint32_t kNoXsyn = 0xFFFFFFFFu;  // xmap value of a synapse on the merged ring
+constexpr uint32_t kWatchCap = 4096;       // samples kept per watched neuron (cpu.rs:78 V_HIST_CAP)
+constexpr uint32_t kNoWatch = 0xFFFFFFFFu; // watch_idx of an unwatched neuron
+constexpr uint32_t kNeverSpiked = 0xFFFFFFFFu;  // gw_ls of a texel that never spiked
 constexpr uint32_t kParamAdexBit = 0x8000u;  // pidx bit: the row is an AdEx row
 constexpr uint32_t kSmemParamRows = 32;      // param tables up to this size are staged in shared memory
 
@@ -92,6 +97,13 @@ struct alignas(16) NetDev {
     const float *xdecay;    // [nx] exp(-dt / tau)
     const float *xw;        // [nx] arrival weight (rt_get(rt_put(w)) with the int ring)
     uint32_t *xpend;        // [D x xwords] arrival bits: bit k of slot s = synapse k arrives at s
+    // editor watches (cpu.rs:63-95, 290-420), kNetWatch / kNetGridWatch only
+    const uint32_t *watch_idx;  // [n_pad] ring row of a watched neuron, or kNoWatch
+    float *watch_ring;          // [2][watch_n][kWatchCap] state slots after step t at t % kWatchCap
+    const int32_t *gw_map;      // [gw_n][n_pad] member-list position of neuron i in group g, or -1
+    const uint32_t *gw_off;     // [gw_n + 1] group ranges in gw_ls
+    uint32_t *gw_ls;            // last spike step per texel (min(t, 2^32-2)), kNeverSpiked
+    uint32_t watch_n, gw_n;
     // scalars
     unsigned long long t;       // step index of the next launch group's k = 0
     unsigned long long t_end;   // steps at or beyond this are skipped (serving)

@@ -200,6 +200,21 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             rlo[q] = rowptr[i];
             rhi[q] = rowptr[i + 1];
             nd.pn_total[i] += 1ull;
+            if (flags & kNetGridWatch) {  // cpu.rs:293-304
+                const uint32_t t32 = t < 0xFFFFFFFEull ? (uint32_t)t : 0xFFFFFFFEu;
+                for (uint32_t g = 0; g < nd.gw_n; ++g) {
+                    const int32_t k = nd.gw_map[(size_t)g * n_pad + i];
+                    if (k >= 0) nd.gw_ls[nd.gw_off[g] + (uint32_t)k] = t32;
+                }
+            }
+        }
+        if (flags & kNetWatch) {  // state after the step, cpu.rs:311-324
+            const uint32_t w = nd.watch_idx[i];
+            if (w != kNoWatch) {
+                const size_t pos = (size_t)(t & (kWatchCap - 1u));
+                nd.watch_ring[(size_t)w * kWatchCap + pos] = v[q];
+                nd.watch_ring[((size_t)nd.watch_n + w) * kWatchCap + pos] = u[q];
+            }
         }
         if (windows) {
             if (win_end) {

@@ -4,8 +4,7 @@ over the B200 C ABI.
 `B200Sim` exposes the same methods, argument meanings and error behaviour as
 `CpuSim` / `CudaSim` (sim/src/cpu.rs, sim/src/cuda.rs): stepping is
 asynchronous, every read synchronises, `spike_counts` raises on a window that
-the record ring can no longer answer, and editor-only calls (`set_v_watch`,
-`set_grid_watches`) are reported as unsupported.
+the record ring can no longer answer.
 """
 from __future__ import annotations
 
@@ -193,9 +192,33 @@ class B200Sim:
     def set_gauss_noise(self, sd: float) -> None:
         check(lib.ne2b_set_gauss_noise(self._h, sd))
 
+    # --- editor observability (lib.rs:164-176) --------------------------
     def set_v_watch(self, ids) -> None:
         a = np.ascontiguousarray(ids, dtype=np.uint32)
         check(lib.ne2b_set_v_watch(self._h, ptr(a), len(a)))
+
+    def drain_watch(self) -> np.ndarray:
+        """[state slot][watch][samples oldest first] since the last drain."""
+        w, c = C.c_uint32(), C.c_uint32()
+        check(lib.ne2b_watch_count(self._h, C.byref(w), C.byref(c)))
+        out = np.zeros(max(2 * w.value * c.value, 1), np.float32)
+        got = C.c_uint32()
+        check(lib.ne2b_drain_watch(self._h, ptr(out), C.byref(got)))
+        return out[: 2 * w.value * got.value].reshape(2, w.value, got.value)
+
+    def set_grid_watches(self, groups) -> None:
+        gp = np.zeros(len(groups) + 1, np.uint32)
+        gp[1:] = np.cumsum([len(g) for g in groups])
+        members = np.ascontiguousarray(np.concatenate([np.asarray(g, np.uint32) for g in groups])
+                                       if groups else np.zeros(0, np.uint32), dtype=np.uint32)
+        check(lib.ne2b_set_grid_watches(self._h, ptr(members), ptr(gp), len(groups)))
+        self._gw_ptr = gp
+
+    def grid_traces(self, tau_ms: float) -> list:
+        gp = getattr(self, "_gw_ptr", np.zeros(1, np.uint32))
+        out = np.zeros(max(int(gp[-1]), 1), np.float32)
+        check(lib.ne2b_grid_traces(self._h, tau_ms, ptr(out)))
+        return [out[gp[g]:gp[g + 1]].copy() for g in range(len(gp) - 1)]
 
     # --- kernel selection (new) -----------------------------------------
     def set_kernel_mode(self, mode: int) -> None:

@@ -599,6 +599,18 @@ struct ne2o_sim {
     uint64_t t, spikes_total;
     uint32_t *spiked;
     uint32_t nspiked;
+    /* editor watches (cpu.rs:63-95): per-step state of watched neurons,
+     * the last NE2O_V_HIST_CAP samples kept (a ring, oldest at hist_head),
+     * and per grid group the last spike step of every texel */
+    uint32_t nwatch;
+    uint32_t *v_watch;
+    float *x_hist;  /* [2][nwatch][NE2O_V_HIST_CAP] */
+    uint32_t hist_head, hist_len;
+    uint32_t ngw;
+    uint32_t *gw_ptr;     /* [ngw+1] member ranges */
+    uint32_t *gw_members; /* texel order */
+    int32_t *gw_map;      /* [ngw][n] texel of neuron, -1 if none */
+    uint32_t *gw_ls;      /* [gw_ptr[ngw]] last spike step, UINT32_MAX never */
 };
 
 static void sim_free_parts(ne2o_sim *s) {
@@ -611,6 +623,7 @@ static void sim_free_parts(ne2o_sim *s) {
     free(s->series);
     free(s->x); free(s->s); free(s->trace); free(s->ext); free(s->ring); free(s->iring);
     free(s->spike_bits); free(s->spike_counts); free(s->pn_total); free(s->spiked);
+    free(s->v_watch); free(s->x_hist); free(s->gw_ptr); free(s->gw_members); free(s->gw_map); free(s->gw_ls);
 }
 
 void ne2o_sim_free(ne2o_sim *s) {
@@ -738,6 +751,8 @@ void ne2o_sim_reset_state(ne2o_sim *s) {
     memset(s->spike_bits, 0, sizeof(uint64_t) * (size_t)s->rec_rows * s->words);
     memset(s->spike_counts, 0, sizeof(uint32_t) * s->rec_rows);
     memset(s->pn_total, 0, sizeof(uint64_t) * n);
+    s->hist_head = s->hist_len = 0; /* cpu.rs:176-183 */
+    if (s->ngw) for (uint32_t k = 0; k < s->gw_ptr[s->ngw]; ++k) s->gw_ls[k] = 0xFFFFFFFFu;
     s->t = 0;
     s->spikes_total = 0;
     s->nspiked = 0;
@@ -875,13 +890,101 @@ void ne2o_sim_step(ne2o_sim *s) {
         for (uint32_t a = 0; a < s->nspiked; ++a) bits[s->spiked[a] / 64] |= 1ull << (s->spiked[a] % 64);
     }
     for (uint32_t a = 0; a < s->nspiked; ++a) s->pn_total[s->spiked[a]] += 1;
+    /* grid watches (cpu.rs:293-304) */
+    if (s->ngw) {
+        const uint32_t t32 = (uint32_t)(t < 0xFFFFFFFEull ? t : 0xFFFFFFFEull);
+        for (uint32_t a = 0; a < s->nspiked; ++a)
+            for (uint32_t g = 0; g < s->ngw; ++g) {
+                const int32_t k = s->gw_map[(size_t)g * n + s->spiked[a]];
+                if (k >= 0) s->gw_ls[s->gw_ptr[g] + (uint32_t)k] = t32;
+            }
+    }
     s->spikes_total += s->nspiked;
     s->t += 1;
 }
 
+/* v-watch recording after each step (cpu.rs:308-326): state slot 0/1 of
+ * every watched id (0 for ids beyond n), capped at NE2O_V_HIST_CAP */
+static void record_watches(ne2o_sim *s) {
+    if (!s->nwatch) return;
+    uint32_t pos;
+    if (s->hist_len < NE2O_V_HIST_CAP) {
+        pos = (s->hist_head + s->hist_len) % NE2O_V_HIST_CAP;
+        s->hist_len++;
+    } else {
+        pos = s->hist_head;
+        s->hist_head = (s->hist_head + 1) % NE2O_V_HIST_CAP;
+    }
+    for (uint32_t slot = 0; slot < 2; ++slot)
+        for (uint32_t k = 0; k < s->nwatch; ++k) {
+            const uint32_t i = s->v_watch[k];
+            s->x_hist[((size_t)slot * s->nwatch + k) * NE2O_V_HIST_CAP + pos] =
+                i < s->n ? s->x[2 * (size_t)i + slot] : 0.0f;
+        }
+}
+
+/* cpu.rs:330-338: a new list resets the history; the same list is a no-op */
+void ne2o_sim_set_v_watch(ne2o_sim *s, const uint32_t *ids, uint32_t count) {
+    if (count == s->nwatch && (count == 0 || memcmp(ids, s->v_watch, 4 * (size_t)count) == 0)) return;
+    free(s->v_watch);
+    free(s->x_hist);
+    s->nwatch = count;
+    s->v_watch = XMALLOC(uint32_t, count ? count : 1);
+    if (count) memcpy(s->v_watch, ids, 4 * (size_t)count);
+    s->x_hist = XMALLOC(float, 2 * (size_t)(count ? count : 1) * NE2O_V_HIST_CAP);
+    s->hist_head = s->hist_len = 0;
+}
+
+/* cpu.rs:350-357 drain_state for both slots: out[slot][watch][c], oldest
+ * first; returns c and empties the history */
+uint32_t ne2o_sim_drain_watch(ne2o_sim *s, float *out) {
+    const uint32_t c = s->hist_len;
+    for (uint32_t slot = 0; slot < 2; ++slot)
+        for (uint32_t k = 0; k < s->nwatch; ++k)
+            for (uint32_t j = 0; j < c; ++j)
+                out[((size_t)slot * s->nwatch + k) * c + j] =
+                    s->x_hist[((size_t)slot * s->nwatch + k) * NE2O_V_HIST_CAP + (s->hist_head + j) % NE2O_V_HIST_CAP];
+    s->hist_head = s->hist_len = 0;
+    return c;
+}
+
+/* cpu.rs:361-387: member lists in texel order; the same lists are a no-op */
+void ne2o_sim_set_grid_watches(ne2o_sim *s, const uint32_t *members, const uint32_t *group_ptr, uint32_t ngroups) {
+    if (ngroups == s->ngw && (ngroups == 0 || (memcmp(group_ptr, s->gw_ptr, 4 * ((size_t)ngroups + 1)) == 0 &&
+                                               memcmp(members, s->gw_members, 4 * (size_t)group_ptr[ngroups]) == 0)))
+        return;
+    free(s->gw_ptr); free(s->gw_members); free(s->gw_map); free(s->gw_ls);
+    const uint32_t total = ngroups ? group_ptr[ngroups] : 0;
+    s->ngw = ngroups;
+    s->gw_ptr = XMALLOC(uint32_t, (size_t)ngroups + 1);
+    memcpy(s->gw_ptr, group_ptr, 4 * ((size_t)ngroups + 1));
+    s->gw_members = XMALLOC(uint32_t, total ? total : 1);
+    if (total) memcpy(s->gw_members, members, 4 * (size_t)total);
+    s->gw_map = XMALLOC(int32_t, (size_t)(ngroups ? ngroups : 1) * (s->n ? s->n : 1));
+    for (size_t j = 0; j < (size_t)ngroups * s->n; ++j) s->gw_map[j] = -1;
+    for (uint32_t g = 0; g < ngroups; ++g)
+        for (uint32_t k = group_ptr[g]; k < group_ptr[g + 1]; ++k)
+            if (members[k] < s->n) s->gw_map[(size_t)g * s->n + members[k]] = (int32_t)(k - group_ptr[g]);
+    s->gw_ls = XMALLOC(uint32_t, total ? total : 1);
+    for (uint32_t k = 0; k < total; ++k) s->gw_ls[k] = 0xFFFFFFFFu;
+}
+
+/* cpu.rs:391-407: exp(-(t - last) * dt / tau) per texel, 0 if never */
+void ne2o_sim_grid_traces(const ne2o_sim *s, float tau_ms, float *out) {
+    const float k = s->cfg.dt_ms / (tau_ms > 1e-6f ? tau_ms : 1e-6f);
+    const uint32_t total = s->ngw ? s->gw_ptr[s->ngw] : 0;
+    for (uint32_t j = 0; j < total; ++j) {
+        const uint32_t l = s->gw_ls[j];
+        out[j] = l == 0xFFFFFFFFu ? 0.0f : expf(-(float)(s->t > l ? s->t - l : 0) * k);
+    }
+}
+
 /* cpu.rs:308-326 */
 void ne2o_sim_run_steps(ne2o_sim *s, uint64_t steps) {
-    for (uint64_t k = 0; k < steps; ++k) ne2o_sim_step(s);
+    for (uint64_t k = 0; k < steps; ++k) {
+        ne2o_sim_step(s);
+        record_watches(s);
+    }
 }
 
 uint64_t ne2o_sim_t(const ne2o_sim *s) { return s->t; }

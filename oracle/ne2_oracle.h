@@ -142,6 +142,12 @@ void      ne2o_sim_free(ne2o_sim *s);
 void      ne2o_sim_step(ne2o_sim *s);
 void      ne2o_sim_run_steps(ne2o_sim *s, uint64_t steps);
 void      ne2o_sim_reset_state(ne2o_sim *s);
+/* editor watches (cpu.rs:63-95, 308-407) */
+#define NE2O_V_HIST_CAP 4096u
+void      ne2o_sim_set_v_watch(ne2o_sim *s, const uint32_t *ids, uint32_t count);
+uint32_t  ne2o_sim_drain_watch(ne2o_sim *s, float *out); /* out: [2][nwatch][returned count] */
+void      ne2o_sim_set_grid_watches(ne2o_sim *s, const uint32_t *members, const uint32_t *group_ptr, uint32_t ngroups);
+void      ne2o_sim_grid_traces(const ne2o_sim *s, float tau_ms, float *out);
 uint64_t  ne2o_sim_t(const ne2o_sim *s);
 uint32_t  ne2o_sim_n(const ne2o_sim *s);
 uint32_t  ne2o_sim_ring_depth(const ne2o_sim *s);

@@ -90,6 +90,10 @@ def lib() -> C.CDLL:
             "ne2o_sim_trace": (None, [vp, vp]), "ne2o_sim_pn_total": (None, [vp, vp]),
             "ne2o_sim_spike_row": (u32, [vp, u32, vp]),
             "ne2o_sim_spike_counts": (i32, [vp, u64, vp, C.c_char_p, C.c_size_t]),
+            "ne2o_sim_set_v_watch": (None, [vp, vp, u32]),
+            "ne2o_sim_drain_watch": (u32, [vp, vp]),
+            "ne2o_sim_set_grid_watches": (None, [vp, vp, vp, u32]),
+            "ne2o_sim_grid_traces": (None, [vp, C.c_float, vp]),
             "ne2o_sim_last_step_spikes": (u32, [vp, vp]),
             "ne2o_sim_set_external": (None, [vp, u32, f32]),
             "ne2o_sim_set_input_constant": (None, [vp, u32, f32]),
@@ -375,6 +379,32 @@ class OSim:
 
     def fingerprint(self, rows) -> int:
         return int(lib().ne2o_sim_fingerprint(self.h, rows))
+
+    # editor watches (cpu.rs:308-407)
+    def set_v_watch(self, ids):
+        self._watch = np.ascontiguousarray(ids, dtype=np.uint32)
+        lib().ne2o_sim_set_v_watch(self.h, _p(self._watch), len(self._watch))
+
+    def drain_watch(self) -> np.ndarray:
+        """[state slot][watch][samples oldest first]"""
+        w = len(getattr(self, "_watch", ()))
+        out = np.zeros(max(2 * w * 4096, 1), np.float32)
+        c = lib().ne2o_sim_drain_watch(self.h, _p(out))
+        return out[: 2 * w * c].reshape(2, w, c)
+
+    def set_grid_watches(self, groups):
+        ptr = np.zeros(len(groups) + 1, np.uint32)
+        ptr[1:] = np.cumsum([len(g) for g in groups])
+        members = np.ascontiguousarray(np.concatenate([np.asarray(g, np.uint32) for g in groups])
+                                       if groups else np.zeros(0, np.uint32), dtype=np.uint32)
+        self._gw = (members, ptr)
+        lib().ne2o_sim_set_grid_watches(self.h, _p(members), _p(ptr), len(groups))
+
+    def grid_traces(self, tau_ms) -> list:
+        members, ptr = getattr(self, "_gw", (np.zeros(0, np.uint32), np.zeros(1, np.uint32)))
+        out = np.zeros(max(int(ptr[-1]), 1), np.float32)
+        lib().ne2o_sim_grid_traces(self.h, tau_ms, _p(out))
+        return [out[ptr[g]:ptr[g + 1]].copy() for g in range(len(ptr) - 1)]
 
 
 def noise_hash(i, t, seed) -> int:

@@ -139,10 +139,8 @@ def test_empty_net_advances_clock():
     assert len(g.spike_counts(5)) == 0
 
 
-def test_unsupported_and_invalid_calls_are_errors():
+def test_invalid_calls_are_errors():
     net, g, _ = one_neuron()
-    with pytest.raises(nb.Ne2bError, match="UNSUPPORTED"):
-        g.set_v_watch([0])
     with pytest.raises(nb.Ne2bError, match="EINVAL"):
         g.set_input_constant(3, 1.0)
     bad = net.flat()
@@ -219,3 +217,80 @@ def test_ne2_file_runs_bit_exact_against_oracle():
     assert first < 0, f"raster diverged at step {first}"
     assert o.spikes_total() > 0
     assert_state_bits_equal(g, o)
+
+
+def _nine():
+    net = O.ONet()
+    for i in range(9):
+        net.add_neuron(i * 10.0, 0.0, 0.0, O.EXC)
+    return net
+
+
+def test_v_watch_equals_oracle_and_keeps_reference_rules():
+    """sim/tests/v_watch.rs on the device: every step recorded, bit-equal to
+    the oracle (int ring), drained once, a changed list restarts, the same
+    list keeps its history, ids beyond n record 0, duplicates repeat, and
+    only the last 4096 samples are kept."""
+    onet = O.ONet.bench_net(500, 20, 3, 0.7, 5.0)
+    gc, oc = configs(True, 64, noise_rate_hz=500.0, noise_kick_mv=20.0, seed=4)
+    g = nb.B200Sim(onet.flat(), gc)
+    o = O.OSim(onet, oc)
+    ids = [0, 7, 7, 499, 10_000]
+    for s in (g, o):
+        s.set_v_watch(ids)
+        s.run_steps(300)
+    a, b = g.drain_watch(), o.drain_watch()
+    assert a.shape == (2, 5, 300) and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.all(a[:, 4] == 0.0) and np.array_equal(a[:, 1], a[:, 2])
+    assert g.drain_watch().shape == (2, 5, 0)
+    for s in (g, o):
+        s.set_v_watch(ids)  # same list: a no-op
+        s.run_steps(50)
+        s.set_v_watch([3])  # new list: history restarts now
+        s.run_steps(5000)  # beyond the 4096-sample cap
+    a, b = g.drain_watch(), o.drain_watch()
+    assert a.shape == (2, 1, 4096) and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    for s in (g, o):
+        s.reset_state()
+        s.run_steps(10)
+    assert np.array_equal(g.drain_watch().view(np.uint32), o.drain_watch().view(np.uint32))
+
+
+@pytest.mark.parametrize("mode", [nb.KERNEL_STREAM, nb.KERNEL_RESIDENT], ids=["stream", "resident"])
+def test_grid_traces_equal_oracle(mode):
+    """sim/tests/grid_trace.rs on the device: texel = member-list position,
+    groups independent, exp(-age*dt/tau) equal to the oracle's, reset
+    clears, no watches means no traces."""
+    onet = O.ONet.bench_net(600, 20, 5, 0.7, 5.0)
+    gc, oc = configs(True, 64, noise_rate_hz=300.0, noise_kick_mv=20.0, seed=8)
+    g = nb.B200Sim(onet.flat(), gc)
+    g.set_kernel_mode(mode)
+    o = O.OSim(onet, oc)
+    assert g.grid_traces(20.0) == []
+    groups = [list(range(0, 600, 3)), [5, 2, 5, 599, 9999], list(range(100))]
+    for s in (g, o):
+        s.set_grid_watches(groups)
+        s.run_steps(777)
+    for a, b in zip(g.grid_traces(20.0), o.grid_traces(20.0)):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert any(np.any(x > 0) for x in g.grid_traces(5.0))
+    for s in (g, o):
+        s.reset_state()
+    assert all(np.all(x == 0.0) for x in g.grid_traces(20.0))
+    for s in (g, o):
+        s.run_steps(123)
+    for a, b in zip(g.grid_traces(2.0), o.grid_traces(2.0)):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_grid_trace_single_spike_decays_as_the_reference_asserts():
+    """grid_trace.rs:23-50"""
+    g = nb.B200Sim(_nine().flat(), dt_ms=0.1)
+    g.set_grid_watches([list(range(9))])
+    g.set_external(4, 1000.0)
+    g.run_steps(1)
+    g.set_external(4, 0.0)
+    g.run_steps(99)
+    tr = g.grid_traces(20.0)[0]
+    assert abs(tr[4] - np.exp(-100 * 0.1 / 20.0)) < 1e-5
+    assert np.all(np.delete(tr, 4) == 0.0)

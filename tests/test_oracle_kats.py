@@ -369,3 +369,68 @@ def test_gauss_noise_moments():
     assert abs(z.mean()) < 0.02
     assert abs(z.var() - 1.0) < 0.03
     assert np.abs(z).max() <= 2 * math.sqrt(3.0)
+
+
+# --- editor watches (sim/tests/v_watch.rs, sim/tests/grid_trace.rs) ---------
+def _four():
+    net = O.ONet()
+    for _ in range(4):
+        net.add_neuron(0.0, 0.0, 0.0, O.EXC)
+    return net
+
+
+def test_watched_neurons_record_every_step():
+    """v_watch.rs:17-40"""
+    sim = O.OSim(_four(), O.cfg())
+    sim.set_v_watch([0, 2])
+    sim.set_external(0, 40.0)
+    sim.run_steps(200)
+    h = sim.drain_watch()[0]
+    assert h.shape == (2, 200)
+    assert np.any(h[0] > 0.0)
+    assert np.all(h[1] < -50.0)
+    assert sim.drain_watch().shape[2] == 0
+    sim.run_steps(30)
+    assert sim.drain_watch().shape[2] == 30
+
+
+def _nine():
+    net = O.ONet()
+    for i in range(9):
+        net.add_neuron(i * 10.0, 0.0, 0.0, O.EXC)
+    return net
+
+
+def test_grid_trace_marks_spiked_member_and_decays():
+    """grid_trace.rs:23-50"""
+    sim = O.OSim(_nine(), O.cfg())
+    sim.set_grid_watches([list(range(9))])
+    sim.set_external(4, 1000.0)
+    sim.run_steps(1)
+    sim.set_external(4, 0.0)
+    sim.run_steps(99)
+    tr = sim.grid_traces(20.0)[0]
+    for k, v in enumerate(tr):
+        if k == 4:
+            assert abs(v - np.exp(-100 * 0.1 / 20.0)) < 1e-5
+        else:
+            assert v == 0.0
+
+
+def test_grid_texel_is_member_list_position_and_groups_are_independent():
+    """grid_trace.rs:52-90"""
+    sim = O.OSim(_nine(), O.cfg())
+    sim.set_grid_watches([[7, 3, 5]])
+    sim.set_external(5, 1000.0)
+    sim.run_steps(1)
+    tr = sim.grid_traces(20.0)[0]
+    assert tr[2] > 0.0 and tr[0] == 0.0 and tr[1] == 0.0
+    sim = O.OSim(_nine(), O.cfg())
+    sim.set_grid_watches([[0, 1, 2], [2, 4]])
+    sim.set_external(2, 1000.0)
+    sim.run_steps(1)
+    a, b = sim.grid_traces(20.0)
+    assert a[2] > 0.0 and a[0] == 0.0 and b[0] > 0.0 and b[1] == 0.0
+    sim.reset_state()
+    assert all(np.all(x == 0.0) for x in sim.grid_traces(20.0))
+    assert O.OSim(_nine(), O.cfg()).grid_traces(20.0) == []

@@ -133,26 +133,35 @@ def dist_setup():
     return ws, rank, local
 
 
-def max_over_ranks(x: float, ws: int) -> float:
+def _reduce(x: float, ws: int, op: str) -> float:
+    """All-reduce one float over the replicas (NCCL on the GPUs, or the CPU
+    tensors of a gloo group)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    return _reduce(x, ws, "max")
 
 
 def sum_over_ranks(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    return _reduce(x, ws, "sum")
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+
+def replica_aggregate(local_ms: float, local_units: float, ws: int) -> tuple[float, float, float]:
+    """Weak-scaling aggregate of independent replicas: the slowest rank's
+    device time, the units all ranks processed, and units per second over
+    that time."""
+    ms = max_over_ranks(local_ms, ws)
+    units = sum_over_ranks(local_units, ws)
+    return ms, units, units / (ms / 1000.0)
 
 
 def barrier(ws: int):
@@ -278,9 +287,8 @@ def run_ours(args):
 
     with Clocks(dev) as clk:
         total_ms, spikes, launches = timed_trials(sim, args.steps, args.warmup, TRIAL_STEPS, ws, torch, scrub)
-    total_ms = max_over_ranks(total_ms, ws)
     n_updates = float(N) * TRIAL_STEPS * args.steps
-    value = sum_over_ranks(n_updates, ws) / (total_ms / 1000.0)
+    total_ms, _, value = replica_aggregate(total_ms, n_updates, ws)
     events = spikes * K_OUT
     step_launches = TRIAL_STEPS * args.steps
     launch_ms = total_ms / step_launches

@@ -306,6 +306,11 @@ typedef struct {
 } ne2b_ne2_meta;
 ne2b_status ne2b_net_load_ne2(const char *path, ne2b_net **out, ne2b_ne2_meta *meta);
 ne2b_status ne2b_net_from_ne2(const uint8_t *bytes, uint64_t len, ne2b_net **out, ne2b_ne2_meta *meta);
+/* Self-test of the resident kernel's bounded grid barrier (no counterpart in
+ * the reference): 4 cooperative blocks of which one never arrives; the
+ * other three give up after limit_ms (1..2000), flag the error and return,
+ * and *timed_out reports it.  The device stays usable; nothing faults. */
+ne2b_status ne2b_selftest_barrier_timeout(int device, uint32_t limit_ms, int32_t *timed_out);
 /* Random K-out workload net (10k/100k/1M configurations). */
 ne2b_status ne2b_gen_random_kout(uint32_t n, uint32_t k, uint64_t seed, float w_scale, float exc_hi,
                                  float inh_hi, float delay_cap_ms, float dt_ms, ne2b_net **out);

@@ -18,8 +18,18 @@ __all__ = [
     "B200Sim", "Batch", "Server", "SpikeWindowError", "footprint", "FlatNet", "NativeNet", "from_synapses",
     "liquid", "random_kout", "to_adex", "load_ne2", "from_ne2_bytes", "config_from_meta", "Config", "default_config", "Ne2bError", "MODEL_IZH", "MODEL_ADEX",
     "KERNEL_AUTO", "KERNEL_STREAM", "KERNEL_RESIDENT",
-    "expf",
+    "expf", "selftest_barrier_timeout",
 ]
+
+
+def selftest_barrier_timeout(limit_ms: int = 50, device: int = 0) -> bool:
+    """Run the bounded grid-barrier self-test (one cooperative block never
+    arrives); True when the waiting blocks gave up and flagged it."""
+    import ctypes
+
+    t = ctypes.c_int32()
+    _abi.check(_abi.lib.ne2b_selftest_barrier_timeout(device, limit_ms, ctypes.byref(t)))
+    return bool(t.value)
 
 
 def expf(x: float) -> float:

@@ -176,6 +176,7 @@ _SIGS = {
     "ne2b_batch_kernel_launches": (C.c_int, [_p, _pu64]),
     "ne2b_server_stream": (C.c_int, [_p, C.POINTER(_p)]),
     "ne2b_server_synchronize": (C.c_int, [_p]),
+    "ne2b_selftest_barrier_timeout": (C.c_int, [C.c_int, _u32, C.POINTER(C.c_int32)]),
     "ne2b_server_set_tile_shape": (C.c_int, [_p, _u32, _u32, _u32]),
     "ne2b_server_kernel_launches": (C.c_int, [_p, _pu64]),
     "ne2b_set_v_watch": (C.c_int, [_p, _p, _u32]),

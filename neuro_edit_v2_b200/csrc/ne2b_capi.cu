@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "ne2b_engine.h"
+#include "ne2b_kernels.h"
 #include "ne2b_parallel.h"
 
 using ne2b::Engine;
@@ -884,6 +885,29 @@ ne2b_status ne2b_server_set_tile_shape(ne2b_server *s, uint32_t block, uint32_t 
     sh.npt = npt;
     sh.blocks_per_sm = bps;
     GUARD(s->eng.set_shape(sh));
+}
+
+ne2b_status ne2b_selftest_barrier_timeout(int device, uint32_t limit_ms, int32_t *timed_out) {
+    if (!timed_out) return set_error(NE2B_EINVAL, "null argument");
+    if (limit_ms == 0 || limit_ms > 2000) return set_error(NE2B_EINVAL, "limit_ms must be in 1..2000");
+    *timed_out = 0;
+    GUARD(([&]() -> ne2b_status {
+        ne2b_status st = ne2b::cuda_error(cudaSetDevice(device), "cudaSetDevice");
+        if (st != NE2B_OK) return st;
+        unsigned int *d = nullptr;
+        st = ne2b::cuda_error(cudaMalloc(&d, 2 * sizeof(unsigned int)), "cudaMalloc");
+        if (st != NE2B_OK) return st;
+        unsigned int h[2] = {0u, 0u};
+        st = ne2b::cuda_error(cudaMemset(d, 0, sizeof h), "cudaMemset");
+        if (st == NE2B_OK)
+            st = ne2b::cuda_error(ne2b::launch_barrier_selftest(d, d + 1, 4, 2, 1000000ull * limit_ms, 0),
+                                  "self-test launch");
+        if (st == NE2B_OK) st = ne2b::cuda_error(cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost), "readback");
+        cudaFree(d);
+        if (st != NE2B_OK) return st;
+        *timed_out = h[1] != 0u ? 1 : 0;
+        return NE2B_OK;
+    })());
 }
 
 ne2b_status ne2b_server_synchronize(ne2b_server *s) {

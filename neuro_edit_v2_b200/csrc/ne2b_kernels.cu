@@ -65,6 +65,16 @@ __global__ void pn_total_kernel(const unsigned long long *pn, uint32_t n, uint32
     out[i] = c > 0xffffffffull ? 0xffffffffu : (uint32_t)c;
 }
 
+// Self-test of the bounded grid barrier: every block but `absent` arrives,
+// so the others give up after `limit_ns`, set the error flag and return
+// (a wait that cannot end, ended by its limit, with no fault).
+__global__ void barrier_selftest_kernel(unsigned int *counter, unsigned int *err, uint32_t absent,
+                                        unsigned long long limit_ns) {
+    __shared__ unsigned int s_flag;
+    if (blockIdx.x == absent) return;
+    grid_barrier(counter, gridDim.x, err, &s_flag, limit_ns);
+}
+
 // ------------------------------------------------------------- launchers
 bool shape_supported(uint32_t block, uint32_t npt) {
 #define X(B, P) if (block == B && npt == P) return true;
@@ -114,6 +124,12 @@ int resident_occupancy(bool int_ring, bool adex, uint32_t block, uint32_t npt, s
 cudaError_t launch_resident(bool int_ring, bool adex, uint32_t block, uint32_t npt, const EngineDev *eng,
                             uint32_t k0, uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st) {
     return NE2B_KIND(int_ring, adex, launch_resident(block, npt, eng, k0, nsteps, grid, smem, st));
+}
+
+cudaError_t launch_barrier_selftest(unsigned int *counter, unsigned int *err, uint32_t blocks, uint32_t absent,
+                                    unsigned long long limit_ns, cudaStream_t st) {
+    void *args[] = {(void *)&counter, (void *)&err, (void *)&absent, (void *)&limit_ns};
+    return cudaLaunchCooperativeKernel((const void *)barrier_selftest_kernel, dim3(blocks), dim3(32), args, 0, st);
 }
 
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st) {

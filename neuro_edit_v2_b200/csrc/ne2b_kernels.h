@@ -23,6 +23,10 @@ int resident_occupancy(bool int_ring, bool adex, uint32_t block, uint32_t npt, s
 cudaError_t launch_resident(bool int_ring, bool adex, uint32_t block, uint32_t npt, const EngineDev *eng,
                             uint32_t k0, uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st);
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st);
+// Bounded grid barrier self-test: `blocks` cooperative blocks of which
+// `absent` never arrives; the others stop after `limit_ns` and set *err.
+cudaError_t launch_barrier_selftest(unsigned int *counter, unsigned int *err, uint32_t blocks, uint32_t absent,
+                                    unsigned long long limit_ns, cudaStream_t st);
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st);
 cudaError_t launch_trace(const uint16_t *tk, const float *tab, uint32_t n, float *out, cudaStream_t st);
 cudaError_t launch_window_count(const uint32_t *rec_bits, uint32_t rec_rows, uint32_t n_pad, uint32_t n,

@@ -445,7 +445,8 @@ __device__ __forceinline__ unsigned int atom_add_release_gpu(unsigned int *p, un
 // stop.  Returns false (for every thread of the block) when the launch must
 // stop.
 __device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int target, unsigned int *err,
-                                             unsigned int *s_flag) {
+                                             unsigned int *s_flag,
+                                             unsigned long long limit_ns = kBarrierLimitNs) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -459,7 +460,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int
                         ok = 0u;
                         break;
                     }
-                    if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+                    if (globaltimer_ns() - t0 > limit_ns) {
                         atomicExch(err, 1u);
                         ok = 0u;
                         break;

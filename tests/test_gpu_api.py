@@ -294,3 +294,22 @@ def test_grid_trace_single_spike_decays_as_the_reference_asserts():
     tr = g.grid_traces(20.0)[0]
     assert abs(tr[4] - np.exp(-100 * 0.1 / 20.0)) < 1e-5
     assert np.all(np.delete(tr, 4) == 0.0)
+
+
+def test_bounded_grid_barrier_times_out_and_device_stays_usable():
+    """A grid-barrier wait that can never end (one block never arrives) stops
+    at its limit with the error flag set, and the device keeps working: a
+    sim afterwards still equals the oracle."""
+    import time
+
+    t0 = time.perf_counter()
+    assert nb.selftest_barrier_timeout(50)
+    assert time.perf_counter() - t0 < 10.0
+    onet = O.ONet.bench_net(1000, 20, 2, 0.7, 5.0)
+    gc, oc = configs(True, 100, noise_rate_hz=500.0, noise_kick_mv=20.0, seed=3)
+    g = nb.B200Sim(onet.flat(), gc)
+    g.set_kernel_mode(nb.KERNEL_RESIDENT)
+    o = O.OSim(onet, oc)
+    g.run_steps(500)
+    o.run_steps(500)
+    assert g.spikes_total() == o.spikes_total() > 0

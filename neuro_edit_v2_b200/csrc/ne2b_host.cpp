@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "../../include/ne2b.h"
@@ -155,35 +156,85 @@ ne2b_status ne2b_net_from_synapses(uint32_t n, const uint8_t *model, const float
             for (uint32_t k = 0; k < kStride && k < param_stride; ++k)
                 net->params[(size_t)i * kStride + k] = params[(size_t)i * param_stride + k];
         net->pos.assign((size_t)n * 3, 0.0f);
-        // stable counting sort by source (== sort_by_key, network.rs:656-657)
-        net->src_ptr.assign((size_t)n + 1, 0);
-        for (uint64_t j = 0; j < n_syn; ++j) {
-            if (src[j] >= n || tgt[j] >= n) {
-                delete net;
-                return set_error(NE2B_EINVAL, "synapse %llu references %u -> %u but only %u neurons exist",
-                                 (unsigned long long)j, src[j], tgt[j], n);
+        // stable counting sort by source (== sort_by_key, network.rs:656-657),
+        // over T chunks of the synapse list in parallel: each chunk counts
+        // its sources, the chunk offsets of a source follow the chunk order,
+        // and each chunk scatters its synapses in order, so the result is the
+        // stable order of the whole list
+        const unsigned hw = std::thread::hardware_concurrency();
+        unsigned T = n_syn >= (1u << 20) ? std::min(8u, hw ? hw : 1u) : 1u;
+        if ((uint64_t)T * n > 4ull * n_syn + (1u << 20)) T = 1;  // per-chunk counts would outweigh the list
+        std::vector<uint32_t> cnt((size_t)T * n, 0);
+        std::vector<uint64_t> bad_ref(T, ~0ull), bad_delay(T, ~0ull);
+        auto chunk = [&](unsigned c, uint64_t *lo, uint64_t *hi) {
+            *lo = n_syn * c / T;
+            *hi = n_syn * (c + 1) / T;
+        };
+        auto run = [&](auto f) {
+            if (T == 1) {
+                f(0u);
+                return;
             }
-            net->src_ptr[src[j] + 1]++;
+            std::vector<std::thread> th;
+            for (unsigned c = 0; c < T; ++c) th.emplace_back(f, c);
+            for (auto &x : th) x.join();
+        };
+        run([&](unsigned c) {
+            uint64_t lo, hi;
+            chunk(c, &lo, &hi);
+            uint32_t *cc = cnt.data() + (size_t)c * n;
+            for (uint64_t j = lo; j < hi; ++j) {
+                if (src[j] >= n || tgt[j] >= n) {
+                    bad_ref[c] = j;
+                    return;
+                }
+                cc[src[j]]++;
+            }
+        });
+        const uint64_t first_bad = *std::min_element(bad_ref.begin(), bad_ref.end());
+        if (first_bad != ~0ull) {
+            delete net;
+            return set_error(NE2B_EINVAL, "synapse %llu references %u -> %u but only %u neurons exist",
+                             (unsigned long long)first_bad, src[first_bad], tgt[first_bad], n);
         }
-        for (uint32_t i = 0; i < n; ++i) net->src_ptr[i + 1] += net->src_ptr[i];
-        std::vector<uint32_t> fill(net->src_ptr.begin(), net->src_ptr.end() - 1);
+        net->src_ptr.assign((size_t)n + 1, 0);
+        {
+            uint32_t base = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                net->src_ptr[i] = base;
+                for (unsigned c = 0; c < T; ++c) {  // counts become chunk offsets
+                    const uint32_t k = cnt[(size_t)c * n + i];
+                    cnt[(size_t)c * n + i] = base;
+                    base += k;
+                }
+            }
+            net->src_ptr[n] = base;
+        }
         net->tgt.resize(n_syn);
         net->w.resize(n_syn);
         net->delay.resize(n_syn);
         bool any_tau = false;
         for (uint64_t j = 0; tau_ms && j < n_syn && !any_tau; ++j) any_tau = tau_ms[j] > 0.0f;
         if (any_tau) net->tau.resize(n_syn);
-        for (uint64_t j = 0; j < n_syn; ++j) {
-            const uint32_t p = fill[src[j]]++;
-            if (any_tau) net->tau[p] = tau_ms[j];  // network.rs:673 (tau travels with its synapse)
-            net->tgt[p] = tgt[j];
-            const float m = fabsf(w[j]);
-            net->w[p] = kind[src[j]] == 1 ? -m : m;  // Dale's law, network.rs:668-672
-            if (!delay_steps(dly[j], dt_ms, &net->delay[p])) {
-                delete net;
-                return set_error(NE2B_EINVAL, "synapse %u -> %u: delay %g ms at dt %g ms exceeds the 65535-step ring",
-                                 src[j], tgt[j], (double)dly[j], (double)dt_ms);
+        run([&](unsigned c) {
+            uint64_t lo, hi;
+            chunk(c, &lo, &hi);
+            uint32_t *fill = cnt.data() + (size_t)c * n;
+            for (uint64_t j = lo; j < hi; ++j) {
+                const uint32_t p = fill[src[j]]++;
+                if (any_tau) net->tau[p] = tau_ms[j];  // network.rs:673 (tau travels with its synapse)
+                net->tgt[p] = tgt[j];
+                const float m = fabsf(w[j]);
+                net->w[p] = kind[src[j]] == 1 ? -m : m;  // Dale's law, network.rs:668-672
+                if (!delay_steps(dly[j], dt_ms, &net->delay[p]) && bad_delay[c] == ~0ull) bad_delay[c] = j;
             }
+        });
+        const uint64_t first_long = *std::min_element(bad_delay.begin(), bad_delay.end());
+        if (first_long != ~0ull) {
+            const uint64_t j = first_long;
+            delete net;
+            return set_error(NE2B_EINVAL, "synapse %u -> %u: delay %g ms at dt %g ms exceeds the 65535-step ring",
+                             src[j], tgt[j], (double)dly[j], (double)dt_ms);
         }
         net->stim_ptr.assign((size_t)n + 1, 0);
         *out = net;

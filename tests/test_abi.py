@@ -131,3 +131,29 @@ def test_request_footprint_needs_no_gpu():
     neurons, syn, ring = nb.footprint(net, cfg)
     assert neurons == 1024 and syn == net.n_syn
     assert ring == neurons * net.arrays().ring_depth()
+
+
+def test_parallel_csr_build_is_the_stable_order():
+    """Above 2^20 synapses the CSR build sorts in parallel chunks; the result
+    must still be the stable order by source (network.rs:656-657), with
+    Dale's sign, delay steps and per-synapse tau carried along."""
+    rng = np.random.default_rng(7)
+    n, e = 5000, 1_500_000
+    src = rng.integers(0, n, e).astype(np.uint32)
+    tgt = rng.integers(0, n, e).astype(np.uint32)
+    w = rng.random(e).astype(np.float32)
+    d = (rng.random(e) * 20).astype(np.float32)
+    tau = np.where(rng.random(e) < 0.1, rng.uniform(1, 20, e), 0).astype(np.float32)
+    kind = (rng.random(n) < 0.2).astype(np.uint8)
+    model = np.zeros(n, np.uint8)
+    params = np.tile(np.array([0.02, 0.2, -65, 8], np.float32), (n, 1))
+    a = nb.from_synapses(model, params, kind, src, tgt, w, d, 0.1, tau_ms=tau).arrays()
+    order = np.argsort(src, kind="stable")
+    assert np.array_equal(a.src_ptr, np.concatenate([[0], np.cumsum(np.bincount(src, minlength=n))]))
+    assert np.array_equal(a.tgt, tgt[order])
+    sign = np.where(kind[src[order]] == 1, -1.0, 1.0).astype(np.float32)
+    assert np.array_equal(a.w, sign * w[order])
+    assert np.array_equal(a.tau_ms, tau[order])
+    q = (d[order] / np.float32(0.1)).astype(np.float64)  # f32 quotient; roundf rounds half away from zero
+    steps = np.maximum(1, np.floor(q + 0.5)).astype(np.uint16)
+    assert np.array_equal(a.delay_steps, steps)

@@ -64,18 +64,60 @@ def load_traffic():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+    """SM clocks and throttle reasons sampled during the timed region: an
+    NVML thread polling every 10 ms (read-only queries), or nvidia-smi at
+    200 ms where NVML is not available."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits: sw power cap, hw slowdown, sw thermal, hw thermal
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.rows = []
+        self.thread = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
 
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            import torch
+
+            p = torch.cuda.get_device_properties(self.device)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
     def __enter__(self):
+        import threading
+
+        try:
+            nv, h = self._nvml_handle()
+            self.stop = threading.Event()
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.rows.append((float(sm), float(smax), reasons))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.01)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
@@ -87,6 +129,9 @@ class Clocks:
         return self
 
     def __exit__(self, *exc):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -96,25 +141,30 @@ class Clocks:
             self.f.close()
 
     def summary(self):
-        if not self.proc or not os.path.exists(self.path):
-            return None
         rows = []
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
-                except ValueError:
-                    continue
+        if self.thread:
+            for sm, smax, bits in self.rows:
+                rows.append((sm, smax, [k for k, b in self.REASON_BITS.items() if bits & b]))
+            source = "nvml 10 ms"
+        elif self.proc and os.path.exists(self.path):
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        rows.append((float(parts[1]), float(parts[2]),
+                                     [names[k] for k in range(4) if parts[5 + k].lower().startswith("active")]))
+                    except ValueError:
+                        continue
+            source = "nvidia-smi 200 ms"
         if not rows:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for _, _, r in rows for k in range(4) if r[k].lower().startswith("active")})
+        reasons = sorted({r for _, _, rs in rows for r in rs})
         load = [r[0] for r in rows if r[0] > 300] or [r[0] for r in rows]
         return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": source}
 
 
 def dist_setup():

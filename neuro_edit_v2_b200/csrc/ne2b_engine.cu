@@ -616,15 +616,24 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         // trace after k non-spiking steps = 1.0 * decay_t * ... * decay_t (k
         // f32 multiplies in order, cpu.rs:252-256); the table stops at 0 or
         // at the subnormal fixed point, where the trace stays forever
+        // (a u16 step counter); a readout tau whose table would pass 65534
+        // entries keeps the f32 trace per neuron instead
         std::vector<float> tab(1, 1.0f);
+        bool trace_f32 = false;
         while (true) {
             const float nx = tab.back() * d.decay_t;
             if (nx == tab.back()) break;
             tab.push_back(nx);
             if (nx == 0.0f) break;
-            if (tab.size() > 65534) return fail(set_error(NE2B_UNSUPPORTED,
-                "readout_tau_ms %g at dt %g needs more than 65534 trace steps", (double)cfg->readout_tau_ms,
-                (double)cfg->dt_ms));
+            if (tab.size() > 65534) {
+                trace_f32 = true;
+                tab.resize(1);
+                break;
+            }
+        }
+        if (trace_f32) {
+            NET_TRY(alloc(&p, sizeof(float) * np)); d.trace_f = (float *)p;
+            NET_TRY(cuda_error(cudaMemsetAsync(d.trace_f, 0, sizeof(float) * np, bst), "memset trace"));
         }
         NET_TRY(alloc(&p, sizeof(float) * tab.size())); d.trace_tab = (const float *)p;
         NET_TRY(up((void *)d.trace_tab, tab.data(), sizeof(float) * tab.size()));
@@ -632,7 +641,8 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     }
     fill_noise(d, *cfg);
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
-              (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u) | (h->nx ? kNetXsyn : 0u);
+              (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u) | (h->nx ? kNetXsyn : 0u) |
+              (d.trace_f ? kNetTraceF32 : 0u);
     tp[5] = now_ms();
     // initial state (cpu.rs:158-183), on the build stream
     NET_TRY(cuda_error(launch_reset_neurons(d, bst), "reset kernel"));
@@ -856,6 +866,7 @@ ne2b_status Engine::reset_net(uint32_t slot) {
     NE2B_CUDA(cudaMemsetAsync(d.ring, 0, sizeof(uint32_t) * (size_t)h.D * h.n_pad, stream_));
     if (d.rec_bits) NE2B_CUDA(cudaMemsetAsync(d.rec_bits, 0, sizeof(uint32_t) * (size_t)d.rec_rows * (h.n_pad / 32), stream_));
     if (d.win_out) NE2B_CUDA(cudaMemsetAsync(d.win_out, 0, sizeof(uint16_t) * (size_t)d.max_windows * h.n_pad, stream_));
+    if (d.trace_f) NE2B_CUDA(cudaMemsetAsync(d.trace_f, 0, sizeof(float) * h.n_pad, stream_));
     if (h.nx) {
         NE2B_CUDA(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h.nx, stream_));
         NE2B_CUDA(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h.D * d.xwords, stream_));
@@ -1044,6 +1055,7 @@ ne2b_status Engine::read_f32(const float *dev, uint32_t n, float *out) {
 
 ne2b_status Engine::read_trace(NetHost &h, float *out) {
     if (h.n == 0) return NE2B_OK;
+    if (h.dev.trace_f) return read_f32(h.dev.trace_f, h.n, out);
     float *tmp = nullptr;
     NE2B_CUDA(cudaMallocAsync((void **)&tmp, sizeof(float) * h.n, stream_));
     cudaError_t e = launch_trace(h.dev.tk, h.dev.trace_tab, h.n, tmp, stream_);
@@ -1280,6 +1292,7 @@ ne2b_status Engine::snapshot(EngineSnapshot &snap) {
         NE2B_TRY(grab(d.u, 4 * np));
         NE2B_TRY(grab(d.s, 4 * np));
         NE2B_TRY(grab(d.tk, 2 * np));
+        NE2B_TRY(grab(d.trace_f, d.trace_f ? 4 * np : 0));
         NE2B_TRY(grab(d.pn_total, 8 * np));
         NE2B_TRY(grab(d.ring, 4 * (size_t)h->D * np));
         NE2B_TRY(grab(d.rec_bits, d.rec_bits ? 4 * (size_t)d.rec_rows * (np / 32) : 0));

@@ -34,6 +34,7 @@ enum NetFlags : uint32_t {
     kNetXsyn = 1u << 6,     // some synapses have their own tau (XSyn)
     kNetWatch = 1u << 7,    // watched neurons record their state every step
     kNetGridWatch = 1u << 8,  // grid groups record each member's last spike step
+    kNetTraceF32 = 1u << 9,   // readout trace kept as f32 (its step table would be too long)
 };
 
 enum TileFlags : uint32_t {
@@ -69,6 +70,7 @@ struct alignas(16) NetDev {
     // neuron arrays
     float *v, *u, *s, *ext;
     uint16_t *tk;              // steps since last spike (trace_tab index), kTraceZero = 0
+    float *trace_f;            // kNetTraceF32 only: the f32 trace itself
     const float *trace_tab;    // trace_tab[k] = decay_t applied k times to 1.0 (f32, in order)
     const float *v0, *u0;
     const uint16_t *pidx;

@@ -188,7 +188,13 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         // trace: 1 on spike, else one more multiply by decay_t (saturating at
         // the table's last entry, 0 or the subnormal fixed point)
         const uint32_t k0 = tk[q];
-        const uint32_t k = sp ? 0u : (k0 == kTraceZero ? k0 : (k0 < tlast ? k0 + 1u : tlast));
+        uint32_t k = sp ? 0u : (k0 == kTraceZero ? k0 : (k0 < tlast ? k0 + 1u : tlast));
+        if (flags & kNetTraceF32) {  // a readout tau too long for the step table: the f32 trace
+            const float tr = nd.trace_f[i];
+            const float tn = sp ? 1.0f : __fmul_rn(tr, nd.decay_t);  // cpu.rs:252-260
+            if (__float_as_uint(tn) != __float_as_uint(tr)) nd.trace_f[i] = tn;
+            k = k0;
+        }
         const float snew = __fmul_rn(sv, decay_s);
         vs[off] = v[q];
         us[off] = u[q];

@@ -313,3 +313,23 @@ def test_bounded_grid_barrier_times_out_and_device_stays_usable():
     g.run_steps(500)
     o.run_steps(500)
     assert g.spikes_total() == o.spikes_total() > 0
+
+
+@pytest.mark.parametrize("tau", [2.0, 1000.0])
+def test_trace_equals_oracle_for_short_and_long_readout_tau(tau):
+    """The readout trace (cpu.rs:252-260): a step-count table for short
+    taus, the f32 trace itself where that table would be too long; both
+    equal the oracle's repeated multiply bit for bit."""
+    onet = O.ONet.bench_net(1500, 30, 6, 0.7, 5.0)
+    gc, oc = configs(True, 100, noise_rate_hz=500.0, noise_kick_mv=20.0, seed=2, readout_tau_ms=tau)
+    g = nb.B200Sim(onet.flat(), gc)
+    o = O.OSim(onet, oc)
+    for _ in range(3):
+        g.run_steps(700)
+        o.run_steps(700)
+        assert np.array_equal(g.trace().view(np.uint32), o.trace().view(np.uint32))
+    g.reset_state()
+    o.reset_state()
+    g.run_steps(50)
+    o.run_steps(50)
+    assert np.array_equal(g.trace().view(np.uint32), o.trace().view(np.uint32))

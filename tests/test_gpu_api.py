@@ -333,3 +333,20 @@ def test_trace_equals_oracle_for_short_and_long_readout_tau(tau):
     g.run_steps(50)
     o.run_steps(50)
     assert np.array_equal(g.trace().view(np.uint32), o.trace().view(np.uint32))
+
+
+def test_adex_noise_gain_drives_lone_neuron_on_gpu():
+    """sim/tests/adex.rs:174-243 on the device, equal to the oracle."""
+    def rates(rate_hz, kick_mv, steps=200_000):
+        net = O.ONet()
+        net.add_neuron(0.0, 0.0, 0.0, O.EXC)
+        net.set_model(0, 1, [281.0, 30.0, -70.6, -50.4, 2.0, 4.0, 144.0, 80.5, -70.6, 20.0])
+        g = nb.B200Sim(net.flat(), noise_rate_hz=rate_hz, noise_kick_mv=kick_mv, seed=5)
+        o = O.OSim(net, O.cfg(noise_rate_hz=rate_hz, noise_kick_mv=kick_mv, seed=5, exp_mode=1))
+        g.run_steps(steps)
+        o.run_steps(steps)
+        assert g.spikes_total() == o.spikes_total()
+        return g.spikes_total() / 20.0
+
+    assert rates(60.0, 14.0) > 0.5
+    assert rates(120.0, 18.0) > 1.5 * rates(30.0, 18.0)

@@ -434,3 +434,20 @@ def test_grid_texel_is_member_list_position_and_groups_are_independent():
     sim.reset_state()
     assert all(np.all(x == 0.0) for x in sim.grid_traces(20.0))
     assert O.OSim(_nine(), O.cfg()).grid_traces(20.0) == []
+
+
+def _lone_adex_rate(rate_hz, kick_mv, ms=20000.0):
+    net = O.ONet()
+    net.add_neuron(0.0, 0.0, 0.0, O.EXC)
+    net.set_model(0, 1, [281.0, 30.0, -70.6, -50.4, 2.0, 4.0, 144.0, 80.5, -70.6, 20.0])
+    sim = O.OSim(net, O.cfg(noise_rate_hz=rate_hz, noise_kick_mv=kick_mv, seed=5))
+    sim.run_steps(int(round(ms / 0.1)))
+    return sim.spikes_total() / (ms / 1000.0)
+
+
+def test_adex_noise_gain_drives_lone_neuron():
+    """sim/tests/adex.rs:174-233: the Poisson kick is scaled by the AdEx gain
+    (C), so a lone AdEx cell fires at 60 Hz x 14 mV and fires more at a
+    higher noise rate."""
+    assert _lone_adex_rate(60.0, 14.0) > 0.5
+    assert _lone_adex_rate(120.0, 18.0) > 1.5 * _lone_adex_rate(30.0, 18.0)

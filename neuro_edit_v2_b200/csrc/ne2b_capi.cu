@@ -371,6 +371,7 @@ ne2b_status ne2b_batch_create(const ne2b_net_desc *nets, const ne2b_config *cfgs
             return set_error(NE2B_EINVAL, "all nets of a batch share one ring mode");
     GUARD(([&]() -> ne2b_status {
         ne2b_batch *b = new ne2b_batch();
+        b->eng.multi_net = true;
         ne2b_status st = b->eng.init(device, cfgs[0].int_weights != 0, count);
         for (uint32_t k = 0; k < count && st == NE2B_OK; ++k) {
             uint32_t slot = 0;
@@ -589,6 +590,7 @@ ne2b_status ne2b_server_create(const ne2b_server_config *cfg, int device, ne2b_s
         }
         s->eng.graph_steps = s->cfg.steps_per_launch;
         s->eng.fixed_grid = true;
+        s->eng.multi_net = true;
         {
             // small tiles: the most blocks per SM, so the latency chains of
             // active tiles (state loads, scans, CSR loads) overlap; measured

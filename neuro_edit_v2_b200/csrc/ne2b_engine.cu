@@ -603,12 +603,11 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     d.n = n;
     d.n_pad = np;
     d.D = h->D;
-    d.t = 0;
-    d.tmod = 0;
     d.t_end = h->t_end;
     d.seed = cfg->seed;
     d.n_inputs = net->n_inputs;
     d.rec_rows = rec_rows;
+    set_step(d, 0);
     d.dt = cfg->dt_ms;
     d.decay_s = host_decay(cfg->dt_ms, cfg->synapse_tau_ms);
     d.decay_t = host_decay(cfg->dt_ms, cfg->readout_tau_ms);
@@ -709,7 +708,7 @@ uint64_t Engine::dev_bytes() const {
 
 uint32_t Engine::grid() const {
     uint32_t bps = shape_.blocks_per_sm;
-    const int occ = step_occupancy(int_ring_, adex_, shape_.block, shape_.npt);
+    const int occ = step_occupancy(int_ring_, adex_, multi_net, shape_.block, shape_.npt);
     if (bps == 0 || (int)bps > occ) bps = (uint32_t)(occ > 0 ? occ : 1);
     uint32_t g = (uint32_t)sm_count_ * bps;
     if (fixed_grid) return g;  // serving: graphs stay valid as nets come and go
@@ -876,8 +875,7 @@ ne2b_status Engine::reset_net(uint32_t slot) {
     if (d.gw_ls) NE2B_CUDA(cudaMemsetAsync(d.gw_ls, 0xFF, sizeof(uint32_t) * std::max<uint32_t>(h.gw_ptr.back(), 1), stream_));
     NE2B_CUDA(cudaMemsetAsync(d_counters_ + slot, 0, sizeof(NetCounters), stream_));
     h.t = 0;
-    d.t = 0;
-    d.tmod = 0;
+    set_step(d, 0);
     if (!h.fixed_stim) d.stim_len = 0;  // repack from t = 0
     return upload_net(h);
 }
@@ -994,7 +992,7 @@ ne2b_status Engine::launch_group(uint32_t steps) {
             NE2B_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
             cudaError_t err = cudaSuccess;
             for (uint32_t k = 0; k < steps && err == cudaSuccess; ++k)
-                err = launch_step(int_ring_, adex_, shape_.block, shape_.npt, d_eng_, k, g, stream_);
+                err = launch_step(int_ring_, adex_, multi_net, shape_.block, shape_.npt, d_eng_, k, g, stream_);
             if (err == cudaSuccess) err = launch_advance(d_nets_, nets_cap_, steps, stream_);
             cudaError_t e2 = cudaStreamEndCapture(stream_, &gr);
             if (err != cudaSuccess) return cuda_error(err, "step launch during capture");
@@ -1009,7 +1007,7 @@ ne2b_status Engine::launch_group(uint32_t steps) {
         launches_ += steps + 1;
         return NE2B_OK;
     }
-    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, adex_, shape_.block, shape_.npt, d_eng_, k, g, stream_));
+    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, adex_, multi_net, shape_.block, shape_.npt, d_eng_, k, g, stream_));
     NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
     launches_ += steps + 1;
     return NE2B_OK;
@@ -1038,8 +1036,7 @@ ne2b_status Engine::run_steps(uint64_t steps) {
         for (NetHost *h : nets_)
             if (h) {
                 h->t = std::min<uint64_t>(h->t + chunk, h->t_end);
-                h->dev.t = h->t;
-                h->dev.tmod = (uint32_t)(h->t % h->D);
+                set_step(h->dev, h->t);
             }
         steps -= chunk;
     }
@@ -1358,7 +1355,7 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
     for (int m : {(int)kModeStream, (int)kModeResident}) {
         if (saved_mode != kModeAuto && m != saved_mode) continue;  // a forced kernel keeps its mode
         for (uint32_t c = 0; c < count; ++c) {
-            const int occ = step_occupancy(int_ring_, adex_, blocks[c], npts[c]);
+            const int occ = step_occupancy(int_ring_, adex_, multi_net, blocks[c], npts[c]);
             for (int half = 0; half < 2; ++half) {
                 if (half && (m == kModeResident || occ < 2)) continue;
                 TileShape s;

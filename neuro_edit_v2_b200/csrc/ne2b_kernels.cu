@@ -18,8 +18,7 @@ __global__ void advance_kernel(NetDev *nets, uint32_t n_nets, uint32_t steps) {
     if (!(nd.flags & kNetActive)) return;
     unsigned long long t = nd.t + steps;
     if (t > nd.t_end) t = nd.t_end;
-    nd.t = t;
-    nd.tmod = (uint32_t)(t % nd.D);
+    set_step(nd, t);
 }
 
 // reset_state for one net (cpu.rs:158-183): state rows from v0/u0, zeros.
@@ -101,13 +100,13 @@ bool pdl_enabled() { return g_pdl; }
     ((int_ring) ? ((adex) ? StepKind<true, true>::call : StepKind<true, false>::call) \
                 : ((adex) ? StepKind<false, true>::call : StepKind<false, false>::call))
 
-int step_occupancy(bool int_ring, bool adex, uint32_t block, uint32_t npt) {
-    return NE2B_KIND(int_ring, adex, occupancy(block, npt));
+int step_occupancy(bool int_ring, bool adex, bool multi, uint32_t block, uint32_t npt) {
+    return NE2B_KIND(int_ring, adex, occupancy(block, npt, multi));
 }
 
-cudaError_t launch_step(bool int_ring, bool adex, uint32_t block, uint32_t npt, const EngineDev *eng,
+cudaError_t launch_step(bool int_ring, bool adex, bool multi, uint32_t block, uint32_t npt, const EngineDev *eng,
                         uint32_t k_step, uint32_t grid, cudaStream_t st) {
-    return NE2B_KIND(int_ring, adex, launch(block, npt, eng, k_step, grid, st));
+    return NE2B_KIND(int_ring, adex, launch(block, npt, multi, eng, k_step, grid, st));
 }
 
 uint32_t resident_head(uint32_t block, uint32_t npt) {

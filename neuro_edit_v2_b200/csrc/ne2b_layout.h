@@ -117,7 +117,30 @@ struct alignas(16) NetDev {
     float dt, pkick, kick, decay_s, decay_t, gauss_k;
     uint32_t trace_last;  // last index of trace_tab (saturation)
     uint32_t xwords;      // ceil(nx / 32)
+    // phases of t kept beside it (set_step), so a step finds its record row
+    // and window without a division: rphase = t % rec_rows, wphase =
+    // (t + 1) % win_steps, widx0 = (t + 1) / win_steps
+    uint32_t rphase, wphase, widx0;
 };
+
+#ifdef __CUDACC__
+#define NE2B_HD __host__ __device__
+#else
+#define NE2B_HD
+#endif
+// Sets t and every phase derived from it (tmod, rphase, wphase, widx0).
+NE2B_HD inline void set_step(NetDev &d, unsigned long long t) {
+    d.t = t;
+    d.tmod = (uint32_t)(t % d.D);
+    d.rphase = d.rec_rows ? (uint32_t)(t % d.rec_rows) : 0u;
+    if (d.win_steps) {
+        d.wphase = (uint32_t)((t + 1) % d.win_steps);
+        const unsigned long long w = (t + 1) / d.win_steps;
+        d.widx0 = w > 0xffffffffull ? 0xffffffffu : (uint32_t)w;
+    } else {
+        d.wphase = d.widx0 = 0u;
+    }
+}
 
 // Mutable per-net counters, kept apart from the read-mostly descriptor.
 struct NetCounters {

@@ -55,13 +55,16 @@ __device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, u
 }
 
 // `nd` is the tile's net descriptor (global memory, or a shared-memory copy
-// staged before the launch's dependency wait); `t` is the absolute step and
-// `tmod` = t % D.  ADEX: the net holds AdEx rows (else the Izhikevich path is
+// staged before the launch's dependency wait); `t` is the absolute step,
+// `tmod` = t % D and `k` = t - nd.t (the step within the launch group).
+// PHASES: the record row and the window come from the phases the
+// descriptor keeps beside its t, with a division only when a phase wraps
+// within the group (else t % rec_rows and (t + 1) / win_steps directly).  ADEX: the net holds AdEx rows (else the Izhikevich path is
 // the only one compiled into this instance).
 // `ptab` is the parameter table (a shared-memory copy when it is small).
-template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX>
+template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES>
 __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
-                                             const Tile &tile, uint64_t t, uint32_t tmod, float *vs, float *us,
+                                             const Tile &tile, uint64_t t, uint32_t tmod, uint32_t k, float *vs, float *us,
                                              float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
@@ -84,8 +87,18 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     bool win_end = false;
     uint32_t widx = 0;
     if (windows) {
-        win_end = mod_steps(t + 1, nd.win_steps) == 0u;
-        widx = (uint32_t)div_steps(t + 1, nd.win_steps) - 1u;
+        if constexpr (PHASES) {
+            uint32_t ph = nd.wphase + k, wi = nd.widx0;
+            if (ph >= nd.win_steps) {
+                wi += ph / nd.win_steps;
+                ph %= nd.win_steps;
+            }
+            win_end = ph == 0u;
+            widx = wi - 1u;
+        } else {
+            win_end = mod_steps(t + 1, nd.win_steps) == 0u;
+            widx = (uint32_t)div_steps(t + 1, nd.win_steps) - 1u;
+        }
     }
 
     uint32_t li[NPT];
@@ -236,7 +249,13 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
 
     // ---- spike record: one ballot word per warp and q
     if (flags & kNetRecord) {
-        const uint32_t row = mod_steps(t, nd.rec_rows);
+        uint32_t row;
+        if constexpr (PHASES) {
+            row = nd.rphase + k;
+            if (row >= nd.rec_rows) row %= nd.rec_rows;
+        } else {
+            row = mod_steps(t, nd.rec_rows);
+        }
         const uint32_t words32 = n_pad >> 5;
 #pragma unroll
         for (int q = 0; q < NPT; ++q) {
@@ -376,48 +395,106 @@ __device__ __forceinline__ void stage_net(const EngineDev *__restrict__ eng, uin
 }
 
 // ------------------------------------------------------ streaming kernel
-// The tile list and the net descriptors are written by host copies, which
-// a launch always follows in full, and by advance_kernel (`t`, `tmod`),
-// after which the next step launch is never programmatic (launch_step
-// gives k_step = 0 a plain stream dependency).  So every block reads its
-// first tile and stages the net descriptor, t included, before the
-// dependency wait, overlapping the previous step's tail; after the wait
-// only the step's own data is read.  The descriptor is restaged only when
-// the net changes from one tile to the next.
-template <bool INT, int BLOCK, int NPT, bool ADEX>
+// Block b processes tiles b, b + G, b + 2G, ... (G = gridDim.x).  The tile
+// list and the net descriptors are written by host copies, which a launch
+// always follows in full, and by advance_kernel (`t` and its phases), after
+// which the next step launch is never programmatic (launch_step gives
+// k_step = 0 a plain stream dependency).  So every block reads its first
+// tile and stages the net descriptor, t included, before the dependency
+// wait, overlapping the previous step's tail; after the wait only the
+// step's own data is read.
+//
+// MULTI (engines of many nets: batches, the server): the block's tiles
+// mostly belong to different nets, so it stages the records of its first
+// kStageTiles tiles, and the descriptor of each net among them, before the
+// wait as well: after the wait a tile costs one dependent round trip (its
+// state) instead of three (record, descriptor, state).  The tile being
+// processed reads its descriptor from one fixed shared-memory copy, refilled
+// from the staged one when the net changes; tiles past the staged ones load
+// their record and descriptor as they come.  Single-net engines restage the
+// descriptor only when the net changes, which it never does.
+constexpr uint32_t kStageTiles = 16;
+
+template <bool INT, int BLOCK, int NPT, bool ADEX, bool MULTI>
 __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
     pdl_trigger();
+    constexpr uint32_t kNetWords = sizeof(NetDev) / 16;
     __shared__ uint32_t s_lists[smem_lists_words<BLOCK, NPT>()];
     __shared__ __align__(16) NetDev s_nd;
     __shared__ __align__(16) ParamRow s_ptab[kSmemParamRows];
     static_assert(sizeof(NetDev) % 16 == 0 && sizeof(ParamRow) % 16 == 0, "16-byte staging");
-    static_assert(sizeof(NetDev) / 16 <= BLOCK, "one 16-byte word per thread");
+    static_assert(kNetWords <= BLOCK && kStageTiles <= BLOCK, "one 16-byte word per thread");
     const SmemLists sl = smem_lists(s_lists, BLOCK * NPT, BLOCK / 32);
     const uint32_t n_tiles = eng->n_tiles;
-    uint32_t tix = blockIdx.x;
-    if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
-    Tile tile = eng->tiles[tix];
-    stage_net(eng, tile.net, &s_nd);
-    const ParamRow *ptab = stage_params<BLOCK>(eng, s_ptab);
-    __syncthreads();
-    pdl_wait();
-    for (;;) {
-        const uint32_t nx = tix + gridDim.x;
-        const uint64_t t = s_nd.t + k_step;
-        uint32_t tmod = s_nd.tmod + k_step;
-        if (tmod >= s_nd.D) tmod %= s_nd.D;
-        process_tile<INT, BLOCK, NPT, false, ADEX>(eng, ptab, s_nd, tile, t, tmod, s_nd.v + tile.start,
-                                                  s_nd.u + tile.start, s_nd.s + tile.start, s_nd.tk + tile.start,
-                                                  s_nd.pidx + tile.start, sl);
-        if (nx >= n_tiles) break;
-        const Tile next = eng->tiles[nx];
-        if (next.net != tile.net) {
-            __syncthreads();  // every thread is done with the staged descriptor
-            stage_net(eng, next.net, &s_nd);
-            __syncthreads();
+    if constexpr (!MULTI) {
+        uint32_t tix = blockIdx.x;
+        if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
+        Tile tile = eng->tiles[tix];
+        stage_net(eng, tile.net, &s_nd);
+        const ParamRow *ptab = stage_params<BLOCK>(eng, s_ptab);
+        __syncthreads();
+        pdl_wait();
+        for (;;) {
+            const uint32_t nx = tix + gridDim.x;
+            const uint64_t t = s_nd.t + k_step;
+            uint32_t tmod = s_nd.tmod + k_step;
+            if (tmod >= s_nd.D) tmod %= s_nd.D;
+            process_tile<INT, BLOCK, NPT, false, ADEX, false>(eng, ptab, s_nd, tile, t, tmod, k_step,
+                                                             s_nd.v + tile.start, s_nd.u + tile.start,
+                                                             s_nd.s + tile.start, s_nd.tk + tile.start,
+                                                             s_nd.pidx + tile.start, sl);
+            if (nx >= n_tiles) break;
+            const Tile next = eng->tiles[nx];
+            if (next.net != tile.net) {
+                __syncthreads();  // every thread is done with the staged descriptor
+                stage_net(eng, next.net, &s_nd);
+                __syncthreads();
+            }
+            tix = nx;
+            tile = next;
         }
-        tix = nx;
-        tile = next;
+    } else {
+        __shared__ __align__(16) NetDev s_stage[kStageTiles];  // slot j: tile j's net, where it changes
+        __shared__ __align__(16) Tile s_tile[kStageTiles];
+        const uint32_t G = gridDim.x, b = blockIdx.x;
+        if (b >= n_tiles) return;  // a fixed grid larger than the tile list
+        const uint32_t m = (n_tiles - b + G - 1) / G;  // this block's tiles
+        const uint32_t ms = m < kStageTiles ? m : kStageTiles;
+        if (threadIdx.x < ms) s_tile[threadIdx.x] = eng->tiles[b + threadIdx.x * G];
+        const ParamRow *ptab = stage_params<BLOCK>(eng, s_ptab);
+        __syncthreads();
+        for (uint32_t w = threadIdx.x; w < ms * kNetWords; w += BLOCK) {
+            const uint32_t j = w / kNetWords, q = w - j * kNetWords;
+            const uint32_t net = s_tile[j].net;
+            const uint4 word = reinterpret_cast<const uint4 *>(eng->nets + net)[q];
+            if (j == 0) reinterpret_cast<uint4 *>(&s_nd)[q] = word;
+            else if (net != s_tile[j - 1].net) reinterpret_cast<uint4 *>(&s_stage[j])[q] = word;
+        }
+        __syncthreads();
+        pdl_wait();
+        uint32_t net = s_tile[0].net;
+        for (uint32_t j = 0; j < m; ++j) {
+            const Tile tile = j < kStageTiles ? s_tile[j] : eng->tiles[b + j * G];
+            if (tile.net != net) {
+                __syncthreads();  // every thread is done with the current descriptor
+                if (j < kStageTiles) {
+                    if (threadIdx.x < kNetWords)
+                        reinterpret_cast<uint4 *>(&s_nd)[threadIdx.x] =
+                            reinterpret_cast<const uint4 *>(&s_stage[j])[threadIdx.x];
+                } else {
+                    stage_net(eng, tile.net, &s_nd);
+                }
+                __syncthreads();
+                net = tile.net;
+            }
+            const uint64_t t = s_nd.t + k_step;
+            uint32_t tmod = s_nd.tmod + k_step;
+            if (tmod >= s_nd.D) tmod %= s_nd.D;
+            process_tile<INT, BLOCK, NPT, false, ADEX, true>(eng, ptab, s_nd, tile, t, tmod, k_step,
+                                                            s_nd.v + tile.start, s_nd.u + tile.start,
+                                                            s_nd.s + tile.start, s_nd.tk + tile.start,
+                                                            s_nd.pidx + tile.start, sl);
+        }
     }
 }
 
@@ -521,8 +598,8 @@ __global__ void __launch_bounds__(BLOCK) resident_kernel(const EngineDev *__rest
             const uint64_t t = nd.t + k0 + k;
             uint32_t tmod = nd.tmod + k0 + k;
             if (tmod >= nd.D) tmod %= nd.D;
-            process_tile<INT, BLOCK, NPT, true, ADEX>(eng, ptab, nd, tile, t, tmod, sv + o, su + o, ss + o,
-                                                      stk + o, spi + o, sl);
+            process_tile<INT, BLOCK, NPT, true, ADEX, false>(eng, ptab, nd, tile, t, tmod, k0 + k, sv + o, su + o,
+                                                             ss + o, stk + o, spi + o, sl);
         }
         if (k + 1 < nsteps && !grid_barrier(eng->barrier, (k + 1) * gridDim.x, eng->err, s_flag)) break;
     }
@@ -559,12 +636,13 @@ static cudaError_t launch_pdl(void (*kernel)(Args...), uint32_t grid, uint32_t b
 }
 
 template <bool INT, bool ADEX>
-int StepKind<INT, ADEX>::occupancy(uint32_t block, uint32_t npt) {
-#define X(B, P)                                                                                    \
-    if (block == B && npt == P) {                                                                  \
-        int b = 0;                                                                                 \
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX>, B, 0);     \
-        return b;                                                                                  \
+int StepKind<INT, ADEX>::occupancy(uint32_t block, uint32_t npt, bool multi) {
+#define X(B, P)                                                                                           \
+    if (block == B && npt == P) {                                                                         \
+        int b = 0;                                                                                        \
+        if (multi) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX, true>, B, 0); \
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX, false>, B, 0);      \
+        return b;                                                                                         \
     }
     NE2B_SHAPES(X)
 #undef X
@@ -572,10 +650,12 @@ int StepKind<INT, ADEX>::occupancy(uint32_t block, uint32_t npt) {
 }
 
 template <bool INT, bool ADEX>
-cudaError_t StepKind<INT, ADEX>::launch(uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step,
-                                        uint32_t grid, cudaStream_t st) {
-#define X(B, P) \
-    if (block == B && npt == P) return launch_pdl(step_kernel<INT, B, P, ADEX>, grid, B, st, k_step > 0, eng, k_step);
+cudaError_t StepKind<INT, ADEX>::launch(uint32_t block, uint32_t npt, bool multi, const EngineDev *eng,
+                                        uint32_t k_step, uint32_t grid, cudaStream_t st) {
+#define X(B, P)                                                                                                   \
+    if (block == B && npt == P)                                                                                   \
+        return multi ? launch_pdl(step_kernel<INT, B, P, ADEX, true>, grid, B, st, k_step > 0, eng, k_step)      \
+                     : launch_pdl(step_kernel<INT, B, P, ADEX, false>, grid, B, st, k_step > 0, eng, k_step);
     NE2B_SHAPES(X)
 #undef X
     return cudaErrorInvalidValue;

@@ -31,9 +31,10 @@ __host__ __device__ constexpr uint32_t resident_head_bytes() {
 
 template <bool INT, bool ADEX>
 struct StepKind {
-    static int occupancy(uint32_t block, uint32_t npt);
-    static cudaError_t launch(uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k_step, uint32_t grid,
-                              cudaStream_t st);
+    // multi: the streaming kernel instance for engines of many nets
+    static int occupancy(uint32_t block, uint32_t npt, bool multi);
+    static cudaError_t launch(uint32_t block, uint32_t npt, bool multi, const EngineDev *eng, uint32_t k_step,
+                              uint32_t grid, cudaStream_t st);
     static int resident_occupancy(uint32_t block, uint32_t npt, size_t smem);
     static cudaError_t launch_resident(uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k0,
                                        uint32_t nsteps, uint32_t grid, size_t smem, cudaStream_t st);

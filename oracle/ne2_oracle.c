@@ -14,6 +14,7 @@
 #include "ne2_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -540,6 +541,56 @@ float ne2o_det_expf(float x) {
     double scale;
     memcpy(&scale, &bits, sizeof scale);
     return (float)(p * scale);
+}
+
+struct expf_job {
+    float (*f)(float);
+    uint32_t lo_bits, hi_bits; /* ordered float keys, see expf_key */
+    uint32_t stride, first, step;
+    uint64_t bad, checked;
+};
+/* total order of float bit patterns as unsigned keys: -x < -0 < +0 < x */
+static uint32_t expf_key(float x) {
+    uint32_t b;
+    memcpy(&b, &x, sizeof b);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+static float expf_unkey(uint32_t k) {
+    uint32_t b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    float x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+}
+static void *expf_worker(void *arg) {
+    struct expf_job *j = (struct expf_job *)arg;
+    for (uint64_t k = (uint64_t)j->lo_bits + (uint64_t)j->first * j->stride; k <= j->hi_bits;
+         k += (uint64_t)j->step * j->stride) {
+        const float x = expf_unkey((uint32_t)k);
+        const float a = j->f(x), b = ne2o_det_expf(x);
+        j->checked++;
+        if (memcmp(&a, &b, sizeof a) != 0) j->bad++;
+    }
+    return NULL;
+}
+uint64_t ne2o_expf_mismatches(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
+                              uint64_t *checked) {
+    if (threads < 1) threads = 1;
+    if (threads > 64) threads = 64;
+    if (stride < 1) stride = 1;
+    struct expf_job jobs[64];
+    pthread_t th[64];
+    for (uint32_t i = 0; i < threads; ++i) {
+        jobs[i] = (struct expf_job){f, expf_key(lo), expf_key(hi), stride, i, threads, 0, 0};
+        pthread_create(&th[i], NULL, expf_worker, &jobs[i]);
+    }
+    uint64_t bad = 0, n = 0;
+    for (uint32_t i = 0; i < threads; ++i) {
+        pthread_join(th[i], NULL);
+        bad += jobs[i].bad;
+        n += jobs[i].checked;
+    }
+    if (checked) *checked = n;
+    return bad;
 }
 
 /* ================================================================ sim */

@@ -123,6 +123,11 @@ float    ne2o_gauss_scale(float sd);
 
 /* deterministic exp shared with the device kernels */
 float ne2o_det_expf(float x);
+/* test support: compares f with ne2o_det_expf bit for bit on every
+ * `stride`-th float in [lo, hi] (by bit pattern, both signs), split over
+ * `threads` threads; returns the mismatches and stores the values checked */
+uint64_t ne2o_expf_mismatches(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
+                              uint64_t *checked);
 
 /* --------------------------------------------------------------- sim */
 typedef struct {

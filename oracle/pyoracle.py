@@ -80,6 +80,7 @@ def lib() -> C.CDLL:
             "ne2o_gauss_numer": (C.c_int64, [u32, u64, u64]),
             "ne2o_gauss_scale": (f32, [f32]),
             "ne2o_det_expf": (f32, [f32]),
+            "ne2o_expf_mismatches": (u64, [vp, f32, f32, u32, u32, vp]),
             "ne2o_cfg_default": (None, [vp]),
             "ne2o_sim_new": (vp, [vp, vp, C.c_char_p, C.c_size_t]),
             "ne2o_sim_free": (None, [vp]), "ne2o_sim_step": (None, [vp]),

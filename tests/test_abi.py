@@ -125,6 +125,22 @@ def test_host_expf_matches_oracle_det_expf():
         assert a == b, x
 
 
+def test_host_expf_equals_oracle_on_a_stride_of_all_floats():
+    """The library's host copy of the device exp equals the oracle's, which
+    is the correctly rounded exp, on every 64th float of [-104, 88.8] (every
+    float with NE2B_EXHAUSTIVE_EXP=1: 2,239,863,196 values)."""
+    key = lambda x: (lambda b: (~b & 0xFFFFFFFF) if b >> 31 else b | 0x80000000)(
+        struct.unpack("<I", struct.pack("<f", x))[0])
+    n = key(88.8) - key(-104.0) + 1
+    assert n == 2_239_863_196
+    stride = 1 if os.environ.get("NE2B_EXHAUSTIVE_EXP") == "1" else 64
+    fn = ctypes.cast(nb._abi.lib.ne2b_expf, ctypes.c_void_p)
+    checked = ctypes.c_uint64()
+    bad = O.lib().ne2o_expf_mismatches(fn, -104.0, 88.8, stride, os.cpu_count() or 1, ctypes.byref(checked))
+    assert checked.value == (n + stride - 1) // stride
+    assert bad == 0
+
+
 def test_request_footprint_needs_no_gpu():
     net = nb.liquid(10, 1)
     cfg = nb.default_config(int_weights=1, window_steps=500)

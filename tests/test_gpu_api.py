@@ -164,6 +164,33 @@ def test_window_counts_equal_sliding_spike_counts():
     assert g.windows_done() == 6
 
 
+@pytest.mark.parametrize("ws, rec", [(1, 2), (7, 5), (100, 64), (250, 300)])
+def test_windows_and_record_rows_wrapping_inside_a_launch_group(ws, rec):
+    """Windows and record rings shorter than a launch group (64 steps) wrap
+    several times inside one group: each window's count equals the oracle's
+    spikes over that window's steps, and the last `rec` record rows equal
+    the oracle's."""
+    onet = O.ONet.bench_net(2000, 40, 3, 0.7, 5.0)
+    steps = 600
+    n_win = steps // ws
+    g = nb.B200Sim(onet.flat(), record_spikes=1, spike_record_steps=rec, int_weights=1, noise_rate_hz=500.0,
+                   window_steps=ws, max_windows=n_win)
+    o = O.OSim(onet, O.cfg(record_spikes=1, spike_record_steps=steps, int_weights=1, noise_rate_hz=500.0))
+    g.run_steps(37)  # the groups then start mid-window
+    g.run_steps(steps - 37)
+    o.run_steps(steps)
+    assert g.windows_done() == n_win
+    n = onet.n
+    bits = lambda words: np.unpackbits(words.view(np.uint8), bitorder="little")[:n].astype(np.int64)
+    rows = np.stack([bits(o.spike_row(steps - 1 - t)) for t in range(steps)])  # [step, neuron]
+    for w in range(n_win):
+        ref = rows[w * ws:(w + 1) * ws].sum(axis=0)
+        assert np.array_equal(g.window_counts(w).astype(np.int64), np.minimum(ref, 65535)), w
+    for back in range(rec):
+        assert np.array_equal(g.spike_row(back), o.spike_row(back)), back
+    assert g.spikes_total() == o.spikes_total() > 0
+
+
 def test_sim_autotune_restores_state_and_keeps_results():
     """Autotuning times candidate kernels on device snapshots and restores
     the state: a tuned sim continues bit-identically to an untuned one."""

@@ -61,6 +61,49 @@ def test_batch_equals_alone_and_oracle():
             assert np.array_equal(b.window_counts(k, w).astype(np.uint32), o.spike_counts(WIN)), (k, w)
 
 
+def test_batch_with_more_tiles_per_block_than_staged_equals_default_grid():
+    """One block per SM gives every block more tiles than the streaming
+    kernel stages before its dependency wait (16), from many nets: the tiles
+    past the staged ones load their records and net descriptors as they
+    come.  Results equal those of another tiling bit for bit, and the
+    oracle's on an izh and an AdEx net."""
+    import torch
+
+    steps, n_nets, side = 300, 200, 12
+    models = [nb.MODEL_ADEX if k % 3 == 0 else nb.MODEL_IZH for k in range(n_nets)]
+    nets = [nb.liquid(side, 300 + k, model=models[k]) for k in range(n_nets)]
+    cfgs = [cfg(11 + k) for k in range(n_nets)]
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert n_nets * -(-side**3 // 128) > 16 * sms  # tiles of 128 neurons per block of a one-per-SM grid
+    a, b = nb.Batch(nets, cfgs), nb.Batch(nets, cfgs)
+    for bb in (a, b):
+        bb.set_kernel_mode(nb.KERNEL_STREAM)
+        for k in range(n_nets):
+            x = streams(k, steps)
+            for i in range(8):
+                bb.play_input(k, i, x[:, i])
+    a.set_tile_shape(128, 1, 1)
+    b.set_tile_shape(256, 2, 0)
+    a.run_steps(steps)
+    b.run_steps(steps)
+    for k in range(n_nets):
+        for w in range(steps // WIN):
+            assert np.array_equal(a.window_counts(k, w), b.window_counts(k, w)), (k, w)
+        assert a.spikes_total(k) == b.spikes_total(k)
+        assert np.array_equal(a.state(k, 0).view(np.uint32), b.state(k, 0).view(np.uint32)), k
+    assert sum(a.spikes_total(k) for k in range(n_nets)) > 0
+    for k in (0, 1):
+        onet = O.ONet.liquid(side, 300 + k, model=O.ADEX if models[k] == nb.MODEL_ADEX else O.IZH)
+        o = O.OSim(onet, O.cfg(int_weights=1, record_spikes=1, spike_record_steps=WIN, seed=11 + k, gauss_sd=0.5,
+                               exp_mode=1))
+        x = streams(k, steps)
+        for i in range(8):
+            o.play_input(i, x[:, i])
+        for w in range(steps // WIN):
+            o.run_steps(WIN)
+            assert np.array_equal(a.window_counts(k, w).astype(np.uint32), o.spike_counts(WIN)), (k, w)
+
+
 def test_batch_autotune_keeps_results():
     nets = liquids()[:4]
     cfgs = [cfg(3 + k) for k in range(4)]

@@ -129,6 +129,14 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
 #pragma unroll
         for (int q = 0; q < NPT; ++q)
             if (valid[q] && (lane & 7) == 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(nrow + li[q]));
+        // and the next step's input values: a new row every step, which
+        // would otherwise be a DRAM miss in the stimulated tiles
+        if (has_stim) {
+            const long long rel = (long long)t + 1 - nd.stim_t0;
+            if (rel >= 0 && rel < (long long)nd.stim_len)
+                for (uint32_t c = threadIdx.x * 8u; c < nd.n_inputs; c += BLOCK * 8u)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(nd.stim_buf + (size_t)rel * nd.n_inputs + c));
+        }
     }
 
     bool spk[NPT];

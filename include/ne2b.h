@@ -96,6 +96,27 @@ typedef struct ne2b_sim ne2b_sim;
 ne2b_status ne2b_create(const ne2b_net_desc *net, const ne2b_config *cfg, int device, ne2b_sim **out);
 ne2b_status ne2b_destroy(ne2b_sim *sim);
 
+/* Network::synapse_csr (net-format/src/network.rs:654-692) built on the
+ * GPU, straight into a new sim.  `net` carries the neurons (n, model, params,
+ * param_stride, x0) and the stimulus map; its CSR fields (n_syn, src_ptr,
+ * tgt, w, delay_steps, tau_ms) must be 0/NULL.  The synapse list
+ * src/tgt/w/delay_ms[n_syn], in any order, is copied to the device and
+ * sorted there by source, stably (a source's synapses keep their list
+ * order), with Dale's sign from kind[n] (1 = inhibitory) and delays of
+ * max(1, roundf(ms / cfg->dt_ms)) steps, at most 65535.  The sim equals
+ * ne2b_net_from_synapses (same arrays, dt = cfg->dt_ms) followed by
+ * ne2b_create, bit for bit, and the same errors are reported.  No
+ * per-synapse tau: nets with their own synapse currents use the host
+ * build. */
+ne2b_status ne2b_create_from_synapses(const ne2b_net_desc *net, const uint8_t *kind, uint64_t n_syn,
+                                      const uint32_t *src, const uint32_t *tgt, const float *w,
+                                      const float *delay_ms, const ne2b_config *cfg, int device, ne2b_sim **out);
+/* The sim's synapse CSR as it sits on the device: rowptr[n + 1], tgt[E],
+ * w_bits[E] (the int32 fixed-point weight with the int ring, else the f32
+ * bits) and delay_steps[E]; E from ne2b_syn_count.  NULL skips an array. */
+ne2b_status ne2b_syn_count(const ne2b_sim *sim, uint64_t *e);
+ne2b_status ne2b_read_csr(ne2b_sim *sim, uint32_t *rowptr, uint32_t *tgt, uint32_t *w_bits, uint16_t *delay_steps);
+
 ne2b_status ne2b_n(const ne2b_sim *sim, uint32_t *n);                 /* Backend::n */
 ne2b_status ne2b_step_count(const ne2b_sim *sim, uint64_t *t);        /* Backend::step_count */
 ne2b_status ne2b_time_ms(const ne2b_sim *sim, double *ms);            /* Backend::time_ms */

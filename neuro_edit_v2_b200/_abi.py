@@ -134,6 +134,10 @@ _SIGS = {
     "ne2b_version": (C.c_char_p, []),
     "ne2b_create": (C.c_int, [C.POINTER(NetDesc), C.POINTER(Config), C.c_int, C.POINTER(_p)]),
     "ne2b_destroy": (C.c_int, [_p]),
+    "ne2b_create_from_synapses": (C.c_int, [C.POINTER(NetDesc), _p, _u64, _p, _p, _p, _p, C.POINTER(Config), C.c_int,
+                                            C.POINTER(_p)]),
+    "ne2b_syn_count": (C.c_int, [_p, _pu64]),
+    "ne2b_read_csr": (C.c_int, [_p, _p, _p, _p, _p]),
     "ne2b_n": (C.c_int, [_p, _pu32]),
     "ne2b_step_count": (C.c_int, [_p, _pu64]),
     "ne2b_time_ms": (C.c_int, [_p, _pf64]),

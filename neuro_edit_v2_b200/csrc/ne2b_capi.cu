@@ -84,6 +84,130 @@ ne2b_status ne2b_destroy(ne2b_sim *sim) {
     return NE2B_OK;
 }
 
+}  // extern "C"
+
+// The synapse list on the device, checked by the prepass, then the net
+// built with its CSR sorted into place there (csrc/ne2b_csr.cu).  Errors
+// are the host build's (ne2b_net_from_synapses).
+static ne2b_status create_from_list(ne2b::Engine &eng, const ne2b_net_desc *net, const uint8_t *kind, uint64_t E,
+                                    const uint32_t *src, const uint32_t *tgt, const float *w, const float *dly,
+                                    const ne2b_config *cfg, uint32_t *slot) {
+    using namespace ne2b;
+    const cudaStream_t st = eng.stream();
+    const uint32_t n = net->n;
+    std::vector<void *> tmp;
+    auto release = [&]() {
+        for (void *p : tmp) cudaFreeAsync(p, st);
+        cudaStreamSynchronize(st);
+    };
+    auto dalloc = [&](size_t bytes, void **p) -> ne2b_status {
+        *p = nullptr;
+        const cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, st);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync (synapse list)");
+        tmp.push_back(*p);
+        return NE2B_OK;
+    };
+#define LIST_TRY(x)                          \
+    do {                                     \
+        const ne2b_status _s = (x);          \
+        if (_s != NE2B_OK) {                 \
+            release();                       \
+            return _s;                       \
+        }                                    \
+    } while (0)
+    DevCsrBuild dc;
+    void *p = nullptr;
+    LIST_TRY(dalloc(4 * E, &p)); dc.syn.src = (const uint32_t *)p;
+    LIST_TRY(dalloc(4 * E, &p)); dc.syn.tgt = (const uint32_t *)p;
+    LIST_TRY(dalloc(4 * E, &p)); dc.syn.w = (const float *)p;
+    LIST_TRY(dalloc(4 * E, &p)); dc.syn.delay_ms = (const float *)p;
+    LIST_TRY(dalloc(n, &p)); dc.syn.kind = (const uint8_t *)p;
+    LIST_TRY(dalloc(2 * E, &p)); dc.steps = (const uint16_t *)p;
+    LIST_TRY(dalloc(4 * (size_t)n, &p)); dc.counts = (const uint32_t *)p;
+    LIST_TRY(dalloc(4 * (size_t)n, &p)); dc.cursor = (uint32_t *)p;
+    LIST_TRY(dalloc(4 * (size_t)csr_scan_blocks(n), &p)); dc.sums = (uint32_t *)p;
+    const uint64_t chunks = csr_chunks(E);
+    LIST_TRY(dalloc(4 * (chunks + 1), &p)); dc.ticket = (uint32_t *)p;
+    dc.done = dc.ticket + 1;
+    LIST_TRY(dalloc(sizeof(CsrScalars), &p)); dc.sc = (CsrScalars *)p;
+    dc.syn.n_syn = E;
+    dc.syn.n = n;
+    dc.syn.dt_ms = cfg->dt_ms;
+    CsrScalars sc{~0ull, ~0ull, 1u, 0u};
+    if (E) {
+        LIST_TRY(eng.pin_copy((void *)dc.syn.src, src, 4 * E));
+        LIST_TRY(eng.pin_copy((void *)dc.syn.tgt, tgt, 4 * E));
+        LIST_TRY(eng.pin_copy((void *)dc.syn.w, w, 4 * E));
+        LIST_TRY(eng.pin_copy((void *)dc.syn.delay_ms, dly, 4 * E));
+    }
+    if (n) LIST_TRY(eng.pin_copy((void *)dc.syn.kind, kind, n));
+    LIST_TRY(eng.pin_copy(dc.sc, &sc, sizeof sc));
+    LIST_TRY(eng.pin_close());
+    LIST_TRY(cuda_error(cudaMemsetAsync((void *)dc.counts, 0, 4 * (size_t)n, st), "memset counts"));
+    LIST_TRY(cuda_error(cudaMemsetAsync(dc.ticket, 0, 4 * (chunks + 1), st), "memset tickets"));
+    LIST_TRY(cuda_error(csr_prepass(dc.syn, (uint32_t *)dc.counts, (uint16_t *)dc.steps, dc.sc, st), "csr prepass"));
+    LIST_TRY(cuda_error(cudaMemcpyAsync(&sc, dc.sc, sizeof sc, cudaMemcpyDeviceToHost, st), "prepass readback"));
+    LIST_TRY(cuda_error(cudaStreamSynchronize(st), "prepass"));
+    if (sc.bad_ref != ~0ull) {
+        const uint64_t j = sc.bad_ref;
+        LIST_TRY(set_error(NE2B_EINVAL, "synapse %llu references %u -> %u but only %u neurons exist",
+                           (unsigned long long)j, src[j], tgt[j], n));
+    }
+    if (sc.bad_delay != ~0ull) {
+        const uint64_t j = sc.bad_delay;
+        LIST_TRY(set_error(NE2B_EINVAL, "synapse %u -> %u: delay %g ms at dt %g ms exceeds the 65535-step ring", src[j],
+                           tgt[j], (double)dly[j], (double)cfg->dt_ms));
+    }
+    dc.max_delay = sc.max_delay;
+    LIST_TRY(eng.add_net_device_csr(net, cfg, dc, slot));
+    LIST_TRY(cuda_error(cudaMemcpyAsync(&sc, dc.sc, sizeof sc, cudaMemcpyDeviceToHost, st), "scatter readback"));
+    LIST_TRY(cuda_error(cudaStreamSynchronize(st), "device CSR build"));
+    release();
+#undef LIST_TRY
+    if (sc.timeout) return set_error(NE2B_ECUDA, "device CSR build: a scatter block's wait exceeded its limit");
+    return NE2B_OK;
+}
+
+extern "C" {
+
+ne2b_status ne2b_create_from_synapses(const ne2b_net_desc *net, const uint8_t *kind, uint64_t n_syn,
+                                      const uint32_t *src, const uint32_t *tgt, const float *w,
+                                      const float *delay_ms, const ne2b_config *cfg, int device, ne2b_sim **out) {
+    if (!out || !net || !cfg) return set_error(NE2B_EINVAL, "ne2b_create_from_synapses: null argument");
+    *out = nullptr;
+    if (net->n_syn || net->src_ptr || net->tgt || net->w || net->delay_steps || net->tau_ms)
+        return set_error(NE2B_EINVAL, "the net's CSR fields must be empty: its synapses come as a list");
+    if (net->n && (!net->model || !net->params || !kind))
+        return set_error(NE2B_EINVAL, "model, params and kind are required");
+    if (n_syn && (!src || !tgt || !w || !delay_ms)) return set_error(NE2B_EINVAL, "synapse arrays are required");
+    if (n_syn > 0xffffffffull) return set_error(NE2B_UNSUPPORTED, "more than 2^32-1 synapses");
+    if (!(cfg->dt_ms >= 0.001f && cfg->dt_ms <= 100.0f))  // lib.rs:35-39 valid_dt_ms
+        return set_error(NE2B_EINVAL, "dt_ms %g outside [0.001, 100]", (double)cfg->dt_ms);
+    GUARD(([&]() -> ne2b_status {
+        ne2b_sim *s = new ne2b_sim();
+        ne2b_status st = s->eng.init(device, cfg->int_weights != 0, 1);
+        if (st == NE2B_OK) st = create_from_list(s->eng, net, kind, n_syn, src, tgt, w, delay_ms, cfg, &s->slot);
+        if (st != NE2B_OK) {
+            delete s;
+            return st;
+        }
+        *out = s;
+        return NE2B_OK;
+    })());
+}
+
+ne2b_status ne2b_syn_count(const ne2b_sim *sim, uint64_t *e) {
+    CHECK_SIM(const_cast<ne2b_sim *>(sim));
+    if (!e) return set_error(NE2B_EINVAL, "null argument");
+    *e = h->e;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_read_csr(ne2b_sim *sim, uint32_t *rowptr, uint32_t *tgt, uint32_t *w_bits, uint16_t *delay_steps) {
+    CHECK_SIM(sim);
+    GUARD(sim->eng.read_csr(*h, rowptr, tgt, w_bits, delay_steps));
+}
+
 ne2b_status ne2b_n(const ne2b_sim *sim, uint32_t *n) {
     CHECK_SIM(const_cast<ne2b_sim *>(sim));
     *n = h->n;

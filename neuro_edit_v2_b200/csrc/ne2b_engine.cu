@@ -344,8 +344,17 @@ ne2b_status Engine::attach_net(NetHost *h, uint32_t *slot_out, bool rebuild) {
     return NE2B_OK;
 }
 
+ne2b_status Engine::add_net_device_csr(const ne2b_net_desc *net, const ne2b_config *cfg, const DevCsrBuild &dc,
+                                       uint32_t *slot_out) {
+    NetHost *h = nullptr;
+    NE2B_TRY(build_net(net, cfg, nullptr, 0, stager_, &h, &dc));
+    const ne2b_status st = attach_net(h, slot_out, true);
+    if (st != NE2B_OK) discard_net(h, stream_);
+    return st;
+}
+
 ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
-                              Stager &sg, NetHost **out) {
+                              Stager &sg, NetHost **out, const DevCsrBuild *dc) {
     *out = nullptr;
     if (!net || !cfg) return set_error(NE2B_EINVAL, "add_net: null net or config");
     const cudaStream_t bst = sg.stream();
@@ -354,19 +363,23 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     const uint32_t n = net->n;
     if (!(cfg->dt_ms >= 0.001f && cfg->dt_ms <= 100.0f))  // lib.rs:35-39 valid_dt_ms
         return set_error(NE2B_EINVAL, "dt_ms %g outside [0.001, 100]", (double)cfg->dt_ms);
-    if (n > 0 && (!net->model || !net->params || !net->src_ptr))
+    if (n > 0 && (!net->model || !net->params || (!net->src_ptr && !dc)))
         return set_error(NE2B_EINVAL, "net: model, params and src_ptr are required");
     if (net->param_stride < 4 && n > 0) return set_error(NE2B_EINVAL, "param_stride %u < 4", net->param_stride);
-    if (n > 0 && net->src_ptr[n] != net->n_syn)
-        return set_error(NE2B_EINVAL, "src_ptr[n] = %u but n_syn = %llu", net->src_ptr[n],
-                         (unsigned long long)net->n_syn);
-    if (net->n_syn > 0xffffffffull) return set_error(NE2B_UNSUPPORTED, "more than 2^32-1 synapses in one net");
-    for (uint32_t i = 0; i < n; ++i)
-        if (net->src_ptr[i] > net->src_ptr[i + 1]) return set_error(NE2B_EINVAL, "src_ptr not monotone at %u", i);
+    const uint64_t n_syn = dc ? dc->syn.n_syn : net->n_syn;
+    if (n_syn > 0xffffffffull) return set_error(NE2B_UNSUPPORTED, "more than 2^32-1 synapses in one net");
+    if (!dc) {
+        if (n > 0 && net->src_ptr[n] != net->n_syn)
+            return set_error(NE2B_EINVAL, "src_ptr[n] = %u but n_syn = %llu", net->src_ptr[n],
+                             (unsigned long long)net->n_syn);
+        for (uint32_t i = 0; i < n; ++i)
+            if (net->src_ptr[i] > net->src_ptr[i + 1]) return set_error(NE2B_EINVAL, "src_ptr not monotone at %u", i);
+    }
     // one parallel pass over the synapses: target range, delay range, tau
-    uint32_t maxd = 1, mind = 0xffff, maxt = 0;
+    // (a device list was checked by its prepass)
+    uint32_t maxd = dc ? dc->max_delay : 1, mind = dc ? 1 : 0xffff, maxt = 0;
     bool any_tau = false;
-    {
+    if (!dc) {
         std::mutex mu;
         parallel_for(net->n_syn, [&](uint64_t lo, uint64_t hi) {
             uint32_t mx = 1, mn = 0xffff, mt = 0;
@@ -386,12 +399,12 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
             any_tau |= tau;
         });
     }
-    if (net->n_syn && maxt >= n) {
+    if (!dc && net->n_syn && maxt >= n) {
         for (uint64_t j = 0; j < net->n_syn; ++j)
             if (net->tgt[j] >= n)
                 return set_error(NE2B_EINVAL, "synapse %llu targets %u >= n %u", (unsigned long long)j, net->tgt[j], n);
     }
-    if (net->n_syn && mind < 1) return set_error(NE2B_EINVAL, "a synapse has delay 0 steps");
+    if (!dc && net->n_syn && mind < 1) return set_error(NE2B_EINVAL, "a synapse has delay 0 steps");
     for (uint32_t i = 0; i < n; ++i)
         if (net->model[i] > 1) return set_error(NE2B_EINVAL, "neuron %u: unknown model id %u", i, net->model[i]);
     if (n > 0 && net->n_inputs > 0 && net->stim_ptr) {
@@ -411,7 +424,7 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     h->n = n;
     h->n_pad = (n + kNeuronAlign - 1) / kNeuronAlign * kNeuronAlign;
     h->D = maxd + 1 < 2 ? 2 : maxd + 1;  // state.rs:221-224
-    h->e = net->n_syn;
+    h->e = n_syn;
     h->n_inputs = net->n_inputs;
     h->t_end = inputs ? steps : ~0ull;
     h->fixed_stim = inputs != nullptr;
@@ -493,8 +506,18 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     NET_TRY(up((void *)d.v0, v0.data(), sizeof(float) * np));
     NET_TRY(up((void *)d.u0, u0.data(), sizeof(float) * np));
     NET_TRY(cuda_error(cudaMemsetAsync(d.ext, 0, sizeof(float) * np, bst), "memset ext"));
-    NET_TRY(up((void *)d.rowptr, net->src_ptr, sizeof(uint32_t) * ((size_t)n + 1)));
-    if (h->e) {
+    if (dc) {
+        // the list's CSR sorted into place on the device (csrc/ne2b_csr.cu)
+        NET_TRY(cuda_error(csr_scan(dc->counts, n, (uint32_t)h->e, (uint32_t *)d.rowptr, dc->cursor, dc->sums, bst),
+                           "device CSR: row pointers"));
+        NET_TRY(cuda_error(csr_scatter(dc->syn, dc->steps, dc->cursor, (uint32_t *)d.tgt, (void *)d.w, (void *)d.delay, int_ring_, d16,
+                                       dc->ticket, dc->done, dc->sc, 5000000000ull, bst),
+                           "device CSR: scatter"));
+        h->build_launches += (n ? 3 : 0) + (h->e ? 1 : 0);
+    } else {
+        NET_TRY(up((void *)d.rowptr, net->src_ptr, sizeof(uint32_t) * ((size_t)n + 1)));
+    }
+    if (h->e && !dc) {
         // one parallel pass over the synapses into pinned staging: targets
         // copied, weights quantised (kernels.rs:61 rt_put: lrintf(w * 4096))
         // for the fixed-point ring, delays narrowed to u8 when D <= 256
@@ -1040,6 +1063,27 @@ ne2b_status Engine::run_steps(uint64_t steps) {
             }
         steps -= chunk;
     }
+    return NE2B_OK;
+}
+
+ne2b_status Engine::read_csr(NetHost &h, uint32_t *rowptr, uint32_t *tgt, uint32_t *w_bits, uint16_t *delay_steps) {
+    const NetDev &d = h.dev;
+    if (rowptr) NE2B_CUDA(cudaMemcpyAsync(rowptr, d.rowptr, sizeof(uint32_t) * ((size_t)h.n + 1), cudaMemcpyDeviceToHost, stream_));
+    if (h.e) {
+        if (tgt) NE2B_CUDA(cudaMemcpyAsync(tgt, d.tgt, sizeof(uint32_t) * h.e, cudaMemcpyDeviceToHost, stream_));
+        if (w_bits) NE2B_CUDA(cudaMemcpyAsync(w_bits, d.w, sizeof(uint32_t) * h.e, cudaMemcpyDeviceToHost, stream_));
+        if (delay_steps) {
+            if (d.flags & kNetDelay16) {
+                NE2B_CUDA(cudaMemcpyAsync(delay_steps, d.delay, sizeof(uint16_t) * h.e, cudaMemcpyDeviceToHost, stream_));
+            } else {
+                std::vector<uint8_t> d8(h.e);
+                NE2B_CUDA(cudaMemcpyAsync(d8.data(), d.delay, h.e, cudaMemcpyDeviceToHost, stream_));
+                NE2B_CUDA(cudaStreamSynchronize(stream_));
+                for (uint64_t j = 0; j < h.e; ++j) delay_steps[j] = d8[j];
+            }
+        }
+    }
+    NE2B_CUDA(cudaStreamSynchronize(stream_));
     return NE2B_OK;
 }
 

@@ -16,9 +16,24 @@
 #include <vector>
 
 #include "../../include/ne2b.h"
+#include "ne2b_csr.h"
 #include "ne2b_layout.h"
 
 namespace ne2b {
+
+// A synapse list on the device, checked by csr_prepass, with the scratch
+// its CSR build uses (all device memory, owned by the caller).
+struct DevCsrBuild {
+    DevSynapses syn;
+    const uint16_t *steps = nullptr;   // delay steps per list entry
+    const uint32_t *counts = nullptr;  // synapses per source
+    uint32_t max_delay = 1;
+    uint32_t *cursor = nullptr;        // [n]
+    uint32_t *sums = nullptr;          // [csr_scan_blocks(n)]
+    uint32_t *ticket = nullptr;        // [1], zeroed
+    uint32_t *done = nullptr;          // [csr_chunks(n_syn)], zeroed
+    CsrScalars *sc = nullptr;
+};
 
 ne2b_status set_error(ne2b_status st, const char *fmt, ...);
 ne2b_status cuda_error(cudaError_t e, const char *what);
@@ -135,8 +150,15 @@ class Engine {
     // while this engine steps.  attach_net publishes a built net (slot,
     // descriptor, counters, parameter rows) on the engine's stream, which
     // must already be ordered after the build's stream work.
+    // `dc`: the synapses are a list already on the device (checked by
+    // csr_prepass), whose CSR the build sorts into place on the device; the
+    // CSR fields of `net` are then unused.
     ne2b_status build_net(const ne2b_net_desc *net, const ne2b_config *cfg, const float *inputs, uint64_t steps,
-                          Stager &sg, NetHost **out);
+                          Stager &sg, NetHost **out, const DevCsrBuild *dc = nullptr);
+    ne2b_status add_net_device_csr(const ne2b_net_desc *net, const ne2b_config *cfg, const DevCsrBuild &dc,
+                                   uint32_t *slot);
+    // The device CSR of a net copied out (weights as stored, delays widened).
+    ne2b_status read_csr(NetHost &h, uint32_t *rowptr, uint32_t *tgt, uint32_t *w_bits, uint16_t *delay_steps);
     ne2b_status attach_net(NetHost *h, uint32_t *slot, bool rebuild = true);
     void discard_net(NetHost *h, cudaStream_t st);  // a built net that is never attached
     ne2b_status remove_net(uint32_t slot, bool rebuild = true, const void *keep = nullptr);

@@ -42,6 +42,55 @@ class B200Sim:
         self._n = int(n.value)
         self.n_inputs = int(net.n_inputs)
 
+    @classmethod
+    def from_synapses(cls, model, params, kind, src, tgt, w, delay_ms, cfg: _abi.Config | None = None,
+                      device: int = 0, x0=None, **cfg_kw) -> "B200Sim":
+        """A sim whose synapse CSR is built on the GPU from a plain synapse
+        list (`Network::synapse_csr`, net-format/src/network.rs:654-692):
+        equal to `B200Sim(from_synapses(...))` bit for bit."""
+        self = cls.__new__(cls)
+        self.cfg = _cfg(cfg, **cfg_kw)
+        model = np.ascontiguousarray(model, dtype=np.uint8)
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        kind = np.ascontiguousarray(kind, dtype=np.uint8)
+        src = np.ascontiguousarray(src, dtype=np.uint32)
+        tgt = np.ascontiguousarray(tgt, dtype=np.uint32)
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        delay_ms = np.ascontiguousarray(delay_ms, dtype=np.float32)
+        x0 = None if x0 is None else np.ascontiguousarray(x0, dtype=np.float32)
+        n = len(model)
+        d = _abi.NetDesc()
+        d.n = n
+        d.model, d.params = model.ctypes.data, params.ctypes.data
+        d.param_stride = params.shape[1] if params.ndim == 2 else (params.size // max(n, 1))
+        d.x0 = None if x0 is None else x0.ctypes.data
+        h = C.c_void_p()
+        check(lib.ne2b_create_from_synapses(C.byref(d), kind.ctypes.data, len(src), src.ctypes.data, tgt.ctypes.data,
+                                            w.ctypes.data, delay_ms.ctypes.data, C.byref(self.cfg), device,
+                                            C.byref(h)))
+        self._h = h
+        self._net = None
+        self._n = n
+        self.n_inputs = 0
+        return self
+
+    def syn_count(self) -> int:
+        e = C.c_uint64()
+        check(lib.ne2b_syn_count(self._h, C.byref(e)))
+        return int(e.value)
+
+    def read_csr(self):
+        """The device CSR: (rowptr u32[n+1], tgt u32[E], weight bits u32[E]
+        (int32 fixed point with the int ring, else f32 bits), delay steps
+        u16[E])."""
+        e = self.syn_count()
+        rowptr = np.empty(self._n + 1, np.uint32)
+        tgt = np.empty(e, np.uint32)
+        wb = np.empty(e, np.uint32)
+        dl = np.empty(e, np.uint16)
+        check(lib.ne2b_read_csr(self._h, rowptr.ctypes.data, tgt.ctypes.data, wb.ctypes.data, dl.ctypes.data))
+        return rowptr, tgt, wb, dl
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib.ne2b_destroy(self._h)

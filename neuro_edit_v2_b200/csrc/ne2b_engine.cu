@@ -245,6 +245,31 @@ Stager::~Stager() {
         cudaFreeHost(b.p);
         cudaEventDestroy(b.ev);
     }
+    for (PinnedBlock &b : ring_) {
+        if (b.ev) cudaEventSynchronize(b.ev);
+        if (b.p) cudaFreeHost(b.p);
+        if (b.ev) cudaEventDestroy(b.ev);
+    }
+}
+
+ne2b_status Stager::copy_streamed(void *dst, const void *src, size_t bytes) {
+    for (size_t off = 0; off < bytes; off += kRingBytes) {
+        const size_t len = std::min(kRingBytes, bytes - off);
+        PinnedBlock &b = ring_[ring_next_];
+        ring_next_ = (ring_next_ + 1) % kRing;
+        if (!b.p) {
+            NE2B_CUDA(cudaMallocHost(&b.p, kRingBytes));
+            NE2B_CUDA(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming));
+            b.cap = kRingBytes;
+        } else {
+            NE2B_CUDA(cudaEventSynchronize(b.ev));  // its previous transfer has left the block
+        }
+        const uint8_t *s = (const uint8_t *)src + off;
+        parallel_for(len, [&](uint64_t lo, uint64_t hi) { memcpy((uint8_t *)b.p + lo, s + lo, hi - lo); });
+        NE2B_CUDA(cudaMemcpyAsync((uint8_t *)dst + off, b.p, len, cudaMemcpyHostToDevice, st_));
+        NE2B_CUDA(cudaEventRecord(b.ev, st_));
+    }
+    return NE2B_OK;
 }
 
 ne2b_status Stager::reserve(size_t bytes, void **host) {
@@ -288,6 +313,7 @@ ne2b_status Stager::copy(void *dst, const void *src, size_t bytes) {
         NE2B_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st_));
         return NE2B_OK;
     }
+    if (bytes > 2 * kRingBytes) return copy_streamed(dst, src, bytes);
     void *stage = nullptr;
     NE2B_TRY(reserve(bytes, &stage));
     parallel_for(bytes, [&](uint64_t lo, uint64_t hi) { memcpy((uint8_t *)stage + lo, (const uint8_t *)src + lo, hi - lo); });

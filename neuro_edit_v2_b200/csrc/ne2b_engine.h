@@ -121,6 +121,15 @@ class Stager {
     ne2b_status close();
 
   private:
+    // copies larger than two ring blocks stream through a fixed ring of
+    // pinned blocks, each refilled once its previous DMA has completed, so
+    // a multi-GB upload pins no more than the ring and overlaps the host
+    // copy with the transfer
+    static constexpr size_t kRingBytes = (size_t)32 << 20;
+    static constexpr int kRing = 4;
+    ne2b_status copy_streamed(void *dst, const void *src, size_t bytes);
+    PinnedBlock ring_[kRing];
+    int ring_next_ = 0;
     cudaStream_t st_ = nullptr;
     std::vector<PinnedBlock> pin_;
     int cur_ = -1;

@@ -252,22 +252,36 @@ Stager::~Stager() {
     }
 }
 
+ne2b_status Stager::ring_next(void **host) {
+    ring_cur_ = ring_next_;
+    ring_next_ = (ring_next_ + 1) % kRing;
+    PinnedBlock &b = ring_[ring_cur_];
+    if (!b.p) {
+        NE2B_CUDA(cudaMallocHost(&b.p, kRingBytes));
+        NE2B_CUDA(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming));
+        b.cap = kRingBytes;
+    } else {
+        NE2B_CUDA(cudaEventSynchronize(b.ev));  // its previous transfer has left the block
+    }
+    *host = b.p;
+    return NE2B_OK;
+}
+
+ne2b_status Stager::ring_issue(void *dst, size_t bytes) {
+    PinnedBlock &b = ring_[ring_cur_];
+    NE2B_CUDA(cudaMemcpyAsync(dst, b.p, bytes, cudaMemcpyHostToDevice, st_));
+    NE2B_CUDA(cudaEventRecord(b.ev, st_));
+    return NE2B_OK;
+}
+
 ne2b_status Stager::copy_streamed(void *dst, const void *src, size_t bytes) {
     for (size_t off = 0; off < bytes; off += kRingBytes) {
         const size_t len = std::min(kRingBytes, bytes - off);
-        PinnedBlock &b = ring_[ring_next_];
-        ring_next_ = (ring_next_ + 1) % kRing;
-        if (!b.p) {
-            NE2B_CUDA(cudaMallocHost(&b.p, kRingBytes));
-            NE2B_CUDA(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming));
-            b.cap = kRingBytes;
-        } else {
-            NE2B_CUDA(cudaEventSynchronize(b.ev));  // its previous transfer has left the block
-        }
+        void *hb = nullptr;
+        NE2B_TRY(ring_next(&hb));
         const uint8_t *s = (const uint8_t *)src + off;
-        parallel_for(len, [&](uint64_t lo, uint64_t hi) { memcpy((uint8_t *)b.p + lo, s + lo, hi - lo); });
-        NE2B_CUDA(cudaMemcpyAsync((uint8_t *)dst + off, b.p, len, cudaMemcpyHostToDevice, st_));
-        NE2B_CUDA(cudaEventRecord(b.ev, st_));
+        parallel_for(len, [&](uint64_t lo, uint64_t hi) { memcpy((uint8_t *)hb + lo, s + lo, hi - lo); });
+        NE2B_TRY(ring_issue((uint8_t *)dst + off, len));
     }
     return NE2B_OK;
 }
@@ -546,32 +560,55 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     if (h->e && !dc) {
         // one parallel pass over the synapses into pinned staging: targets
         // copied, weights quantised (kernels.rs:61 rt_put: lrintf(w * 4096))
-        // for the fixed-point ring, delays narrowed to u8 when D <= 256
-        uint32_t *tg = nullptr;
-        void *wst = nullptr;
-        void *dst8 = nullptr;
-        NET_TRY(sg.reserve(4 * h->e, (void **)&tg));
-        NET_TRY(sg.reserve(4 * h->e, &wst));
-        NET_TRY(sg.reserve((d16 ? 2 : 1) * h->e, &dst8));
+        // for the fixed-point ring, delays narrowed to u8 when D <= 256;
+        // synapses [j0, j0 + m) into host buffers at their offset 0
         const bool iq = int_ring_;
-        parallel_for(h->e, [&](uint64_t lo, uint64_t hi) {
-            memcpy(tg + lo, net->tgt + lo, 4 * (hi - lo));
-            if (iq) {
-                int32_t *wq = (int32_t *)wst;
-                for (uint64_t j = lo; j < hi; ++j) wq[j] = (int32_t)lrintf(net->w[j] * 4096.0f);
-            } else {
-                memcpy((float *)wst + lo, net->w + lo, 4 * (hi - lo));
+        const size_t db = d16 ? 2 : 1;
+        auto fill = [&](uint32_t *tg, void *wst, void *dst8, uint64_t j0, uint64_t m) {
+            parallel_for(m, [&](uint64_t lo, uint64_t hi) {
+                if (tg) memcpy(tg + lo, net->tgt + j0 + lo, 4 * (hi - lo));
+                if (wst && iq) {
+                    int32_t *wq = (int32_t *)wst;
+                    for (uint64_t j = lo; j < hi; ++j) wq[j] = (int32_t)lrintf(net->w[j0 + j] * 4096.0f);
+                } else if (wst) {
+                    memcpy((float *)wst + lo, net->w + j0 + lo, 4 * (hi - lo));
+                }
+                if (dst8 && d16) {
+                    memcpy((uint16_t *)dst8 + lo, net->delay_steps + j0 + lo, 2 * (hi - lo));
+                } else if (dst8) {
+                    uint8_t *d8 = (uint8_t *)dst8;
+                    for (uint64_t j = lo; j < hi; ++j) d8[j] = (uint8_t)net->delay_steps[j0 + j];
+                }
+            });
+        };
+        if (4 * h->e > 2 * Stager::kRingBytes) {
+            // a large net streams through the stager's ring of pinned blocks
+            const uint64_t per = Stager::kRingBytes / 4;
+            for (uint64_t j0 = 0; j0 < h->e; j0 += per) {
+                const uint64_t m = std::min<uint64_t>(per, h->e - j0);
+                void *hb = nullptr;
+                NET_TRY(sg.ring_next(&hb));
+                fill((uint32_t *)hb, nullptr, nullptr, j0, m);
+                NET_TRY(sg.ring_issue((uint32_t *)d.tgt + j0, 4 * m));
+                NET_TRY(sg.ring_next(&hb));
+                fill(nullptr, hb, nullptr, j0, m);
+                NET_TRY(sg.ring_issue((uint32_t *)d.w + j0, 4 * m));
+                NET_TRY(sg.ring_next(&hb));
+                fill(nullptr, nullptr, hb, j0, m);
+                NET_TRY(sg.ring_issue((uint8_t *)d.delay + db * j0, db * m));
             }
-            if (d16) {
-                memcpy((uint16_t *)dst8 + lo, net->delay_steps + lo, 2 * (hi - lo));
-            } else {
-                uint8_t *d8 = (uint8_t *)dst8;
-                for (uint64_t j = lo; j < hi; ++j) d8[j] = (uint8_t)net->delay_steps[j];
-            }
-        });
-        NET_TRY(sg.issue((void *)d.tgt, tg, 4 * h->e));
-        NET_TRY(sg.issue((void *)d.w, wst, 4 * h->e));
-        NET_TRY(sg.issue((void *)d.delay, dst8, (d16 ? 2 : 1) * h->e));
+        } else {
+            uint32_t *tg = nullptr;
+            void *wst = nullptr;
+            void *dst8 = nullptr;
+            NET_TRY(sg.reserve(4 * h->e, (void **)&tg));
+            NET_TRY(sg.reserve(4 * h->e, &wst));
+            NET_TRY(sg.reserve(db * h->e, &dst8));
+            fill(tg, wst, dst8, 0, h->e);
+            NET_TRY(sg.issue((void *)d.tgt, tg, 4 * h->e));
+            NET_TRY(sg.issue((void *)d.w, wst, 4 * h->e));
+            NET_TRY(sg.issue((void *)d.delay, dst8, db * h->e));
+        }
     }
     if (any_tau) {
         // XSyn::build (sim/src/state.rs:245-274): synapses with tau > 0 get

@@ -120,14 +120,19 @@ class Stager {
     ne2b_status copy(void *dst, const void *src, size_t bytes);  // small copies go from pageable memory
     ne2b_status close();
 
-  private:
-    // copies larger than two ring blocks stream through a fixed ring of
+    // Copies larger than two ring blocks stream through a fixed ring of
     // pinned blocks, each refilled once its previous DMA has completed, so
     // a multi-GB upload pins no more than the ring and overlaps the host
-    // copy with the transfer
+    // copy with the transfer.  ring_next hands out the next block (kRingBytes)
+    // once it is free; ring_issue sends its first `bytes` to `dst`.
     static constexpr size_t kRingBytes = (size_t)32 << 20;
+    ne2b_status ring_next(void **host);
+    ne2b_status ring_issue(void *dst, size_t bytes);
+
+  private:
     static constexpr int kRing = 4;
     ne2b_status copy_streamed(void *dst, const void *src, size_t bytes);
+    int ring_cur_ = -1;
     PinnedBlock ring_[kRing];
     int ring_next_ = 0;
     cudaStream_t st_ = nullptr;

@@ -459,9 +459,14 @@ class Server:
         """Finished requests whose results are ready to take."""
         cnt = C.c_uint32()
         check(lib.ne2b_server_finished_ids(self._h, None, 0, C.byref(cnt)))
-        ids = np.zeros(max(cnt.value, 1), dtype=np.uint64)
-        check(lib.ne2b_server_finished_ids(self._h, ptr(ids), cnt.value, C.byref(cnt)))
-        return [int(x) for x in ids[: cnt.value]]
+        cap = cnt.value
+        if cap == 0:
+            return []
+        ids = np.zeros(cap, dtype=np.uint64)
+        # more requests may become ready between the two calls: only the
+        # first min(cap, count) entries are filled
+        check(lib.ne2b_server_finished_ids(self._h, ptr(ids), cap, C.byref(cnt)))
+        return [int(x) for x in ids[: min(cap, cnt.value)]]
 
     def take(self, rid: int) -> tuple[np.ndarray, int]:
         n, w = C.c_uint32(), C.c_uint32()

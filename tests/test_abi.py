@@ -141,6 +141,30 @@ def test_host_expf_equals_oracle_on_a_stride_of_all_floats():
     assert bad == 0
 
 
+@pytest.mark.parametrize("first, second, want", [(0, 2, []), (1, 3, [7]), (2, 2, [7, 8])])
+def test_server_finished_lists_only_the_ids_it_received(monkeypatch, first, second, want):
+    """ne2b_server_finished_ids is called for the count, then for the ids; a
+    request that becomes ready between the two calls raises the second count
+    above the buffer, and only the filled entries are ids."""
+    from neuro_edit_v2_b200 import sim as S
+
+    calls = []
+
+    def fake(h, ids, cap, cnt):
+        calls.append(cap)
+        if ids:
+            arr = (ctypes.c_uint64 * cap).from_address(ids)
+            for i in range(min(cap, second)):
+                arr[i] = 7 + i
+        cnt._obj.value = first if len(calls) == 1 else second
+        return 0
+
+    monkeypatch.setattr(S.lib, "ne2b_server_finished_ids", fake)
+    srv = S.Server.__new__(S.Server)
+    srv._h = None
+    assert srv.finished() == want
+
+
 def test_request_footprint_needs_no_gpu():
     net = nb.liquid(10, 1)
     cfg = nb.default_config(int_weights=1, window_steps=500)

@@ -265,6 +265,8 @@ def run_profile(args):
 
     if args.served_mix:
         return run_profile_served(args, nb, torch)
+    if args.batched_liquids:
+        return run_profile_batched(args, nb, torch)
     net = nb.random_kout(args.profile_neurons, K_OUT, SEED)
     sim = nb.B200Sim(net, make_cfg(nb, args.active))
     if args.kernel:
@@ -277,6 +279,48 @@ def run_profile(args):
     ms, spikes, launches = timed_trials(sim, 1, 3, args.trial_steps, 1, torch, scrub)
     print(json.dumps({"profile_run": True, "neurons": args.profile_neurons, "trial_steps": args.trial_steps,
                       "ms": ms, "spikes": spikes, "launches": launches, "tiling": tiling}), flush=True)
+
+
+def run_profile_batched(args, nb, torch):
+    """The first --batched-liquids liquids of the batched workload (with
+    their input streams, or none with --no-inputs) stepped as one batch:
+    3 warm-up trials + 1 trial of --trial-steps steps, for ncu."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from neuro_edit_v2_b200 import workloads as W
+
+    count = args.batched_liquids
+    sides = W.batched_liquid_sizes(256, 4)[:count]
+    n_inputs = 0 if args.no_inputs else 8
+    with ThreadPoolExecutor(8) as ex:
+        nets = list(ex.map(lambda k: nb.liquid(sides[k], seed=1000 + k, n_inputs=n_inputs), range(count)))
+    cfgs = [nb.default_config(int_weights=1, window_steps=W.WINDOW_STEPS, max_windows=20, seed=k) for k in range(count)]
+    b = nb.Batch(nets, cfgs)
+    if n_inputs:
+        rng = np.random.default_rng(5)
+        for k in range(count):
+            b.set_input_matrix(k, W.bit_streams(rng, 1000))
+    if args.kernel:
+        b.set_kernel_mode({"stream": nb.KERNEL_STREAM, "resident": nb.KERNEL_RESIDENT}[args.kernel])
+    if args.shape:
+        bl, npt = (int(x) for x in args.shape.split("x"))
+        b.set_tile_shape(bl, npt)
+    stream = torch.cuda.ExternalStream(b.stream_handle())
+    for _ in range(3):
+        b.reset_state()
+        b.run_steps(args.trial_steps)
+    b.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    b.reset_state()
+    e0.record(stream)
+    b.run_steps(args.trial_steps)
+    e1.record(stream)
+    e1.synchronize()
+    print(json.dumps({"profile_run": True, "batched_liquids": count, "inputs": n_inputs, "neurons": sum(n.n for n in nets),
+                      "trial_steps": args.trial_steps, "ms": e0.elapsed_time(e1),
+                      "spikes": sum(b.spikes_total(k) for k in range(count)), "tile_shape": b.tile_shape()}),
+          flush=True)
 
 
 def run_profile_served(args, nb, torch):
@@ -715,6 +759,10 @@ def main():
                          "autotuning it, e.g. for an ncu launch list)")
     ap.add_argument("--served-mix", type=int, default=0,
                     help="--profile the first N requests of the serving stream stepped as one batch")
+    ap.add_argument("--batched-liquids", type=int, default=0,
+                    help="--profile the first N liquids of the batched workload stepped as one batch")
+    ap.add_argument("--no-inputs", action="store_true",
+                    help="with --batched-liquids: build the liquids without input streams")
     ap.add_argument("--floors", action="store_true",
                     help="print the measured launch / streaming / atomic floors (neuro_edit_v2_b200/_lib/probe_floors)")
     args = ap.parse_args()

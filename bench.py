@@ -567,7 +567,16 @@ def bench_batched(nb, torch, scrub, steps: int, warmup: int, serial_sample: int 
         one.close()
     batched_tps = len(nets) * steps / (total_ms / 1000.0)
     serial_tps = serial_sample / (ser_ms / 1000.0)
+    # the same byte contract as the single net (all liquids are izh): the
+    # per-step bytes over the per-step time of the timed trials
+    peak, peak_kind = load_peaks()
+    step_s = total_ms / 1000.0 / (steps * trial)
+    alg = B_NEURON * neurons + (B_SPIKE * spikes + B_EVENT * events) / trial
+    achieved = alg / step_s / 1e9
     return {"nets": len(nets), "neurons": neurons, "synapses": sum(n.n_syn for n in nets), "trial_steps": trial,
+            "roofline": {"achieved_gbs": achieved, "frac": achieved / peak, "peak": peak,
+                         "peak_kind": f"{peak_kind} hbm_gbs", "alg_bytes_per_step": alg, "step_us": step_s * 1e6,
+                         "bytes_per_neuron": B_NEURON},
             "windows_per_trial": wins, "tile_shape": {"block": shape[0], "neurons_per_thread": shape[1],
                                                       "blocks_per_sm": shape[2]},
             "trials_per_s": batched_tps, "ms_per_batch_trial": total_ms / steps,

@@ -10,7 +10,8 @@
 
 // Tile shapes compiled in: (threads per block, neurons per thread).
 #define NE2B_SHAPES(X) \
-    X(128, 1) X(128, 2) X(128, 4) X(128, 8) X(256, 1) X(256, 2) X(256, 4) X(256, 8) X(512, 1) X(512, 2) X(512, 4)
+    X(64, 1) X(64, 2) X(64, 4) X(128, 1) X(128, 2) X(128, 4) X(128, 8) X(256, 1) X(256, 2) X(256, 4) X(256, 8) \
+    X(512, 1) X(512, 2) X(512, 4)
 
 namespace ne2b {
 

@@ -115,7 +115,7 @@ def test_batch_autotune_keeps_results():
             for i in range(8):
                 bb.play_input(k, i, x[:, i])
     shape = a.autotune(64)
-    assert shape[0] in (128, 256, 512)
+    assert shape[0] in (64, 128, 256, 512)
     a.run_steps(600)
     b.run_steps(600)
     for k in range(4):

@@ -55,6 +55,15 @@ def test_device_csr_equals_host_csr(int_weights, n, e, srcs):
     assert dev.ring_depth() == host.ring_depth()
 
 
+def test_large_lists_stream_through_the_pinned_ring():
+    """20M synapses: the device build uploads a 320 MB list and the host
+    build a 180 MB CSR, both larger than two 32 MB staging blocks, so both
+    stream through the stager's ring of pinned blocks."""
+    host, dev = both(200_000, 20_000_000, 13)
+    assert dev.syn_count() == host.syn_count() == 20_000_000
+    same_csr(host, dev)
+
+
 def test_long_delays_use_the_u16_ring_on_both_paths():
     host, dev = both(3000, 60_000, 5, max_delay_ms=60.0)
     assert dev.ring_depth() > 257

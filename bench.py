@@ -267,7 +267,9 @@ def run_profile(args):
         return run_profile_served(args, nb, torch)
     if args.batched_liquids:
         return run_profile_batched(args, nb, torch)
-    net = nb.random_kout(args.profile_neurons, K_OUT, SEED)
+    net = nb.random_kout(args.profile_neurons, K_OUT, SEED, w_scale=0.7 * (281.0 if args.adex else 1.0))
+    if args.adex:  # the AdEx variant of the 1M workload (weights x C = 281 pF)
+        nb.to_adex(net)
     sim = nb.B200Sim(net, make_cfg(nb, args.active))
     if args.kernel:
         sim.set_kernel_mode({"stream": nb.KERNEL_STREAM, "resident": nb.KERNEL_RESIDENT}[args.kernel])
@@ -761,6 +763,7 @@ def main():
     ap.add_argument("--trial-steps", type=int, default=200, help="trial length in --profile mode")
     ap.add_argument("--active", action="store_true", help="--profile the active (Poisson-kick) regime")
     ap.add_argument("--profile-neurons", type=int, default=N, help="network size in --profile mode")
+    ap.add_argument("--adex", action="store_true", help="--profile the AdEx variant of the random net")
     ap.add_argument("--kernel", choices=["stream", "resident"], default=None, help="force the step kernel")
     ap.add_argument("--autotune", action="store_true", help="--profile with the autotuned kernel and tiling")
     ap.add_argument("--shape", default=None,

@@ -177,6 +177,9 @@ ne2b_status ne2b_kernel_mode(ne2b_sim *sim, int32_t *mode, int32_t *resident);
  * steps_per_trial steps from a device snapshot of its state and keep the
  * fastest (the state is restored afterwards; AUTO mode may switch kernel). */
 ne2b_status ne2b_autotune(ne2b_sim *sim, uint32_t steps_per_trial);
+/* The step kernels' tile shape: threads per block x neurons per thread,
+ * one of 64 x {1, 2, 4}, {128, 256} x {1, 2, 4, 8} and 512 x {1, 2, 4};
+ * blocks_per_sm 0 = as many as fit. */
 ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *neurons_per_thread,
                             uint32_t *blocks_per_sm);
 ne2b_status ne2b_set_tile_shape(ne2b_sim *sim, uint32_t block, uint32_t neurons_per_thread,

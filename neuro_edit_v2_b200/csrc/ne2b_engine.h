@@ -220,7 +220,7 @@ class Engine {
     ne2b_status set_mode(int m);
     bool fixed_grid = false;  // grid independent of the tile count (serving)
     bool multi_net = false;   // many nets (batch, server): the streaming kernel stages tiles ahead
-    uint32_t graph_steps = 64;
+    uint32_t graph_steps = 256;
     uint32_t resident_steps = 4096;  // max steps per resident launch
     uint64_t stim_chunk = 2048;
 

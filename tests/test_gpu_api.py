@@ -166,7 +166,7 @@ def test_window_counts_equal_sliding_spike_counts():
 
 @pytest.mark.parametrize("ws, rec", [(1, 2), (7, 5), (100, 64), (250, 300)])
 def test_windows_and_record_rows_wrapping_inside_a_launch_group(ws, rec):
-    """Windows and record rings shorter than a launch group (64 steps) wrap
+    """Windows and record rings shorter than a launch group (256 steps) wrap
     several times inside one group: each window's count equals the oracle's
     spikes over that window's steps, and the last `rec` record rows equal
     the oracle's."""

@@ -80,7 +80,9 @@ class Clocks:
         self.proc = None
         self.rows = []
         self.thread = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+
+        self.path = os.path.join(tempfile.gettempdir(), f"ne2b_clocks_{os.getpid()}.csv")
 
     def _nvml_handle(self):
         import pynvml

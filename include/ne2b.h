@@ -241,6 +241,14 @@ ne2b_status ne2b_batch_set_kernel_mode(ne2b_batch *b, int32_t mode);
 ne2b_status ne2b_batch_kernel_mode(ne2b_batch *b, int32_t *mode, int32_t *resident);
 ne2b_status ne2b_batch_stream(ne2b_batch *b, void **stream);
 ne2b_status ne2b_batch_kernel_launches(ne2b_batch *b, uint64_t *launches);
+/* ne2b_fit_ridge_multi on features that stay on the device: trial r is net
+ * nets[r] of the batch, its features the spike counts of its first
+ * `windows` windows, window-major ([windows][n], F = windows x n; all the
+ * nets the same size, each with those windows done).  Ordered after the
+ * batch's queued steps; *n_features receives F. */
+ne2b_status ne2b_batch_fit_ridge_multi(ne2b_batch *b, const uint32_t *nets, uint32_t t, uint32_t windows,
+                                       const uint32_t *labels, uint32_t k, double lambda, uint32_t *n_features,
+                                       double *w);
 
 /* -------------------------------------------------------------- serving */
 /* Continuous batching of trial requests: requests are admitted into free
@@ -295,6 +303,18 @@ ne2b_status ne2b_server_synchronize(ne2b_server *s);
 ne2b_status ne2b_server_set_tile_shape(ne2b_server *s, uint32_t block, uint32_t npt, uint32_t blocks_per_sm);
 ne2b_status ne2b_server_stream(ne2b_server *s, void **stream);
 ne2b_status ne2b_server_kernel_launches(ne2b_server *s, uint64_t *launches);
+
+/* ------------------------------------------------------ readout training */
+/* fit_ridge_multi (sim/src/readout.rs:190-252): multi-class ridge solved in
+ * the dual on the column-centred design x[T x F] (row-major f32, in host or
+ * device memory), labels[T] in 0..k-1; w[k x (F + 1)] receives one weight
+ * row per class, bias last.  The Gram matrix, its Cholesky factor and the
+ * weights are computed on `device` with the reference's f64 operations in
+ * the reference's order, so w equals the reference's bit for bit; a Gram
+ * matrix that is not positive definite gives zero dual weights, as there.
+ * T at most 32768 (the T x T Gram matrix is f64). */
+ne2b_status ne2b_fit_ridge_multi(const float *x, uint32_t t, uint32_t f, const uint32_t *labels, uint32_t k,
+                                 double lambda, int device, double *w);
 
 /* ----------------------------------------------------------- net building */
 /* A host-side network owned by the library, in the ne2b_net_desc layout. */

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libne2b.so")
 SOURCES = ["ne2b_step_k00.cu", "ne2b_step_k01.cu", "ne2b_step_k10.cu", "ne2b_step_k11.cu", "ne2b_kernels.cu",
-           "ne2b_engine.cu", "ne2b_capi.cu", "ne2b_noalloc.cu", "ne2b_csr.cu", "ne2b_host.cpp",
+           "ne2b_engine.cu", "ne2b_capi.cu", "ne2b_noalloc.cu", "ne2b_csr.cu", "ne2b_readout.cu", "ne2b_host.cpp",
            "ne2b_ne2.cpp"]
 HEADERS = ["ne2b_device.cuh", "ne2b_layout.h", "ne2b_kernels.h", "ne2b_engine.h", "ne2b_handles.h", "ne2b_parallel.h",
            "ne2b_step.cuh", "ne2b_step_kind.h", "ne2b_net.h", "ne2b_csr.h"]

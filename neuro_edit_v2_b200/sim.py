@@ -360,6 +360,21 @@ class Batch:
         check(lib.ne2b_batch_window_counts(self._h, net, window, ptr(out)))
         return out
 
+    def fit_ridge_multi(self, nets, windows: int, labels, k: int, lam: float) -> np.ndarray:
+        """Ridge readout (readout.rs:190-252) trained on the device from the
+        window counts of `nets` (one trial each, features [windows][n]):
+        [k x (windows * n + 1)] weights, bias last."""
+        ns = np.ascontiguousarray(nets, dtype=np.uint32)
+        lab = np.ascontiguousarray(labels, dtype=np.uint32)
+        if lab.shape != ns.shape:
+            raise ValueError("one label per trial")
+        n = self.sizes[int(ns[0])]
+        w = np.zeros((k, windows * n + 1), np.float64)
+        nf = C.c_uint32()
+        check(lib.ne2b_batch_fit_ridge_multi(self._h, ptr(ns), len(ns), windows, ptr(lab), k, float(lam),
+                                             C.byref(nf), ptr(w)))
+        return w
+
     def spikes_total(self, net: int) -> int:
         v = C.c_uint64()
         check(lib.ne2b_batch_spikes_total(self._h, net, C.byref(v)))

@@ -593,6 +593,95 @@ uint64_t ne2o_expf_mismatches(float (*f)(float), float lo, float hi, uint32_t st
     return bad;
 }
 
+/* ============================================================ readout */
+/* sim/src/readout.rs:144-188: L L^T = a, then L z = b, L^T w = z */
+int ne2o_cholesky_solve(const double *a, const double *b, uint32_t n, double *w) {
+    double *l = (double *)calloc((size_t)n * n, sizeof(double));
+    double *z = (double *)calloc(n ? n : 1, sizeof(double));
+    int ok = 1;
+    for (uint32_t i = 0; i < n && ok; ++i)
+        for (uint32_t j = 0; j <= i; ++j) {
+            double sum = a[(size_t)i * n + j];
+            for (uint32_t k = 0; k < j; ++k) sum -= l[(size_t)i * n + k] * l[(size_t)j * n + k];
+            if (i == j) {
+                if (sum <= 0.0) {
+                    ok = 0;
+                    break;
+                }
+                l[(size_t)i * n + j] = sqrt(sum);
+            } else {
+                l[(size_t)i * n + j] = sum / l[(size_t)j * n + j];
+            }
+        }
+    if (ok) {
+        for (uint32_t i = 0; i < n; ++i) {
+            double sum = b[i];
+            for (uint32_t k = 0; k < i; ++k) sum -= l[(size_t)i * n + k] * z[k];
+            z[i] = sum / l[(size_t)i * n + i];
+        }
+        for (uint32_t i = n; i-- > 0;) {
+            double sum = z[i];
+            for (uint32_t k = i + 1; k < n; ++k) sum -= l[(size_t)k * n + i] * w[k];
+            w[i] = sum / l[(size_t)i * n + i];
+        }
+    }
+    free(l);
+    free(z);
+    return ok;
+}
+
+/* sim/src/readout.rs:190-252: centre the columns, Gram G = Xc Xc^T + lambda I
+ * (four accumulators per dot as the reference sums), one Cholesky solve per
+ * class against the centred one-hot targets, w = Xc^T a, bias = ybar - w.mu */
+void ne2o_fit_ridge_multi(const float *x, uint32_t t, uint32_t f, const uint32_t *labels, uint32_t k, double lambda,
+                          double *w_out) {
+    double *mu = (double *)calloc(f ? f : 1, sizeof(double));
+    double *xc = (double *)malloc(sizeof(double) * ((size_t)t * f + 1));
+    double *ybar = (double *)calloc(k ? k : 1, sizeof(double));
+    double *g = (double *)malloc(sizeof(double) * ((size_t)t * t + 1));
+    double *yc = (double *)malloc(sizeof(double) * (t + 1));
+    double *a = (double *)malloc(sizeof(double) * (t + 1));
+    for (uint32_t r = 0; r < t; ++r)
+        for (uint32_t c = 0; c < f; ++c) mu[c] += (double)x[(size_t)r * f + c];
+    for (uint32_t c = 0; c < f; ++c) mu[c] /= (double)t;
+    for (size_t i = 0; i < (size_t)t * f; ++i) xc[i] = (double)x[i] - mu[i % f];
+    for (uint32_t r = 0; r < t; ++r) ybar[labels[r]] += 1.0 / (double)t;
+    for (uint32_t i = 0; i < t; ++i) {
+        const double *ri = xc + (size_t)i * f;
+        for (uint32_t j = 0; j <= i; ++j) {
+            const double *rj = xc + (size_t)j * f;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            const uint32_t f4 = f / 4 * 4;
+            for (uint32_t c = 0; c < f4; c += 4)
+                for (int q = 0; q < 4; ++q) acc[q] += ri[c + q] * rj[c + q];
+            double s = 0.0;
+            for (uint32_t c = f4; c < f; ++c) s += ri[c] * rj[c];
+            s += ((acc[0] + acc[1]) + acc[2]) + acc[3];
+            g[(size_t)i * t + j] = s;
+            g[(size_t)j * t + i] = s;
+        }
+        g[(size_t)i * t + i] += lambda;
+    }
+    for (uint32_t c = 0; c < k; ++c) {
+        for (uint32_t r = 0; r < t; ++r) yc[r] = (labels[r] == c ? 1.0 : 0.0) - ybar[c];
+        if (!ne2o_cholesky_solve(g, yc, t, a))
+            for (uint32_t r = 0; r < t; ++r) a[r] = 0.0;
+        double *w = w_out + (size_t)c * (f + 1);
+        for (uint32_t q = 0; q <= f; ++q) w[q] = 0.0;
+        for (uint32_t r = 0; r < t; ++r)
+            for (uint32_t q = 0; q < f; ++q) w[q] += a[r] * xc[(size_t)r * f + q];
+        double dot = 0.0;
+        for (uint32_t q = 0; q < f; ++q) dot += w[q] * mu[q];
+        w[f] = ybar[c] - dot;
+    }
+    free(mu);
+    free(xc);
+    free(ybar);
+    free(g);
+    free(yc);
+    free(a);
+}
+
 /* ================================================================ sim */
 /* sim/src/state.rs:35-49 defaults, net-format/src/lib.rs:26-39 */
 void ne2o_cfg_default(ne2o_cfg *c) {

@@ -126,6 +126,14 @@ float ne2o_det_expf(float x);
 /* test support: compares f with ne2o_det_expf bit for bit on every
  * `stride`-th float in [lo, hi] (by bit pattern, both signs), split over
  * `threads` threads; returns the mismatches and stores the values checked */
+/* readout training, sim/src/readout.rs:190-252 fit_ridge_multi: multi-class
+ * ridge in the dual on the column-centred design x[T*F] (f32), labels[T] in
+ * 0..k-1; w_out[k][F + 1] (bias last).  A Gram matrix that is not positive
+ * definite gives zero dual weights, as the reference does. */
+void ne2o_fit_ridge_multi(const float *x, uint32_t t, uint32_t f, const uint32_t *labels, uint32_t k, double lambda,
+                          double *w_out);
+/* readout.rs:144-188 cholesky_solve (row-major n x n); 0 when not PD */
+int ne2o_cholesky_solve(const double *a, const double *b, uint32_t n, double *w);
 uint64_t ne2o_expf_mismatches(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
                               uint64_t *checked);
 

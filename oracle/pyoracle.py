@@ -81,6 +81,8 @@ def lib() -> C.CDLL:
             "ne2o_gauss_scale": (f32, [f32]),
             "ne2o_det_expf": (f32, [f32]),
             "ne2o_expf_mismatches": (u64, [vp, f32, f32, u32, u32, vp]),
+            "ne2o_fit_ridge_multi": (None, [vp, u32, u32, vp, u32, f64, vp]),
+            "ne2o_cholesky_solve": (i32, [vp, vp, u32, vp]),
             "ne2o_cfg_default": (None, [vp]),
             "ne2o_sim_new": (vp, [vp, vp, C.c_char_p, C.c_size_t]),
             "ne2o_sim_free": (None, [vp]), "ne2o_sim_step": (None, [vp]),
@@ -418,3 +420,13 @@ def gauss_numer(i, t, seed) -> int:
 
 def det_expf(x) -> float:
     return float(lib().ne2o_det_expf(x))
+
+
+def fit_ridge_multi(x, labels, k: int, lam: float) -> np.ndarray:
+    """sim/src/readout.rs:190-252 on a [T x F] design: [k x (F + 1)] weights, bias last."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    lab = np.ascontiguousarray(labels, dtype=np.uint32)
+    t, f = x.shape
+    w = np.zeros((k, f + 1), np.float64)
+    lib().ne2o_fit_ridge_multi(_p(x), t, f, _p(lab), k, float(lam), _p(w))
+    return w

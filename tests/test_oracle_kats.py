@@ -451,3 +451,35 @@ def test_adex_noise_gain_drives_lone_neuron():
     higher noise rate."""
     assert _lone_adex_rate(60.0, 14.0) > 0.5
     assert _lone_adex_rate(120.0, 18.0) > 1.5 * _lone_adex_rate(30.0, 18.0)
+
+
+def test_ridge_multi_oracle_equals_the_dual_solution():
+    """readout.rs:190-252 restated: the dual ridge weights equal numpy's
+    solve of (Xc Xc^T + lambda I) A = Yc, w = Xc^T A, bias = ybar - w.mu."""
+    rng = np.random.default_rng(0)
+    t, f, k, lam = 60, 203, 3, 0.5
+    x = rng.poisson(2.0, (t, f)).astype(np.float32)
+    lab = rng.integers(0, k, t)
+    w = O.fit_ridge_multi(x, lab, k, lam)
+    xd = x.astype(np.float64)
+    mu = xd.mean(0)
+    xc = xd - mu
+    ybar = np.array([np.mean(lab == c) for c in range(k)])
+    yc = np.stack([(lab == c) - ybar[c] for c in range(k)], 1)
+    a = np.linalg.solve(xc @ xc.T + lam * np.eye(t), yc)
+    ww = (xc.T @ a).T
+    ref = np.concatenate([ww, (ybar - ww @ mu)[:, None]], 1)
+    assert np.abs(w - ref).max() < 1e-12 * max(1.0, np.abs(ref).max())
+
+
+def test_cholesky_solve_rejects_a_matrix_that_is_not_positive_definite():
+    """readout.rs:153-156: a non-positive pivot ends the factorization."""
+    import ctypes
+
+    a = np.array([[1.0, 2.0], [2.0, 1.0]])
+    b = np.ones(2)
+    w = np.zeros(2)
+    assert O.lib().ne2o_cholesky_solve(a.ctypes.data, b.ctypes.data, 2, w.ctypes.data) == 0
+    a = np.array([[4.0, 2.0], [2.0, 3.0]])
+    assert O.lib().ne2o_cholesky_solve(a.ctypes.data, b.ctypes.data, 2, w.ctypes.data) == 1
+    assert np.allclose(a @ w, b)

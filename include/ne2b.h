@@ -249,6 +249,9 @@ ne2b_status ne2b_batch_kernel_launches(ne2b_batch *b, uint64_t *launches);
 ne2b_status ne2b_batch_fit_ridge_multi(ne2b_batch *b, const uint32_t *nets, uint32_t t, uint32_t windows,
                                        const uint32_t *labels, uint32_t k, double lambda, uint32_t *n_features,
                                        double *w);
+/* ne2b_fit_ridge on the same device-resident features, host targets y[T]. */
+ne2b_status ne2b_batch_fit_ridge(ne2b_batch *b, const uint32_t *nets, uint32_t t, uint32_t windows, const float *y,
+                                 float lambda, uint32_t *n_features, double *w);
 
 /* -------------------------------------------------------------- serving */
 /* Continuous batching of trial requests: requests are admitted into free
@@ -315,6 +318,13 @@ ne2b_status ne2b_server_kernel_launches(ne2b_server *s, uint64_t *launches);
  * T at most 32768 (the T x T Gram matrix is f64). */
 ne2b_status ne2b_fit_ridge_multi(const float *x, uint32_t t, uint32_t f, const uint32_t *labels, uint32_t k,
                                  double lambda, int device, double *w);
+/* fit_ridge (readout.rs:103-141): binary ridge in the primal on x[T x F]
+ * (host or device memory) and host targets y[T]; w[F + 1], bias last, equal
+ * to the reference's bit for bit (the (F + 1)^2 normal matrix, its
+ * Cholesky factor and the fallback with 1e-3 + lambda more on the diagonal
+ * as there).  F at most 32767. */
+ne2b_status ne2b_fit_ridge(const float *x, uint32_t t, uint32_t f, const float *y, float lambda, int device,
+                           double *w);
 
 /* ----------------------------------------------------------- net building */
 /* A host-side network owned by the library, in the ne2b_net_desc layout. */

@@ -12,14 +12,14 @@ from ._abi import (KERNEL_AUTO, KERNEL_RESIDENT, KERNEL_STREAM, MODEL_ADEX, MODE
                    default_config)
 from .net import (FlatNet, NativeNet, config_from_meta, from_ne2_bytes, from_synapses, liquid, load_ne2, random_kout,
                   to_adex)
-from .readout import fit_ridge_multi, ridge_predict
+from .readout import fit_ridge, fit_ridge_multi, ridge_predict
 from .sim import B200Sim, Batch, Server, SpikeWindowError, footprint
 
 __all__ = [
     "B200Sim", "Batch", "Server", "SpikeWindowError", "footprint", "FlatNet", "NativeNet", "from_synapses",
     "liquid", "random_kout", "to_adex", "load_ne2", "from_ne2_bytes", "config_from_meta", "Config", "default_config", "Ne2bError", "MODEL_IZH", "MODEL_ADEX",
     "KERNEL_AUTO", "KERNEL_STREAM", "KERNEL_RESIDENT",
-    "expf", "selftest_barrier_timeout", "fit_ridge_multi", "ridge_predict",
+    "expf", "selftest_barrier_timeout", "fit_ridge", "fit_ridge_multi", "ridge_predict",
 ]
 
 

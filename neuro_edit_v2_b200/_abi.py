@@ -139,6 +139,8 @@ _SIGS = {
     "ne2b_syn_count": (C.c_int, [_p, _pu64]),
     "ne2b_fit_ridge_multi": (C.c_int, [_p, _u32, _u32, _p, _u32, _f64, C.c_int, _p]),
     "ne2b_batch_fit_ridge_multi": (C.c_int, [_p, _p, _u32, _u32, _p, _u32, _f64, _pu32, _p]),
+    "ne2b_fit_ridge": (C.c_int, [_p, _u32, _u32, _p, _f32, C.c_int, _p]),
+    "ne2b_batch_fit_ridge": (C.c_int, [_p, _p, _u32, _u32, _p, _f32, _pu32, _p]),
     "ne2b_read_csr": (C.c_int, [_p, _p, _p, _p, _p]),
     "ne2b_n": (C.c_int, [_p, _pu32]),
     "ne2b_step_count": (C.c_int, [_p, _pu64]),

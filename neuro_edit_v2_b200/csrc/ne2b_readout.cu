@@ -1,8 +1,10 @@
 // ne2b_readout.cu — readout training on the GPU, from features that are
 // already on the device (a batch's per-window spike counts) or that the
 // caller passes: the multi-class ridge of sim/src/readout.rs:190-252
-// (`fit_ridge_multi`), solved in the dual.
+// (`fit_ridge_multi`), solved in the dual, and the binary ridge of
+// readout.rs:103-141 (`fit_ridge`), solved in the primal.
 //
+// fit_ridge_multi:
 //   1. column means mu (f64, rows summed in order) and the centred design
 //      Xc = x - mu (f64);
 //   2. the Gram matrix G = Xc Xc^T + lambda I: tiled in shared memory, each
@@ -16,6 +18,13 @@
 //   4. per class, L z = y and L^T a = z on the host (T^2 work), in the
 //      reference's loop order;
 //   5. w = Xc^T a on the device (rows summed in order), bias on the host.
+//
+// fit_ridge: the (F + 1) x (F + 1) normal matrix, each entry summed over the
+// rows in order as the reference accumulates it, the bias column, lambda on
+// the diagonal and off the bias again ((s + lambda) - lambda, as there), the
+// same Cholesky, and the solve on the host; a matrix that is not positive
+// definite is refactored with 1e-3 + lambda more on the diagonal (from a
+// copy kept on the device), then gives zeros.
 //
 // Every f64 operation is an explicit round-to-nearest intrinsic, so nothing
 // is contracted into an FMA: the weights equal the reference's bit for bit.
@@ -153,6 +162,87 @@ __global__ void weights_kernel(const double *__restrict__ xc, const double *__re
     w[(size_t)c * f + q] = s;
 }
 
+// Upper-triangle tiles (bi <= bj) of the normal matrix: a[i][j] = sum over
+// rows r, in order, of x[r][i] x[r][j] (f32 read as f64); both halves of
+// the (F + 1)-wide matrix are written.
+__global__ void __launch_bounds__(256) normal_kernel(const float *__restrict__ x, uint32_t t, uint32_t f,
+                                                     double *__restrict__ a) {
+    __shared__ double si[kGramK][kGramTile + 1];
+    __shared__ double sj[kGramK][kGramTile + 1];
+    const uint32_t id = blockIdx.x;
+    uint32_t bj = (uint32_t)((sqrt(8.0 * id + 1.0) - 1.0) / 2.0);
+    while ((bj + 1) * (bj + 2) / 2 <= id) ++bj;
+    while (bj * (bj + 1) / 2 > id) --bj;
+    const uint32_t bi = id - bj * (bj + 1) / 2;  // bi <= bj
+    const uint32_t i0 = bi * kGramTile, j0 = bj * kGramTile, nf = f + 1u;
+    const uint32_t tx = threadIdx.x & 15u, ty = threadIdx.x >> 4;
+    double acc[2][2] = {};
+    for (uint32_t r0 = 0; r0 < t; r0 += kGramK) {
+        for (uint32_t e = threadIdx.x; e < kGramK * kGramTile; e += 256) {
+            const uint32_t r = e / kGramTile, c = e % kGramTile;
+            const bool in_r = r0 + r < t;
+            si[r][c] = (in_r && i0 + c < f) ? (double)x[(size_t)(r0 + r) * f + i0 + c] : 0.0;
+            sj[r][c] = (in_r && j0 + c < f) ? (double)x[(size_t)(r0 + r) * f + j0 + c] : 0.0;
+        }
+        __syncthreads();
+        const uint32_t rn = min(kGramK, t - r0);
+        for (uint32_t r = 0; r < rn; ++r)
+#pragma unroll
+            for (int p = 0; p < 2; ++p)
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    acc[p][q] = __dadd_rn(acc[p][q], __dmul_rn(si[r][ty * 2 + p], sj[r][tx * 2 + q]));
+        __syncthreads();
+    }
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const uint32_t i = i0 + ty * 2 + p, j = j0 + tx * 2 + q;
+            if (i >= f || j >= f || i > j) continue;
+            a[(size_t)i * nf + j] = acc[p][q];
+            a[(size_t)j * nf + i] = acc[p][q];
+        }
+}
+
+// The bias column (sum of each feature over the rows, in order), the
+// right-hand side b[i] = sum of x[r][i] y[r], and b[f] = sum of y.
+__global__ void bias_rhs_kernel(const float *__restrict__ x, const float *__restrict__ y, uint32_t t, uint32_t f,
+                                double *__restrict__ a, double *__restrict__ b) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nf = f + 1u;
+    if (j > f) return;
+    double s = 0.0, sb = 0.0;
+    for (uint32_t r = 0; r < t; ++r) {
+        const double yr = (double)y[r];
+        if (j < f) {
+            const double xv = (double)x[(size_t)r * f + j];
+            s = __dadd_rn(s, xv);
+            sb = __dadd_rn(sb, __dmul_rn(xv, yr));
+        } else {
+            sb = __dadd_rn(sb, yr);
+        }
+    }
+    b[j] = sb;
+    if (j < f) {
+        a[(size_t)j * nf + f] = s;
+        a[(size_t)f * nf + j] = s;
+    } else {
+        double ones = 0.0;
+        for (uint32_t r = 0; r < t; ++r) ones = __dadd_rn(ones, 1.0);
+        a[(size_t)f * nf + f] = ones;
+    }
+}
+
+// a[i][i] += add for every i; with `unbias`, a[f][f] then loses lambda again.
+__global__ void diag_kernel(double *a, uint32_t n, double add, bool unbias, double lambda) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = __dadd_rn(a[(size_t)i * n + i], add);
+    if (unbias && i + 1u == n) v = __dsub_rn(v, lambda);
+    a[(size_t)i * n + i] = v;
+}
+
 // trial r's features: window counts [windows][n] of one net (u16 -> f32)
 __global__ void gather_counts_kernel(const uint16_t *const *__restrict__ win, uint32_t n, uint32_t n_pad,
                                      uint32_t windows, float *__restrict__ x) {
@@ -183,6 +273,78 @@ struct DevBuf {
     }
 };
 
+// G = L L^T in place (lower triangle; n launches of two kernels); true when
+// G is positive definite.
+ne2b_status cholesky(double *g, uint32_t n, unsigned int *bad, cudaStream_t st, bool *pd) {
+    NE2B_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned int), st));
+    for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t below = n - j - 1u;
+        chol_column_kernel<<<(below + 255) / 256 + (below == 0), 256, 0, st>>>(g, n, j, bad);
+        const dim3 blk(16, 16), grd((below + 15) / 16 + (below == 0), (below + 15) / 16 + (below == 0));
+        chol_update_kernel<<<grd, blk, 0, st>>>(g, n, j, bad);
+    }
+    NE2B_CUDA(cudaGetLastError());
+    unsigned int bad_h = 0;
+    NE2B_CUDA(cudaMemcpyAsync(&bad_h, bad, sizeof bad_h, cudaMemcpyDeviceToHost, st));
+    NE2B_CUDA(cudaStreamSynchronize(st));
+    *pd = bad_h == 0;
+    return NE2B_OK;
+}
+
+// L z = b, L^T w = z with L the lower triangle of l (readout.rs:170-186 order).
+void host_solve(const std::vector<double> &l, const double *b, uint32_t n, double *w) {
+    std::vector<double> z(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        double s = b[i];
+        for (uint32_t q = 0; q < i; ++q) s -= l[(size_t)i * n + q] * z[q];
+        z[i] = s / l[(size_t)i * n + i];
+    }
+    for (uint32_t i = n; i-- > 0;) {
+        double s = z[i];
+        for (uint32_t q = i + 1; q < n; ++q) s -= l[(size_t)q * n + i] * w[q];
+        w[i] = s / l[(size_t)i * n + i];
+    }
+}
+
+// fit_ridge on a device design x[T x F] and host targets y[T].
+ne2b_status fit_binary_on_device(const float *x, uint32_t t, uint32_t f, const float *y_host, float lambda,
+                                 cudaStream_t st, double *w_out) {
+    const uint32_t nf = f + 1u;
+    DevBuf buf(st);
+    double *a = nullptr, *a0 = nullptr, *b = nullptr;
+    float *y = nullptr;
+    unsigned int *bad = nullptr;
+    NE2B_TRY(buf.get(&a, (size_t)nf * nf));
+    NE2B_TRY(buf.get(&a0, (size_t)nf * nf));
+    NE2B_TRY(buf.get(&b, nf));
+    NE2B_TRY(buf.get(&y, t));
+    NE2B_TRY(buf.get(&bad, 1));
+    NE2B_CUDA(cudaMemcpyAsync(y, y_host, sizeof(float) * t, cudaMemcpyHostToDevice, st));
+    const uint32_t nt = (f + kGramTile - 1) / kGramTile;
+    normal_kernel<<<nt * (nt + 1) / 2, 256, 0, st>>>(x, t, f, a);
+    bias_rhs_kernel<<<(nf + 255) / 256, 256, 0, st>>>(x, y, t, f, a, b);
+    const double lam = (double)lambda;
+    diag_kernel<<<(nf + 255) / 256, 256, 0, st>>>(a, nf, lam, true, lam);
+    NE2B_CUDA(cudaMemcpyAsync(a0, a, sizeof(double) * nf * nf, cudaMemcpyDeviceToDevice, st));
+    bool pd = false;
+    NE2B_TRY(cholesky(a, nf, bad, st, &pd));
+    if (!pd) {  // readout.rs:131-139: more regularisation, once
+        NE2B_CUDA(cudaMemcpyAsync(a, a0, sizeof(double) * nf * nf, cudaMemcpyDeviceToDevice, st));
+        diag_kernel<<<(nf + 255) / 256, 256, 0, st>>>(a, nf, 1e-3 + lam, false, 0.0);
+        NE2B_TRY(cholesky(a, nf, bad, st, &pd));
+    }
+    if (!pd) {
+        for (uint32_t i = 0; i < nf; ++i) w_out[i] = 0.0;
+        return NE2B_OK;
+    }
+    std::vector<double> l((size_t)nf * nf), bh(nf);
+    NE2B_CUDA(cudaMemcpyAsync(l.data(), a, sizeof(double) * l.size(), cudaMemcpyDeviceToHost, st));
+    NE2B_CUDA(cudaMemcpyAsync(bh.data(), b, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
+    NE2B_CUDA(cudaStreamSynchronize(st));
+    host_solve(l, bh.data(), nf, w_out);
+    return NE2B_OK;
+}
+
 ne2b_status check_labels(const uint32_t *labels, uint32_t t, uint32_t f, uint32_t k) {
     if (t < 2 || k < 2 || f == 0)
         return set_error(NE2B_EINVAL, "fit_ridge_multi: need T >= 2, K >= 2, F >= 1 (T=%u F=%u K=%u)", t, f, k);
@@ -204,41 +366,24 @@ ne2b_status fit_on_device(const float *x, uint32_t t, uint32_t f, const uint32_t
     NE2B_TRY(buf.get(&a, (size_t)t * k));
     NE2B_TRY(buf.get(&w, (size_t)f * k));
     NE2B_TRY(buf.get(&bad, 1));
-    NE2B_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned int), st));
     col_mean_kernel<<<(f + 255) / 256, 256, 0, st>>>(x, t, f, mu);
     const uint64_t n = (uint64_t)t * f;
     center_kernel<<<(unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 64), 256, 0, st>>>(x, n, f, mu, xc);
     const uint32_t nt = (t + kGramTile - 1) / kGramTile;
     gram_kernel<<<nt * (nt + 1) / 2, 256, 0, st>>>(xc, t, f, lambda, g);
-    for (uint32_t j = 0; j < t; ++j) {
-        const uint32_t below = t - j - 1u;
-        chol_column_kernel<<<(below + 255) / 256 + (below == 0), 256, 0, st>>>(g, t, j, bad);
-        const dim3 blk(16, 16), grd((below + 15) / 16 + (below == 0), (below + 15) / 16 + (below == 0));
-        chol_update_kernel<<<grd, blk, 0, st>>>(g, t, j, bad);
-    }
-    NE2B_CUDA(cudaGetLastError());
+    bool pd = false;
+    NE2B_TRY(cholesky(g, t, bad, st, &pd));
     // the triangular solves on the host, in the reference's order
     std::vector<double> L((size_t)t * t), mu_h(f);
-    unsigned int bad_h = 0;
     NE2B_CUDA(cudaMemcpyAsync(L.data(), g, sizeof(double) * L.size(), cudaMemcpyDeviceToHost, st));
     NE2B_CUDA(cudaMemcpyAsync(mu_h.data(), mu, sizeof(double) * f, cudaMemcpyDeviceToHost, st));
-    NE2B_CUDA(cudaMemcpyAsync(&bad_h, bad, sizeof bad_h, cudaMemcpyDeviceToHost, st));
     NE2B_CUDA(cudaStreamSynchronize(st));
-    std::vector<double> ybar(k, 0.0), ah((size_t)t * k, 0.0), z(t);
+    std::vector<double> ybar(k, 0.0), ah((size_t)t * k, 0.0), yc(t);
     for (uint32_t r = 0; r < t; ++r) ybar[labels[r]] += 1.0 / (double)t;
-    if (!bad_h)
+    if (pd)
         for (uint32_t c = 0; c < k; ++c) {
-            double *ac = ah.data() + (size_t)c * t;
-            for (uint32_t i = 0; i < t; ++i) {
-                double s = (labels[i] == c ? 1.0 : 0.0) - ybar[c];
-                for (uint32_t q = 0; q < i; ++q) s -= L[(size_t)i * t + q] * z[q];
-                z[i] = s / L[(size_t)i * t + i];
-            }
-            for (uint32_t i = t; i-- > 0;) {
-                double s = z[i];
-                for (uint32_t q = i + 1; q < t; ++q) s -= L[(size_t)q * t + i] * ac[q];
-                ac[i] = s / L[(size_t)i * t + i];
-            }
+            for (uint32_t i = 0; i < t; ++i) yc[i] = (labels[i] == c ? 1.0 : 0.0) - ybar[c];
+            host_solve(L, yc.data(), t, ah.data() + (size_t)c * t);
         }
     NE2B_CUDA(cudaMemcpyAsync(a, ah.data(), sizeof(double) * ah.size(), cudaMemcpyHostToDevice, st));
     weights_kernel<<<dim3((f + 255) / 256, k), 256, 0, st>>>(xc, a, t, f, k, w);
@@ -299,47 +444,111 @@ ne2b_status ne2b_fit_ridge_multi(const float *x, uint32_t t, uint32_t f, const u
     }
 }
 
+}  // extern "C"
+
+// A batch's window counts as a [t x windows*n] design on its stream.
+static ne2b_status gather_batch(ne2b_batch *b, const uint32_t *nets, uint32_t t, uint32_t windows,
+                                ne2b::DevBuf &buf, float **x, uint32_t *f_out) {
+    if (t == 0 || windows == 0) return set_error(NE2B_EINVAL, "batch readout: no trials or no windows");
+    std::vector<const uint16_t *> win(t);
+    uint32_t n = 0, n_pad = 0;
+    for (uint32_t r = 0; r < t; ++r) {
+        if (nets[r] >= b->slots.size()) return set_error(NE2B_EINVAL, "net %u out of range", nets[r]);
+        ne2b::NetHost *h = b->eng.net(b->slots[nets[r]]);
+        if (!h) return set_error(NE2B_EINVAL, "net %u has no network", nets[r]);
+        if (r == 0) {
+            n = h->n;
+            n_pad = h->n_pad;
+        } else if (h->n != n) {
+            return set_error(NE2B_EINVAL, "the trials' nets differ in size (%u and %u neurons)", n, h->n);
+        }
+        const uint64_t done = h->dev.win_steps ? h->t / h->dev.win_steps : 0;
+        if (!h->dev.win_out || done < windows || windows > h->dev.max_windows)
+            return set_error(NE2B_EINVAL, "net %u has %llu of the %u windows asked for", nets[r],
+                             (unsigned long long)done, windows);
+        win[r] = h->dev.win_out;
+    }
+    const uint64_t f64 = (uint64_t)windows * n;
+    if (f64 == 0 || f64 > 0xffffffffull) return set_error(NE2B_UNSUPPORTED, "%llu features", (unsigned long long)f64);
+    const uint32_t f = (uint32_t)f64;
+    cudaStream_t st = b->eng.stream();  // after the batch's queued steps
+    const uint16_t **wd = nullptr;
+    NE2B_TRY(buf.get(&wd, t));
+    NE2B_TRY(buf.get(x, (size_t)t * f));
+    NE2B_CUDA(cudaMemcpyAsync(wd, win.data(), sizeof(void *) * t, cudaMemcpyHostToDevice, st));
+    ne2b::gather_counts_kernel<<<dim3((f + 255) / 256 < 1024 ? (f + 255) / 256 : 1024, t), 256, 0, st>>>(
+        wd, n, n_pad, windows, *x);
+    NE2B_CUDA(cudaGetLastError());
+    *f_out = f;
+    return NE2B_OK;
+}
+
+extern "C" {
+
 ne2b_status ne2b_batch_fit_ridge_multi(ne2b_batch *b, const uint32_t *nets, uint32_t t, uint32_t windows,
                                        const uint32_t *labels, uint32_t k, double lambda, uint32_t *n_features,
                                        double *w) {
     if (!b || !nets || !labels || !w) return set_error(NE2B_EINVAL, "ne2b_batch_fit_ridge_multi: null argument");
-    if (t == 0 || windows == 0) return set_error(NE2B_EINVAL, "ne2b_batch_fit_ridge_multi: no trials or no windows");
     try {
-        std::vector<const uint16_t *> win(t);
-        uint32_t n = 0, n_pad = 0;
-        for (uint32_t r = 0; r < t; ++r) {
-            if (nets[r] >= b->slots.size()) return set_error(NE2B_EINVAL, "net %u out of range", nets[r]);
-            ne2b::NetHost *h = b->eng.net(b->slots[nets[r]]);
-            if (!h) return set_error(NE2B_EINVAL, "net %u has no network", nets[r]);
-            if (r == 0) {
-                n = h->n;
-                n_pad = h->n_pad;
-            } else if (h->n != n) {
-                return set_error(NE2B_EINVAL, "the trials' nets differ in size (%u and %u neurons)", n, h->n);
-            }
-            const uint64_t done = h->dev.win_steps ? h->t / h->dev.win_steps : 0;
-            if (!h->dev.win_out || done < windows || windows > h->dev.max_windows)
-                return set_error(NE2B_EINVAL, "net %u has %llu of the %u windows asked for", nets[r],
-                                 (unsigned long long)done, windows);
-            win[r] = h->dev.win_out;
-        }
-        const uint64_t f64 = (uint64_t)windows * n;
-        if (f64 > 0xffffffffull) return set_error(NE2B_UNSUPPORTED, "more than 2^32-1 features");
-        const uint32_t f = (uint32_t)f64;
+        ne2b::DevBuf buf(b->eng.stream());
+        float *x = nullptr;
+        uint32_t f = 0;
+        NE2B_TRY(gather_batch(b, nets, t, windows, buf, &x, &f));
         const ne2b_status cs = ne2b::check_labels(labels, t, f, k);
         if (cs != NE2B_OK) return cs;
         if (n_features) *n_features = f;
-        cudaStream_t st = b->eng.stream();  // after the batch's queued steps
-        ne2b::DevBuf buf(st);
-        const uint16_t **wd = nullptr;
+        return ne2b::fit_on_device(x, t, f, labels, k, lambda, b->eng.stream(), w);
+    } catch (const std::bad_alloc &) {
+        return set_error(NE2B_ENOMEM, "host allocation failed");
+    }
+}
+
+ne2b_status ne2b_fit_ridge(const float *x, uint32_t t, uint32_t f, const float *y, float lambda, int device,
+                           double *w) {
+    if (!x || !y || !w) return set_error(NE2B_EINVAL, "ne2b_fit_ridge: null argument");
+    if (t == 0 || f == 0) return set_error(NE2B_EINVAL, "fit_ridge: need T >= 1, F >= 1 (T=%u F=%u)", t, f);
+    if (f >= 32768) return set_error(NE2B_UNSUPPORTED, "fit_ridge: at most 32767 features (F=%u)", f);
+    try {
+        cudaError_t e = cudaSetDevice(device);
+        if (e != cudaSuccess) return ne2b::cuda_error(e, "cudaSetDevice");
+        cudaPointerAttributes attr{};
+        const bool on_device = cudaPointerGetAttributes(&attr, x) == cudaSuccess && attr.type == cudaMemoryTypeDevice;
+        cudaGetLastError();
+        cudaStream_t st = nullptr;
+        e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return ne2b::cuda_error(e, "cudaStreamCreate");
+        ne2b_status r = NE2B_OK;
+        {
+            ne2b::DevBuf buf(st);
+            const float *xd = x;
+            if (!on_device) {
+                float *p = nullptr;
+                r = buf.get(&p, (size_t)t * f);
+                if (r == NE2B_OK)
+                    r = ne2b::cuda_error(cudaMemcpyAsync(p, x, sizeof(float) * (size_t)t * f, cudaMemcpyHostToDevice, st),
+                                         "design upload");
+                xd = p;
+            }
+            if (r == NE2B_OK) r = ne2b::fit_binary_on_device(xd, t, f, y, lambda, st, w);
+        }
+        cudaStreamDestroy(st);
+        return r;
+    } catch (const std::bad_alloc &) {
+        return set_error(NE2B_ENOMEM, "host allocation failed");
+    }
+}
+
+ne2b_status ne2b_batch_fit_ridge(ne2b_batch *b, const uint32_t *nets, uint32_t t, uint32_t windows, const float *y,
+                                 float lambda, uint32_t *n_features, double *w) {
+    if (!b || !nets || !y || !w) return set_error(NE2B_EINVAL, "ne2b_batch_fit_ridge: null argument");
+    try {
+        ne2b::DevBuf buf(b->eng.stream());
         float *x = nullptr;
-        NE2B_TRY(buf.get(&wd, t));
-        NE2B_TRY(buf.get(&x, (size_t)t * f));
-        NE2B_CUDA(cudaMemcpyAsync(wd, win.data(), sizeof(void *) * t, cudaMemcpyHostToDevice, st));
-        ne2b::gather_counts_kernel<<<dim3((f + 255) / 256 < 1024 ? (f + 255) / 256 : 1024, t), 256, 0, st>>>(
-            wd, n, n_pad, windows, x);
-        NE2B_CUDA(cudaGetLastError());
-        return ne2b::fit_on_device(x, t, f, labels, k, lambda, st, w);
+        uint32_t f = 0;
+        NE2B_TRY(gather_batch(b, nets, t, windows, buf, &x, &f));
+        if (f >= 32768) return set_error(NE2B_UNSUPPORTED, "fit_ridge: at most 32767 features (F=%u)", f);
+        if (n_features) *n_features = f;
+        return ne2b::fit_binary_on_device(x, t, f, y, lambda, b->eng.stream(), w);
     } catch (const std::bad_alloc &) {
         return set_error(NE2B_ENOMEM, "host allocation failed");
     }

@@ -41,6 +41,19 @@ def fit_ridge_multi(x, labels, k: int, lam: float, device: int = 0) -> np.ndarra
     return w
 
 
+def fit_ridge(x, y, lam: float, device: int = 0) -> np.ndarray:
+    """F + 1 ridge weights (bias last) of the design x [T x F] for the
+    targets y (e.g. 0/1 or +-1)."""
+    p, t, f, keep = _design_pointer(x)
+    yy = np.ascontiguousarray(y, dtype=np.float32)
+    if yy.shape != (t,):
+        raise ValueError("one target per row")
+    w = np.zeros(f + 1, np.float64)
+    check(lib.ne2b_fit_ridge(p, t, f, yy.ctypes.data, float(lam), device, w.ctypes.data))
+    del keep
+    return w
+
+
 def ridge_predict(w: np.ndarray, x) -> np.ndarray:
     """Argmax class per row (the reference's ridge_predict): x @ w[:, :F].T + bias."""
     x = np.asarray(x, dtype=np.float64)

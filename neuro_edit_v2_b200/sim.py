@@ -375,6 +375,19 @@ class Batch:
                                              C.byref(nf), ptr(w)))
         return w
 
+    def fit_ridge(self, nets, windows: int, y, lam: float) -> np.ndarray:
+        """Binary ridge readout (readout.rs:103-141) trained on the device
+        from the window counts of `nets`: windows * n + 1 weights, bias last."""
+        ns = np.ascontiguousarray(nets, dtype=np.uint32)
+        yy = np.ascontiguousarray(y, dtype=np.float32)
+        if yy.shape != ns.shape:
+            raise ValueError("one target per trial")
+        n = self.sizes[int(ns[0])]
+        w = np.zeros(windows * n + 1, np.float64)
+        nf = C.c_uint32()
+        check(lib.ne2b_batch_fit_ridge(self._h, ptr(ns), len(ns), windows, ptr(yy), float(lam), C.byref(nf), ptr(w)))
+        return w
+
     def spikes_total(self, net: int) -> int:
         v = C.c_uint64()
         check(lib.ne2b_batch_spikes_total(self._h, net, C.byref(v)))

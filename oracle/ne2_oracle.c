@@ -630,6 +630,39 @@ int ne2o_cholesky_solve(const double *a, const double *b, uint32_t n, double *w)
     return ok;
 }
 
+/* sim/src/readout.rs:103-141: a[i][j] (i <= j) and b accumulated row by row,
+ * the bias column, symmetrised, lambda on the diagonal and taken off the
+ * bias again; not positive definite: 1e-3 + lambda more on the diagonal,
+ * then zeros */
+void ne2o_fit_ridge(const float *x, uint32_t t, uint32_t f, const float *y, float lambda, double *w_out) {
+    const uint32_t nf = f + 1;
+    double *a = (double *)calloc((size_t)nf * nf, sizeof(double));
+    double *b = (double *)calloc(nf, sizeof(double));
+    for (uint32_t r = 0; r < t; ++r) {
+        const float *row = x + (size_t)r * f;
+        for (uint32_t i = 0; i < f; ++i) {
+            const double xi = (double)row[i];
+            b[i] += xi * (double)y[r];
+            for (uint32_t j = i; j < f; ++j) a[(size_t)i * nf + j] += xi * (double)row[j];
+        }
+        b[f] += (double)y[r];
+        for (uint32_t j = 0; j < f; ++j) a[(size_t)j * nf + f] += (double)row[j];
+        a[(size_t)f * nf + f] += 1.0;
+    }
+    for (uint32_t i = 0; i < nf; ++i) {
+        for (uint32_t j = 0; j < i; ++j) a[(size_t)i * nf + j] = a[(size_t)j * nf + i];
+        a[(size_t)i * nf + i] += (double)lambda;
+    }
+    a[(size_t)f * nf + f] -= (double)lambda;
+    if (!ne2o_cholesky_solve(a, b, nf, w_out)) {
+        for (uint32_t i = 0; i < nf; ++i) a[(size_t)i * nf + i] += 1e-3 + (double)lambda;
+        if (!ne2o_cholesky_solve(a, b, nf, w_out))
+            for (uint32_t i = 0; i < nf; ++i) w_out[i] = 0.0;
+    }
+    free(a);
+    free(b);
+}
+
 /* sim/src/readout.rs:190-252: centre the columns, Gram G = Xc Xc^T + lambda I
  * (four accumulators per dot as the reference sums), one Cholesky solve per
  * class against the centred one-hot targets, w = Xc^T a, bias = ybar - w.mu */

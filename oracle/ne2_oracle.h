@@ -132,6 +132,9 @@ float ne2o_det_expf(float x);
  * definite gives zero dual weights, as the reference does. */
 void ne2o_fit_ridge_multi(const float *x, uint32_t t, uint32_t f, const uint32_t *labels, uint32_t k, double lambda,
                           double *w_out);
+/* readout.rs:103-141 fit_ridge: binary ridge in the primal (normal
+ * equations with a bias column, the bias unregularised); w_out[F + 1] */
+void ne2o_fit_ridge(const float *x, uint32_t t, uint32_t f, const float *y, float lambda, double *w_out);
 /* readout.rs:144-188 cholesky_solve (row-major n x n); 0 when not PD */
 int ne2o_cholesky_solve(const double *a, const double *b, uint32_t n, double *w);
 uint64_t ne2o_expf_mismatches(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,

@@ -82,6 +82,7 @@ def lib() -> C.CDLL:
             "ne2o_det_expf": (f32, [f32]),
             "ne2o_expf_mismatches": (u64, [vp, f32, f32, u32, u32, vp]),
             "ne2o_fit_ridge_multi": (None, [vp, u32, u32, vp, u32, f64, vp]),
+            "ne2o_fit_ridge": (None, [vp, u32, u32, vp, f32, vp]),
             "ne2o_cholesky_solve": (i32, [vp, vp, u32, vp]),
             "ne2o_cfg_default": (None, [vp]),
             "ne2o_sim_new": (vp, [vp, vp, C.c_char_p, C.c_size_t]),
@@ -429,4 +430,14 @@ def fit_ridge_multi(x, labels, k: int, lam: float) -> np.ndarray:
     t, f = x.shape
     w = np.zeros((k, f + 1), np.float64)
     lib().ne2o_fit_ridge_multi(_p(x), t, f, _p(lab), k, float(lam), _p(w))
+    return w
+
+
+def fit_ridge(x, y, lam: float) -> np.ndarray:
+    """sim/src/readout.rs:103-141 on a [T x F] design: F + 1 weights, bias last."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    t, f = x.shape
+    w = np.zeros(f + 1, np.float64)
+    lib().ne2o_fit_ridge(_p(x), t, f, _p(y), float(lam), _p(w))
     return w

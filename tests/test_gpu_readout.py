@@ -76,6 +76,45 @@ def test_batch_window_counts_train_the_readout_on_the_device():
     assert np.array_equal(w.view(np.uint64), ref.view(np.uint64))
 
 
+@pytest.mark.parametrize("t, f, lam", [(80, 31, 0.5), (200, 517, 1.0), (33, 64, 0.25)])
+def test_binary_ridge_equals_the_oracle_bit_for_bit(t, f, lam):
+    x, r = design(t, f, 3 * t + f)
+    y = (r % 2).astype(np.float32) * 2 - 1
+    w = nb.fit_ridge(x, y, lam)
+    ref = O.fit_ridge(x, y, lam)
+    assert np.array_equal(w.view(np.uint64), ref.view(np.uint64))
+    assert np.abs(w).max() > 0
+
+
+def test_binary_ridge_fallback_regularisation_matches():
+    """A duplicated feature and lambda = 0: the normal matrix is singular, so
+    the reference refactors with 1e-3 more on the diagonal (readout.rs:131-139)."""
+    x, r = design(60, 12, 4)
+    x[:, 5] = x[:, 4]
+    y = (r % 2).astype(np.float32)
+    w = nb.fit_ridge(x, y, 0.0)
+    ref = O.fit_ridge(x, y, 0.0)
+    assert np.array_equal(np.nan_to_num(w).view(np.uint64), np.nan_to_num(ref).view(np.uint64))
+
+
+def test_batch_counts_train_the_binary_readout():
+    t, win, nwin = 20, 100, 5
+    net = nb.liquid(7, 9)
+    cfgs = [nb.default_config(int_weights=1, window_steps=win, max_windows=nwin, seed=50 + r) for r in range(t)]
+    b = nb.Batch([net] * t, cfgs)
+    rng = np.random.default_rng(2)
+    for r in range(t):
+        bits = (rng.random((win * nwin // 10 + 1, 8)) < 0.05).astype(np.float32)
+        b.set_input_matrix(r, np.repeat(bits, 10, axis=0)[: win * nwin])
+    b.run_steps(win * nwin)
+    b.synchronize()
+    y = (np.arange(t) % 2).astype(np.float32)
+    w = b.fit_ridge(np.arange(t), nwin, y, 1.0)
+    x = np.stack([np.concatenate([b.window_counts(r, q).astype(np.float32) for q in range(nwin)]) for r in range(t)])
+    ref = O.fit_ridge(x, y, 1.0)
+    assert np.array_equal(w.view(np.uint64), ref.view(np.uint64))
+
+
 def test_arguments_the_reference_rejects():
     x, _ = design(10, 5, 1)
     with pytest.raises(nb.Ne2bError, match="label"):

@@ -483,3 +483,17 @@ def test_cholesky_solve_rejects_a_matrix_that_is_not_positive_definite():
     a = np.array([[4.0, 2.0], [2.0, 3.0]])
     assert O.lib().ne2o_cholesky_solve(a.ctypes.data, b.ctypes.data, 2, w.ctypes.data) == 1
     assert np.allclose(a @ w, b)
+
+
+def test_ridge_oracle_equals_the_normal_equations():
+    """readout.rs:103-141 restated: (X1^T X1 + lambda I', bias unregularised) w = X1^T y."""
+    rng = np.random.default_rng(1)
+    t, f, lam = 80, 31, 0.5
+    x = rng.poisson(2.0, (t, f)).astype(np.float32)
+    y = (rng.random(t) < 0.5).astype(np.float32)
+    w = O.fit_ridge(x, y, lam)
+    x1 = np.concatenate([x.astype(np.float64), np.ones((t, 1))], 1)
+    a = x1.T @ x1 + lam * np.eye(f + 1)
+    a[f, f] -= lam
+    ref = np.linalg.solve(a, x1.T @ y.astype(np.float64))
+    assert np.abs(w - ref).max() < 1e-11 * max(1.0, np.abs(ref).max())

@@ -108,6 +108,9 @@ ne2b_status ne2b_destroy(ne2b_sim *sim);
  * ne2b_create, bit for bit, and the same errors are reported.  No
  * per-synapse tau: nets with their own synapse currents use the host
  * build. */
+/* The list arrays and `kind` may each be in host or device memory; device
+ * arrays are read in place (no upload), and must stay valid until the call
+ * returns. */
 ne2b_status ne2b_create_from_synapses(const ne2b_net_desc *net, const uint8_t *kind, uint64_t n_syn,
                                       const uint32_t *src, const uint32_t *tgt, const float *w,
                                       const float *delay_ms, const ne2b_config *cfg, int device, ne2b_sim **out);

@@ -115,13 +115,33 @@ static ne2b_status create_from_list(ne2b::Engine &eng, const ne2b_net_desc *net,
             return _s;                       \
         }                                    \
     } while (0)
+    // arrays already in device memory are read where they are; host arrays
+    // are copied (through the stager's pinned ring when large)
+    bool foreign = false;  // device memory of another GPU
+    auto on_device = [&](const void *q) {
+        cudaPointerAttributes a{};
+        const bool dev = q && cudaPointerGetAttributes(&a, q) == cudaSuccess && a.type == cudaMemoryTypeDevice;
+        cudaGetLastError();
+        if (dev && a.device != eng.device()) foreign = true;
+        return dev;
+    };
+    const bool d_src = on_device(src), d_tgt = on_device(tgt), d_w = on_device(w), d_dly = on_device(dly),
+               d_kind = on_device(kind);
+    if (foreign) return set_error(NE2B_EINVAL, "a synapse-list array is in another GPU's memory (the sim is on GPU %d)",
+                                  eng.device());
+    auto value_at = [&](const void *base, bool dev, uint64_t j) -> uint32_t {  // one 4-byte entry, for messages
+        uint32_t v = 0;
+        if (!dev) memcpy(&v, (const uint8_t *)base + 4 * j, 4);
+        else cudaMemcpy(&v, (const uint8_t *)base + 4 * j, 4, cudaMemcpyDeviceToHost);
+        return v;
+    };
     DevCsrBuild dc;
     void *p = nullptr;
-    LIST_TRY(dalloc(4 * E, &p)); dc.syn.src = (const uint32_t *)p;
-    LIST_TRY(dalloc(4 * E, &p)); dc.syn.tgt = (const uint32_t *)p;
-    LIST_TRY(dalloc(4 * E, &p)); dc.syn.w = (const float *)p;
-    LIST_TRY(dalloc(4 * E, &p)); dc.syn.delay_ms = (const float *)p;
-    LIST_TRY(dalloc(n, &p)); dc.syn.kind = (const uint8_t *)p;
+    if (d_src) dc.syn.src = src; else { LIST_TRY(dalloc(4 * E, &p)); dc.syn.src = (const uint32_t *)p; }
+    if (d_tgt) dc.syn.tgt = tgt; else { LIST_TRY(dalloc(4 * E, &p)); dc.syn.tgt = (const uint32_t *)p; }
+    if (d_w) dc.syn.w = w; else { LIST_TRY(dalloc(4 * E, &p)); dc.syn.w = (const float *)p; }
+    if (d_dly) dc.syn.delay_ms = dly; else { LIST_TRY(dalloc(4 * E, &p)); dc.syn.delay_ms = (const float *)p; }
+    if (d_kind) dc.syn.kind = kind; else { LIST_TRY(dalloc(n, &p)); dc.syn.kind = (const uint8_t *)p; }
     LIST_TRY(dalloc(2 * E, &p)); dc.steps = (const uint16_t *)p;
     LIST_TRY(dalloc(4 * (size_t)n, &p)); dc.counts = (const uint32_t *)p;
     LIST_TRY(dalloc(4 * (size_t)n, &p)); dc.cursor = (uint32_t *)p;
@@ -135,12 +155,12 @@ static ne2b_status create_from_list(ne2b::Engine &eng, const ne2b_net_desc *net,
     dc.syn.dt_ms = cfg->dt_ms;
     CsrScalars sc{~0ull, ~0ull, 1u, 0u};
     if (E) {
-        LIST_TRY(eng.pin_copy((void *)dc.syn.src, src, 4 * E));
-        LIST_TRY(eng.pin_copy((void *)dc.syn.tgt, tgt, 4 * E));
-        LIST_TRY(eng.pin_copy((void *)dc.syn.w, w, 4 * E));
-        LIST_TRY(eng.pin_copy((void *)dc.syn.delay_ms, dly, 4 * E));
+        if (!d_src) LIST_TRY(eng.pin_copy((void *)dc.syn.src, src, 4 * E));
+        if (!d_tgt) LIST_TRY(eng.pin_copy((void *)dc.syn.tgt, tgt, 4 * E));
+        if (!d_w) LIST_TRY(eng.pin_copy((void *)dc.syn.w, w, 4 * E));
+        if (!d_dly) LIST_TRY(eng.pin_copy((void *)dc.syn.delay_ms, dly, 4 * E));
     }
-    if (n) LIST_TRY(eng.pin_copy((void *)dc.syn.kind, kind, n));
+    if (n && !d_kind) LIST_TRY(eng.pin_copy((void *)dc.syn.kind, kind, n));
     LIST_TRY(eng.pin_copy(dc.sc, &sc, sizeof sc));
     LIST_TRY(eng.pin_close());
     LIST_TRY(cuda_error(cudaMemsetAsync((void *)dc.counts, 0, 4 * (size_t)n, st), "memset counts"));
@@ -151,12 +171,15 @@ static ne2b_status create_from_list(ne2b::Engine &eng, const ne2b_net_desc *net,
     if (sc.bad_ref != ~0ull) {
         const uint64_t j = sc.bad_ref;
         LIST_TRY(set_error(NE2B_EINVAL, "synapse %llu references %u -> %u but only %u neurons exist",
-                           (unsigned long long)j, src[j], tgt[j], n));
+                           (unsigned long long)j, value_at(src, d_src, j), value_at(tgt, d_tgt, j), n));
     }
     if (sc.bad_delay != ~0ull) {
         const uint64_t j = sc.bad_delay;
-        LIST_TRY(set_error(NE2B_EINVAL, "synapse %u -> %u: delay %g ms at dt %g ms exceeds the 65535-step ring", src[j],
-                           tgt[j], (double)dly[j], (double)cfg->dt_ms));
+        const uint32_t db = value_at(dly, d_dly, j);
+        float dv;
+        memcpy(&dv, &db, sizeof dv);
+        LIST_TRY(set_error(NE2B_EINVAL, "synapse %u -> %u: delay %g ms at dt %g ms exceeds the 65535-step ring",
+                           value_at(src, d_src, j), value_at(tgt, d_tgt, j), (double)dv, (double)cfg->dt_ms));
     }
     dc.max_delay = sc.max_delay;
     LIST_TRY(eng.add_net_device_csr(net, cfg, dc, slot));

@@ -28,6 +28,22 @@ def _cfg(cfg: _abi.Config | None, **kw) -> _abi.Config:
     return cfg
 
 
+def _list_array(a, dtype):
+    """(length, pointer, keep-alive) of a 1-D synapse-list column: a numpy array (made
+    contiguous in `dtype`) or a contiguous device array of that dtype (any
+    object with __cuda_array_interface__, e.g. a CUDA torch tensor), whose
+    pointer is passed as it is."""
+    cai = getattr(a, "__cuda_array_interface__", None)
+    if cai is not None:
+        if np.dtype(cai["typestr"]) != np.dtype(dtype) or len(cai["shape"]) != 1:
+            raise ValueError(f"a device list column must be 1-D {np.dtype(dtype).name}")
+        if cai.get("strides") not in (None, (np.dtype(dtype).itemsize,)):
+            raise ValueError("a device list column must be contiguous")
+        return int(cai["shape"][0]), int(cai["data"][0]), a
+    a = np.ascontiguousarray(a, dtype=dtype).reshape(-1)
+    return len(a), a.ctypes.data, a
+
+
 class B200Sim:
     """One network on one B200: `Backend` with kind B200."""
 
@@ -52,21 +68,20 @@ class B200Sim:
         self.cfg = _cfg(cfg, **cfg_kw)
         model = np.ascontiguousarray(model, dtype=np.uint8)
         params = np.ascontiguousarray(params, dtype=np.float32)
-        kind = np.ascontiguousarray(kind, dtype=np.uint8)
-        src = np.ascontiguousarray(src, dtype=np.uint32)
-        tgt = np.ascontiguousarray(tgt, dtype=np.uint32)
-        w = np.ascontiguousarray(w, dtype=np.float32)
-        delay_ms = np.ascontiguousarray(delay_ms, dtype=np.float32)
+        cols = [_list_array(a, t) for a, t in ((kind, np.uint8), (src, np.uint32), (tgt, np.uint32),
+                                               (w, np.float32), (delay_ms, np.float32))]
+        (nk, pk, _), (e, ps, _), (nt, pt, _), (nw, pw, _), (nd, pd, _) = cols
         x0 = None if x0 is None else np.ascontiguousarray(x0, dtype=np.float32)
         n = len(model)
+        if nk != n or not nt == nw == nd == e:
+            raise ValueError("one kind per neuron and equal-length src, tgt, w, delay_ms")
         d = _abi.NetDesc()
         d.n = n
         d.model, d.params = model.ctypes.data, params.ctypes.data
         d.param_stride = params.shape[1] if params.ndim == 2 else (params.size // max(n, 1))
         d.x0 = None if x0 is None else x0.ctypes.data
         h = C.c_void_p()
-        check(lib.ne2b_create_from_synapses(C.byref(d), kind.ctypes.data, len(src), src.ctypes.data, tgt.ctypes.data,
-                                            w.ctypes.data, delay_ms.ctypes.data, C.byref(self.cfg), device,
+        check(lib.ne2b_create_from_synapses(C.byref(d), pk, e, ps, pt, pw, pd, C.byref(self.cfg), device,
                                             C.byref(h)))
         self._h = h
         self._net = None

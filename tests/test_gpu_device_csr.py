@@ -128,3 +128,37 @@ def test_errors_equal_the_host_build(case):
     with pytest.raises(nb.Ne2bError) as g:
         nb.B200Sim.from_synapses(model, params, kind, src, tgt, w, d)
     assert str(g.value) == str(h.value)
+
+
+@pytest.mark.parametrize("which", ["all", "list_only"])
+def test_device_resident_lists_are_read_in_place(which):
+    """Synapse lists already in device memory (CUDA torch tensors here) give
+    the CSR, ring and errors of the same list passed from the host."""
+    torch = pytest.importorskip("torch")
+    model, params, kind, src, tgt, w, d = synapse_list(3000, 120_000, 11)
+    cfg = nb.default_config()
+    host = nb.B200Sim.from_synapses(model, params, kind, src, tgt, w, d, cfg)
+    cols = [torch.from_numpy(a).cuda() for a in (src.view(np.int32), tgt.view(np.int32), w, d)]
+    cols[0], cols[1] = _u32(cols[0]), _u32(cols[1])
+    k = torch.from_numpy(kind).cuda() if which == "all" else kind
+    dev = nb.B200Sim.from_synapses(model, params, k, *cols, cfg)
+    same_csr(host, dev)
+    assert dev.ring_depth() == host.ring_depth()
+    bad = d.copy()
+    bad[4321] = np.float32(7000.0)
+    with pytest.raises(nb.Ne2bError) as h:
+        nb.B200Sim.from_synapses(model, params, kind, src, tgt, w, bad, cfg)
+    with pytest.raises(nb.Ne2bError) as g:
+        nb.B200Sim.from_synapses(model, params, k, *cols[:3], torch.from_numpy(bad).cuda(), cfg)
+    assert str(g.value) == str(h.value)
+
+
+def _u32(t):
+    """A CUDA int32 tensor presented as uint32 through the array interface."""
+    class View:
+        def __init__(self, t):
+            self.t = t
+            cai = dict(t.__cuda_array_interface__)
+            cai["typestr"] = "<u4"
+            self.__cuda_array_interface__ = cai
+    return View(t)

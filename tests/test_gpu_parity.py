@@ -238,3 +238,26 @@ def test_resident_and_stream_agree_over_many_launches():
         assert np.array_equal(a.state(slot).view(np.uint32), b.state(slot).view(np.uint32))
     assert np.array_equal(a.trace().view(np.uint32), b.trace().view(np.uint32))
     assert np.array_equal(a.spike_counts(400), b.spike_counts(400))
+
+
+@MODES
+@pytest.mark.parametrize("shape", [(64, 1), (256, 1), (128, 4)], ids=lambda s: f"{s[0]}x{s[1]}")
+def test_synchronous_bursts_int_ring_bit_exact(mode, shape):
+    """A strong constant drive on every neuron makes whole tiles spike in the
+    same step, so a tile delivers up to BLOCK x NPT x 100 synapses: many
+    passes of the block-strided delivery, each thread with its four
+    synapses in flight, the last pass partial.  Bit-exact against the
+    oracle, rows and state."""
+    n = 20_000
+    onet = O.ONet.random_kout(n, 100, 4)
+
+    def drive(s):
+        if isinstance(s, nb.B200Sim):
+            s.set_tile_shape(*shape)
+        set_ext(s, n, range(n), 40.0)
+
+    g, o, first = lockstep(onet, 200, int_weights=True, chunk=50, gauss_sd=1.0, synapse_tau_ms=5.0, drive=drive,
+                           mode=mode)
+    assert first < 0, f"raster diverged at step {first}"
+    assert g.spikes_total() > 5 * n  # ~390 Hz: every neuron fires every few steps
+    assert_state_bits_equal(g, o)

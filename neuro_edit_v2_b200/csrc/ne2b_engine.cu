@@ -15,6 +15,7 @@
 #include <thread>
 
 #include "ne2b_kernels.h"
+#include "ne2b_step_kind.h"
 #include "ne2b_parallel.h"
 
 namespace ne2b {
@@ -794,13 +795,23 @@ uint64_t Engine::dev_bytes() const {
 
 uint32_t Engine::grid() const {
     uint32_t bps = shape_.blocks_per_sm;
-    const int occ = step_occupancy(int_ring_, adex_, multi_net, shape_.block, shape_.npt);
+    const int occ = step_occupancy(int_ring_, adex_, step_variant(), shape_.block, shape_.npt);
     if (bps == 0 || (int)bps > occ) bps = (uint32_t)(occ > 0 ? occ : 1);
     uint32_t g = (uint32_t)sm_count_ * bps;
     if (fixed_grid) return g;  // serving: graphs stay valid as nets come and go
     // never more blocks than tiles: idle blocks still cost launch time
     const uint32_t nt = n_tiles_ ? n_tiles_ : 1;
     return g < nt ? g : nt;
+}
+
+int Engine::step_variant() const {
+    if (multi_net) return kStepMulti;
+    if (stim_tiles_) return kStepSingle;
+    constexpr uint32_t kOptional =
+        kNetHasExt | kNetRecord | kNetWindows | kNetXsyn | kNetWatch | kNetGridWatch | kNetTraceF32;
+    for (const NetHost *h : nets_)
+        if (h && (h->dev.flags & kOptional)) return kStepSingle;
+    return kStepPlain;
 }
 
 // Resident plan: G co-resident blocks, each owning a contiguous range of
@@ -886,6 +897,8 @@ ne2b_status Engine::rebuild_tiles() {
             tiles.push_back(t);
         }
     }
+    stim_tiles_ = 0;
+    for (const Tile &t : tiles) stim_tiles_ += (t.flags & kTileHasStim) ? 1u : 0u;
     const uint32_t old_grid = grid();
     std::vector<uint32_t> block_tiles;
     resident_ = plan_resident(tiles, block_tiles);
@@ -1070,6 +1083,13 @@ ne2b_status Engine::launch_group(uint32_t steps) {
         launches_ += 2;
         return NE2B_OK;
     }
+    // the instance follows the nets' features (an external current or a
+    // watch can be switched on and off between launches)
+    const int var = step_variant();
+    if (var != graph_variant_) {
+        clear_graphs();
+        graph_variant_ = var;
+    }
     const uint32_t g = grid();
     if (steps == graph_steps) {
         auto it = graphs_.find(steps);
@@ -1078,7 +1098,7 @@ ne2b_status Engine::launch_group(uint32_t steps) {
             NE2B_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
             cudaError_t err = cudaSuccess;
             for (uint32_t k = 0; k < steps && err == cudaSuccess; ++k)
-                err = launch_step(int_ring_, adex_, multi_net, shape_.block, shape_.npt, d_eng_, k, g, stream_);
+                err = launch_step(int_ring_, adex_, var, shape_.block, shape_.npt, d_eng_, k, g, stream_);
             if (err == cudaSuccess) err = launch_advance(d_nets_, nets_cap_, steps, stream_);
             cudaError_t e2 = cudaStreamEndCapture(stream_, &gr);
             if (err != cudaSuccess) return cuda_error(err, "step launch during capture");
@@ -1093,7 +1113,7 @@ ne2b_status Engine::launch_group(uint32_t steps) {
         launches_ += steps + 1;
         return NE2B_OK;
     }
-    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, adex_, multi_net, shape_.block, shape_.npt, d_eng_, k, g, stream_));
+    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, adex_, var, shape_.block, shape_.npt, d_eng_, k, g, stream_));
     NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
     launches_ += steps + 1;
     return NE2B_OK;
@@ -1462,7 +1482,7 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
     for (int m : {(int)kModeStream, (int)kModeResident}) {
         if (saved_mode != kModeAuto && m != saved_mode) continue;  // a forced kernel keeps its mode
         for (uint32_t c = 0; c < count; ++c) {
-            const int occ = step_occupancy(int_ring_, adex_, multi_net, blocks[c], npts[c]);
+            const int occ = step_occupancy(int_ring_, adex_, step_variant(), blocks[c], npts[c]);
             for (int half = 0; half < 2; ++half) {
                 if (half && (m == kModeResident || occ < 2)) continue;
                 TileShape s;

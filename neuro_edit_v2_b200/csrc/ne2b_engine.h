@@ -232,6 +232,8 @@ class Engine {
     ne2b_status upload_ptab();
     ne2b_status upload_eng();
     uint32_t grid() const;
+    // the streaming kernel instance for the engine's nets (StepVariant)
+    int step_variant() const;
     bool plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &block_tiles);
     void clear_graphs();
 
@@ -258,6 +260,8 @@ class Engine {
     EngineDev *d_eng_ = nullptr;
     TileShape shape_;
     std::map<uint32_t, cudaGraphExec_t> graphs_;
+    int graph_variant_ = -1;   // the step instance the cached graphs launch
+    uint32_t stim_tiles_ = 0;  // tiles with stimulus entries
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     float last_ms_ = 0.0f;
     uint64_t launches_ = 0;  // kernels launched (graph nodes counted per replay)

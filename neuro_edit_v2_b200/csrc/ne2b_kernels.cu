@@ -100,13 +100,13 @@ bool pdl_enabled() { return g_pdl; }
     ((int_ring) ? ((adex) ? StepKind<true, true>::call : StepKind<true, false>::call) \
                 : ((adex) ? StepKind<false, true>::call : StepKind<false, false>::call))
 
-int step_occupancy(bool int_ring, bool adex, bool multi, uint32_t block, uint32_t npt) {
-    return NE2B_KIND(int_ring, adex, occupancy(block, npt, multi));
+int step_occupancy(bool int_ring, bool adex, int variant, uint32_t block, uint32_t npt) {
+    return NE2B_KIND(int_ring, adex, occupancy(block, npt, variant));
 }
 
-cudaError_t launch_step(bool int_ring, bool adex, bool multi, uint32_t block, uint32_t npt, const EngineDev *eng,
+cudaError_t launch_step(bool int_ring, bool adex, int variant, uint32_t block, uint32_t npt, const EngineDev *eng,
                         uint32_t k_step, uint32_t grid, cudaStream_t st) {
-    return NE2B_KIND(int_ring, adex, launch(block, npt, multi, eng, k_step, grid, st));
+    return NE2B_KIND(int_ring, adex, launch(block, npt, variant, eng, k_step, grid, st));
 }
 
 uint32_t resident_head(uint32_t block, uint32_t npt) {

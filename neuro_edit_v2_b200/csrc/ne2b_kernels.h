@@ -11,14 +11,15 @@ bool shape_supported(uint32_t block, uint32_t npt);
 void set_pdl(bool on);  // programmatic dependent launch of the streaming kernels (default on)
 void shape_list(uint32_t *blocks, uint32_t *npts, uint32_t *count);
 // `adex`: an AdEx row is present in some net (else the Izhikevich-only
-// instance of the step kernels runs).  `multi`: the engine holds many nets
-// (a batch or the server), whose streaming kernel stages several tiles'
-// records and net descriptors ahead.
-int step_occupancy(bool int_ring, bool adex, bool multi, uint32_t block, uint32_t npt);
+// instance of the step kernels runs).  `variant` (StepVariant): kStepMulti
+// when the engine holds many nets (a batch or the server), whose streaming
+// kernel stages several tiles' records and net descriptors ahead; kStepPlain
+// for one net without the optional features; else kStepSingle.
+int step_occupancy(bool int_ring, bool adex, int variant, uint32_t block, uint32_t npt);
 // k_step > 0 launches are programmatic (they follow step k_step - 1 of the
 // same launch group); k_step = 0 follows advance_kernel or host copies and
 // waits for them in full.
-cudaError_t launch_step(bool int_ring, bool adex, bool multi, uint32_t block, uint32_t npt, const EngineDev *eng,
+cudaError_t launch_step(bool int_ring, bool adex, int variant, uint32_t block, uint32_t npt, const EngineDev *eng,
                         uint32_t k_step, uint32_t grid, cudaStream_t st);
 uint32_t resident_head(uint32_t block, uint32_t npt);
 int resident_occupancy(bool int_ring, bool adex, uint32_t block, uint32_t npt, size_t smem);

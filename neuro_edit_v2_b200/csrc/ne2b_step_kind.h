@@ -30,11 +30,15 @@ __host__ __device__ constexpr uint32_t resident_head_bytes() {
     return (uint32_t)((smem_lists_words<BLOCK, NPT>() + 1) * 4 + 15) / 16 * 16;
 }
 
+// Streaming kernel instances: one net with any features, one net without the
+// optional ones (external current, stimulus, records, windows, custom-tau
+// synapses, f32 trace, watches), many nets (batches, the server).
+enum StepVariant : int { kStepSingle = 0, kStepMulti = 1, kStepPlain = 2 };
+
 template <bool INT, bool ADEX>
 struct StepKind {
-    // multi: the streaming kernel instance for engines of many nets
-    static int occupancy(uint32_t block, uint32_t npt, bool multi);
-    static cudaError_t launch(uint32_t block, uint32_t npt, bool multi, const EngineDev *eng, uint32_t k_step,
+    static int occupancy(uint32_t block, uint32_t npt, int variant);
+    static cudaError_t launch(uint32_t block, uint32_t npt, int variant, const EngineDev *eng, uint32_t k_step,
                               uint32_t grid, cudaStream_t st);
     static int resident_occupancy(uint32_t block, uint32_t npt, size_t smem);
     static cudaError_t launch_resident(uint32_t block, uint32_t npt, const EngineDev *eng, uint32_t k0,

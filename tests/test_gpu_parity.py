@@ -261,3 +261,66 @@ def test_synchronous_bursts_int_ring_bit_exact(mode, shape):
     assert first < 0, f"raster diverged at step {first}"
     assert g.spikes_total() > 5 * n  # ~390 Hz: every neuron fires every few steps
     assert_state_bits_equal(g, o)
+
+
+def plain_lockstep(onet, steps, chunk, mode=None, adex=False, toggles=None, **kw):
+    """Both backends without spike records (so the GPU runs the plain step
+    instance while nothing else is switched on): after every chunk the
+    spike totals and every state bit must agree.  `toggles[c]` (an external
+    amplitude, or None) is applied to every third neuron before chunk c."""
+    from helpers import configs
+
+    gc, oc = configs(True, 64, 1, **kw)
+    gc.record_spikes = oc.record_spikes = 0
+    g = nb.B200Sim(onet.flat(0.1), gc)
+    if mode is not None:
+        g.set_kernel_mode(mode)
+    o = O.OSim(onet, oc)
+    n = g.n()
+    for c in range(steps // chunk):
+        amp = toggles[c] if toggles and c < len(toggles) else None
+        if amp is not None:
+            set_ext(g, n, range(0, n, 3), amp)
+            set_ext(o, n, range(0, n, 3), amp)
+        g.run_steps(chunk)
+        o.run_steps(chunk)
+        assert g.spikes_total() == o.spikes_total(), f"spike totals differ after chunk {c}"
+        assert_state_bits_equal(g, o)
+    return g
+
+
+@pytest.mark.parametrize("n", [20_000, 100_000])
+def test_plain_instance_random_net_bit_exact(n):
+    """No records, no drive: the plain step instance, 768 steps in three
+    full launch groups, state and spike totals bit-exact."""
+    g = plain_lockstep(O.ONet.random_kout(n, 100, 2), 768, 256, mode=nb.KERNEL_STREAM, gauss_sd=1.0,
+                       synapse_tau_ms=5.0, noise_rate_hz=100.0, noise_kick_mv=20.0)
+    assert g.spikes_total() > 0
+
+
+def test_plain_instance_1m_net_bit_exact():
+    """The 1M-neuron workload (random K=100, ~1e8 synapses, Gaussian noise)
+    on the plain instance for one full launch group: the state that stays in
+    L2 between steps is every bit the oracle's."""
+    g = plain_lockstep(O.ONet.random_kout(1_000_000, 100, 1), 256, 256, mode=nb.KERNEL_STREAM, gauss_sd=1.0,
+                       synapse_tau_ms=5.0, noise_rate_hz=20.0, noise_kick_mv=20.0)
+    assert g.spikes_total() > 0
+
+
+def test_plain_instance_adex_bit_exact():
+    onet = O.ONet.random_kout(20_000, 100, 5, w_scale=0.7 * 281.0)
+    for i in range(onet.n):
+        onet.set_model(i, O.ADEX, ADEX_TONIC)
+    g = plain_lockstep(onet, 512, 256, mode=nb.KERNEL_STREAM, gauss_sd=1.0, synapse_tau_ms=5.0,
+                       noise_rate_hz=100.0, noise_kick_mv=20.0)
+    assert g.spikes_total() > 0
+
+
+def test_features_switched_on_and_off_between_launches_stay_bit_exact():
+    """An external current switched on, off and on again between launch
+    groups moves the engine between the plain and the full step instance
+    (its cached graphs included); state and spike totals stay bit-exact."""
+    g = plain_lockstep(O.ONet.random_kout(20_000, 100, 6), 256 * 6, 256, mode=nb.KERNEL_STREAM, gauss_sd=1.0,
+                       synapse_tau_ms=5.0, noise_rate_hz=50.0, noise_kick_mv=20.0,
+                       toggles=[None, 9.0, 0.0, None, 12.0, 0.0])
+    assert g.spikes_total() > 0

@@ -805,12 +805,13 @@ uint32_t Engine::grid() const {
 }
 
 int Engine::step_variant() const {
-    if (multi_net) return kStepMulti;
-    if (stim_tiles_) return kStepSingle;
-    constexpr uint32_t kOptional =
-        kNetHasExt | kNetRecord | kNetWindows | kNetXsyn | kNetWatch | kNetGridWatch | kNetTraceF32;
+    constexpr uint32_t kDebug = kNetRecord | kNetXsyn | kNetWatch | kNetGridWatch | kNetTraceF32;
+    constexpr uint32_t kInput = kNetHasExt | kNetWindows;
+    uint32_t used = 0;
     for (const NetHost *h : nets_)
-        if (h && (h->dev.flags & kOptional)) return kStepSingle;
+        if (h) used |= h->dev.flags;
+    if (multi_net) return (used & kDebug) ? kStepMulti : kStepMultiLean;
+    if (stim_tiles_ || (used & (kDebug | kInput))) return kStepSingle;
     return kStepPlain;
 }
 

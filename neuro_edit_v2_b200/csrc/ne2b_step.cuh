@@ -69,10 +69,11 @@ __device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, u
 // within the group (else t % rec_rows and (t + 1) / win_steps directly).  ADEX: the net holds AdEx rows (else the Izhikevich path is
 // the only one compiled into this instance).
 // `ptab` is the parameter table (a shared-memory copy when it is small).
-// PLAIN: no net of the engine uses an external current, a stimulus, record
-// rows, windows, custom-tau synapses, the f32 trace or watches, so their
-// code is compiled out (the engine launches this instance only then).
-template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool PLAIN = false>
+// LEAN: no net of the engine uses record rows, custom-tau synapses, the f32
+// trace or watches; NOIO: nor an external current, a stimulus or windows.
+// Their code is compiled out (the engine launches such an instance only
+// then).
+template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool LEAN = false, bool NOIO = false>
 __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
                                              const Tile &tile, uint64_t t, uint32_t tmod, uint32_t k, float *vs, float *us,
                                              float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
@@ -90,10 +91,10 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     const uint64_t nbase = noise_base_step(t, nd.seed);
     const uint32_t tlast = nd.trace_last;
     uint32_t *__restrict__ ringw = (uint32_t *)nd.ring;
-    const bool has_ext = !PLAIN && (flags & kNetHasExt);
-    const bool has_stim = !PLAIN && (tile.flags & kTileHasStim);
-    const bool windows = !PLAIN && (flags & kNetWindows);
-    const bool xsyn_on = !PLAIN && (flags & kNetXsyn);
+    const bool has_ext = !NOIO && (flags & kNetHasExt);
+    const bool has_stim = !NOIO && (tile.flags & kTileHasStim);
+    const bool windows = !NOIO && (flags & kNetWindows);
+    const bool xsyn_on = !LEAN && (flags & kNetXsyn);
     bool win_end = false;
     uint32_t widx = 0;
     if (windows) {
@@ -220,7 +221,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         // the table's last entry, 0 or the subnormal fixed point)
         const uint32_t k0 = tk[q];
         uint32_t k = sp ? 0u : (k0 == kTraceZero ? k0 : (k0 < tlast ? k0 + 1u : tlast));
-        if (!PLAIN && (flags & kNetTraceF32)) {  // a readout tau too long for the step table: the f32 trace
+        if (!LEAN && (flags & kNetTraceF32)) {  // a readout tau too long for the step table: the f32 trace
             const float tr = nd.trace_f[i];
             const float tn = sp ? 1.0f : __fmul_rn(tr, nd.decay_t);  // cpu.rs:252-260
             if (__float_as_uint(tn) != __float_as_uint(tr)) nd.trace_f[i] = tn;
@@ -237,7 +238,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             rlo[q] = rowptr[i];
             rhi[q] = rowptr[i + 1];
             nd.pn_total[i] += 1ull;
-            if (!PLAIN && (flags & kNetGridWatch)) {  // cpu.rs:293-304
+            if (!LEAN && (flags & kNetGridWatch)) {  // cpu.rs:293-304
                 const uint32_t t32 = t < 0xFFFFFFFEull ? (uint32_t)t : 0xFFFFFFFEu;
                 for (uint32_t g = 0; g < nd.gw_n; ++g) {
                     const int32_t k = nd.gw_map[(size_t)g * n_pad + i];
@@ -245,7 +246,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
                 }
             }
         }
-        if (!PLAIN && (flags & kNetWatch)) {  // state after the step, cpu.rs:311-324
+        if (!LEAN && (flags & kNetWatch)) {  // state after the step, cpu.rs:311-324
             const uint32_t w = nd.watch_idx[i];
             if (w != kNoWatch) {
                 const size_t pos = (size_t)(t & (kWatchCap - 1u));
@@ -266,7 +267,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     }
 
     // ---- spike record: one ballot word per warp and q
-    if (!PLAIN && (flags & kNetRecord)) {
+    if (!LEAN && (flags & kNetRecord)) {
         uint32_t row;
         if constexpr (PHASES) {
             row = nd.rphase + k;
@@ -466,9 +467,10 @@ __device__ __forceinline__ void stage_net(const EngineDev *__restrict__ eng, uin
 // descriptor only when the net changes, which it never does.
 constexpr uint32_t kStageTiles = 16;
 
+// PLAIN: the lean instance; single-net, it also drops the input features
+// (LEAN and NOIO), many-net only the others (LEAN).
 template <bool INT, int BLOCK, int NPT, bool ADEX, bool MULTI, bool PLAIN>
 __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
-    static_assert(!(MULTI && PLAIN), "the plain instance is single-net");
     pdl_trigger();
     constexpr uint32_t kNetWords = sizeof(NetDev) / 16;
     __shared__ uint32_t s_lists[smem_lists_words<BLOCK, NPT>()];
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
             const uint64_t t = s_nd.t + k_step;
             uint32_t tmod = s_nd.tmod + k_step;
             if (tmod >= s_nd.D) tmod %= s_nd.D;
-            process_tile<INT, BLOCK, NPT, false, ADEX, false, PLAIN>(eng, ptab, s_nd, tile, t, tmod, k_step,
+            process_tile<INT, BLOCK, NPT, false, ADEX, false, PLAIN, PLAIN>(eng, ptab, s_nd, tile, t, tmod, k_step,
                                                              s_nd.v + tile.start, s_nd.u + tile.start,
                                                              s_nd.s + tile.start, s_nd.tk + tile.start,
                                                              s_nd.pidx + tile.start, sl);
@@ -542,7 +544,7 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
             const uint64_t t = s_nd.t + k_step;
             uint32_t tmod = s_nd.tmod + k_step;
             if (tmod >= s_nd.D) tmod %= s_nd.D;
-            process_tile<INT, BLOCK, NPT, false, ADEX, true>(eng, ptab, s_nd, tile, t, tmod, k_step,
+            process_tile<INT, BLOCK, NPT, false, ADEX, true, PLAIN>(eng, ptab, s_nd, tile, t, tmod, k_step,
                                                             s_nd.v + tile.start, s_nd.u + tile.start,
                                                             s_nd.s + tile.start, s_nd.tk + tile.start,
                                                             s_nd.pidx + tile.start, sl);
@@ -694,6 +696,8 @@ int StepKind<INT, ADEX>::occupancy(uint32_t block, uint32_t npt, int variant) {
         int b = 0;                                                                                              \
         if (variant == kStepMulti)                                                                              \
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX, true, false>, B, 0);  \
+        else if (variant == kStepMultiLean)                                                                     \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX, true, true>, B, 0);   \
         else if (variant == kStepPlain)                                                                         \
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX, false, true>, B, 0);  \
         else                                                                                                    \
@@ -712,6 +716,8 @@ cudaError_t StepKind<INT, ADEX>::launch(uint32_t block, uint32_t npt, int varian
     if (block == B && npt == P)                                                                                   \
         return variant == kStepMulti                                                                              \
                    ? launch_pdl(step_kernel<INT, B, P, ADEX, true, false>, grid, B, st, k_step > 0, eng, k_step)  \
+               : variant == kStepMultiLean                                                                        \
+                   ? launch_pdl(step_kernel<INT, B, P, ADEX, true, true>, grid, B, st, k_step > 0, eng, k_step)   \
                : variant == kStepPlain                                                                            \
                    ? launch_pdl(step_kernel<INT, B, P, ADEX, false, true>, grid, B, st, k_step > 0, eng, k_step)  \
                    : launch_pdl(step_kernel<INT, B, P, ADEX, false, false>, grid, B, st, k_step > 0, eng, k_step);

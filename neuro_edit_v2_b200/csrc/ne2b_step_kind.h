@@ -32,8 +32,9 @@ __host__ __device__ constexpr uint32_t resident_head_bytes() {
 
 // Streaming kernel instances: one net with any features, one net without the
 // optional ones (external current, stimulus, records, windows, custom-tau
-// synapses, f32 trace, watches), many nets (batches, the server).
-enum StepVariant : int { kStepSingle = 0, kStepMulti = 1, kStepPlain = 2 };
+// synapses, f32 trace, watches), many nets (batches, the server), and many
+// nets without records, custom-tau synapses, f32 trace or watches.
+enum StepVariant : int { kStepSingle = 0, kStepMulti = 1, kStepPlain = 2, kStepMultiLean = 3 };
 
 template <bool INT, bool ADEX>
 struct StepKind {

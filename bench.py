@@ -43,7 +43,12 @@ SEED = 1
 B_NEURON = 60  # algorithmic bytes per Izhikevich neuron-update
 B_SPIKE = 24   # per spike
 B_EVENT = 17   # per delivered synaptic event
-ACTIVE_KICK_HZ = 100.0  # companion regime: Poisson kicks (sim/src/state.rs:15-22)
+ACTIVE_KICK_HZ = 100.0  # companion regime: Poisson kicks (sim/src/state.rs:15-22), ~22 Hz firing
+ADEX_ACTIVE_KICK_HZ = 60.0  # the AdEx variant's kicks for ~20 Hz firing
+LIQUID_KICK_HZ = 30.0  # the batched liquids' active variant: ~20 Hz firing
+L2_NOTE = ("L2 scrubbed (256 MB write) before each timed trial; a trial is 10,000 dependent steps whose "
+           "per-step working set (state ~7 MB + one ring slot) stays in L2 from step to step, as in any run of "
+           "this net; the CSR (~90 MB) and ring (~67 MB) together exceed L2")
 
 
 def load_peaks():
@@ -56,11 +61,21 @@ def load_peaks():
 
 
 def load_traffic():
+    """DRAM bytes per launch of the headline's step kernel from a stored ncu
+    capture (profiles/step_kernel_traffic.json): not measured in this run."""
     p = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f)
     return None
+
+
+def headline_config(ring_depth: int, ws: int) -> dict:
+    """The workload both arms measure (identical dict in both lines)."""
+    return {"workload": "100k izh random K=100, 1000 ms trial at dt 0.1 ms from reset, Gaussian noise sd 1, "
+                        "tau_syn 5 ms, int32 ring",
+            "neurons": N, "synapses": N * K_OUT, "trial_steps": TRIAL_STEPS, "ring_depth": ring_depth,
+            "l2": L2_NOTE, "parallelism": f"replicas x{ws}"}
 
 
 class Clocks:
@@ -424,10 +439,16 @@ def run_ours(args):
     extra = {}
     if not args.no_extras and ws == 1:
         peak_v, _ = load_peaks()
-        for name, fn in (("c1m_izh", lambda: bench_1m(nb, torch, scrub, nb.MODEL_IZH, 2, 3, peak_v)),
-                         ("c1m_adex", lambda: bench_1m(nb, torch, scrub, nb.MODEL_ADEX, 2, 3, peak_v)),
-                         ("batched_256", lambda: bench_batched(nb, torch, scrub, 2, 3)),
-                         ("serving", lambda: bench_serving(nb, args.serving_requests, args.admission_threads))):
+        jobs = (("c1m_izh", lambda: bench_1m(nb, torch, scrub, nb.MODEL_IZH, 2, 3, peak_v)),
+                ("c1m_adex", lambda: bench_1m(nb, torch, scrub, nb.MODEL_ADEX, 2, 3, peak_v)),
+                ("fp32_ring_100k", lambda: bench_fp32_ring(nb, torch, scrub, net, args.steps, peak_v)),
+                ("batched_256", lambda: bench_batched(nb, torch, scrub, 2, 3)),
+                ("batched_256_active", lambda: bench_batched(nb, torch, scrub, 2, 3, kick_hz=LIQUID_KICK_HZ)),
+                ("serving", lambda: bench_serving(nb, args.serving_requests, args.admission_threads)))
+        only = set(args.extras.split(",")) if args.extras else None
+        for name, fn in jobs:
+            if only is not None and name not in only:
+                continue
             try:
                 extra[name] = fn()
             except Exception as e:  # report, never hide
@@ -450,11 +471,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32 state, int32 fixed-point ring",
         "data": "synthetic: seeded generator of the 100k configuration (random K=100, distance delays)",
-        "config": {"workload": "100k izh random K=100, 1000 ms trial at dt 0.1 ms, Gaussian noise sd 1, "
-                               "tau_syn 5 ms, int32 ring",
-                   "neurons": N, "synapses": N * K_OUT, "trial_steps": TRIAL_STEPS, "ring_depth": sim.ring_depth(),
-                   "l2": "scrubbed (256 MB write) between timed steps; inputs ~130 MB > L2",
-                   "parallelism": f"replicas x{ws}"},
+        "config": headline_config(sim.ring_depth(), ws),
         "synaptic_events_per_s": events / (total_ms / 1000.0) * ws,
         "firing_rate_hz": spikes / (N * args.steps * TRIAL_STEPS * 1e-4),
         "active_regime": {
@@ -471,6 +488,7 @@ def run_ours(args):
                      "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg_bytes, "launch_us": launch_ms * 1000.0,
                      "traffic": (tr or {}).get("bytes_per_launch"),
+                     "traffic_kind": "stored ncu capture of this kernel and workload, not measured in this run",
                      "traffic_source": (tr or {}).get("source")},
         "e2e": {"value": e2e_val, "unit": "neuron-updates/s", "h2d_bytes_per_step": 4 * N,
                 "d2h_bytes_per_step": 4 * N + 8},
@@ -490,7 +508,10 @@ def run_ours(args):
 # ----------------------------------------------------------------- extras
 def bench_1m(nb, torch, scrub, model: int, steps: int, warmup: int, peak: float):
     """1,000,000 neurons x K=100 (~100M synapses), 500 ms trials, izh or AdEx
-    (AdEx weights x C = 281 pF so a weight moves v by the same mV)."""
+    (AdEx weights x C = 281 pF so a weight moves v by the same mV): the
+    configuration as stated (Gaussian noise sd 1, silent), then the same sim
+    in an active regime (Poisson kicks x 20 mV added: ~20 Hz, ~2e5 synaptic
+    events per step into the HBM-resident ring)."""
     n, trial = 1_000_000, 5000
     adex = model == nb.MODEL_ADEX
     net = nb.random_kout(n, K_OUT, SEED, w_scale=0.7 * (281.0 if adex else 1.0))
@@ -498,20 +519,52 @@ def bench_1m(nb, torch, scrub, model: int, steps: int, warmup: int, peak: float)
         nb.to_adex(net)
     sim = nb.B200Sim(net, nb.default_config(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0, seed=SEED))
     del net
-    tiling = sim.autotune(128)
-    ms, spikes, launches = timed_trials(sim, steps, warmup, trial, 1, torch, scrub)
-    per_launch_s = ms / 1000.0 / (trial * steps)
     b_neuron = 84 if adex else B_NEURON
-    alg = b_neuron * n + (B_SPIKE * spikes + B_EVENT * spikes * K_OUT) / (trial * steps)
-    achieved = alg / per_launch_s / 1e9
+
+    def measure(kick_hz):
+        sim.set_noise(kick_hz, 20.0 if kick_hz else 0.0)
+        tiling = sim.autotune(128)
+        ms, spikes, launches = timed_trials(sim, steps, warmup, trial, 1, torch, scrub)
+        per_launch_s = ms / 1000.0 / (trial * steps)
+        events = spikes * K_OUT
+        alg = b_neuron * n + (B_SPIKE * spikes + B_EVENT * events) / (trial * steps)
+        achieved = alg / per_launch_s / 1e9
+        return {"kick_hz": kick_hz, "neuron_updates_per_s": n * trial * steps / (ms / 1000.0),
+                "synaptic_events_per_s": events / (ms / 1000.0),
+                "firing_rate_hz": spikes / (n * steps * trial * 1e-4), "ms_per_trial": ms / steps,
+                "events_per_step": events / (trial * steps),
+                "roofline": {"achieved_gbs": achieved, "frac": achieved / peak, "alg_bytes_per_launch": alg,
+                             "launch_us": per_launch_s * 1e6, "bytes_per_neuron": b_neuron,
+                             "target_frac": 0.6},
+                "gpu_launches": launches, "tiling": tiling}
+
     out = {"neurons": n, "synapses": n * K_OUT, "trial_steps": trial, "ring_depth": sim.ring_depth(),
-           "neuron_updates_per_s": n * trial * steps / (ms / 1000.0),
-           "synaptic_events_per_s": spikes * K_OUT / (ms / 1000.0),
-           "firing_rate_hz": spikes / (n * steps * trial * 1e-4), "ms_per_trial": ms / steps,
-           "roofline": {"achieved_gbs": achieved, "frac": achieved / peak, "alg_bytes_per_launch": alg,
-                        "launch_us": per_launch_s * 1e6, "bytes_per_neuron": b_neuron},
-           "gpu_launches": launches, "dev_mem_bytes": sim.dev_mem_bytes(), "tiling": tiling}
+           "dev_mem_bytes": sim.dev_mem_bytes()}
+    out["quiet"] = measure(0.0)
+    out["active"] = measure(ADEX_ACTIVE_KICK_HZ if adex else ACTIVE_KICK_HZ)
     sim.close()
+    return out
+
+
+def bench_fp32_ring(nb, torch, scrub, net, steps: int, peak: float):
+    """The 100k configuration with the f32 ring (float atomics), quiet as
+    stated and in the active regime: the fp32-ring mode of the benchmark
+    configurations, beside the int32 headline."""
+    out = {}
+    for name, kick in (("quiet", 0.0), ("active", ACTIVE_KICK_HZ)):
+        sim = nb.B200Sim(net, nb.default_config(int_weights=0, gauss_sd=1.0, synapse_tau_ms=5.0,
+                                                noise_rate_hz=kick, noise_kick_mv=20.0, seed=SEED))
+        tiling = sim.autotune(256)
+        k = max(1, steps // 2) if kick else steps
+        ms, spikes, launches = timed_trials(sim, k, 3, TRIAL_STEPS, 1, torch, scrub)
+        events = spikes * K_OUT
+        alg = B_NEURON * N + (B_SPIKE * spikes + B_EVENT * events) / (TRIAL_STEPS * k)
+        step_s = ms / 1000.0 / (TRIAL_STEPS * k)
+        out[name] = {"kick_hz": kick, "neuron_updates_per_s": N * TRIAL_STEPS * k / (ms / 1000.0),
+                     "synaptic_events_per_s": events / (ms / 1000.0),
+                     "firing_rate_hz": spikes / (N * k * TRIAL_STEPS * 1e-4), "ms_per_trial": ms / k,
+                     "roofline_frac": alg / step_s / 1e9 / peak, "gpu_launches": launches, "tiling": tiling}
+        sim.close()
     return out
 
 
@@ -538,13 +591,23 @@ def batch_trials(b, torch, scrub, steps: int, warmup: int, trial: int):
     return total
 
 
-def bench_batched(nb, torch, scrub, steps: int, warmup: int, serial_sample: int = 32):
+_LIQUIDS = None
+
+
+def bench_batched(nb, torch, scrub, steps: int, warmup: int, serial_sample: int = 32, kick_hz: float = 0.0):
+    """256 liquids with their input streams, one batch, 1000 ms trials, against
+    the same kernels one net at a time on a sample of 32 nets spread over the
+    size range; `kick_hz` > 0 adds Poisson kicks x 20 mV (the active variant)."""
+    global _LIQUIDS
     from neuro_edit_v2_b200 import workloads as W
 
-    nets, inputs = W.batched_liquids(256)
+    if _LIQUIDS is None:
+        _LIQUIDS = W.batched_liquids(256)
+    nets, inputs = _LIQUIDS
     trial = TRIAL_STEPS
     wins = trial // W.WINDOW_STEPS
-    cfgs = [nb.default_config(int_weights=1, window_steps=W.WINDOW_STEPS, max_windows=wins, seed=k)
+    cfgs = [nb.default_config(int_weights=1, window_steps=W.WINDOW_STEPS, max_windows=wins, seed=k,
+                              noise_rate_hz=kick_hz, noise_kick_mv=20.0 if kick_hz else 0.0)
             for k in range(len(nets))]
     b = nb.Batch(nets, cfgs)
     for k, x in enumerate(inputs):
@@ -562,15 +625,19 @@ def bench_batched(nb, torch, scrub, steps: int, warmup: int, serial_sample: int 
             events += int((c * deg).sum())
     launches = b.kernel_launches()
     b.close()
-    # the same kernels, one network at a time, on a sample of the set
+    # the same kernels, one network at a time, on a sample of the set: every
+    # 8th net, so the sample spans the size range (the nets are in a seeded
+    # random size order); its trials/s is scaled to the whole set by neurons
+    sample = list(range(0, len(nets), max(1, len(nets) // serial_sample)))[:serial_sample]
     ser_ms = 0.0
-    for k in range(serial_sample):
+    for k in sample:
         one = nb.Batch([nets[k]], [cfgs[k]])
         one.set_input_matrix(0, inputs[k])
         ser_ms += batch_trials(one, torch, scrub, 1, 1, trial)
         one.close()
     batched_tps = len(nets) * steps / (total_ms / 1000.0)
-    serial_tps = serial_sample / (ser_ms / 1000.0)
+    serial_tps = len(sample) / (ser_ms / 1000.0)
+    sample_neurons = sum(nets[k].n for k in sample) / len(sample)
     # the same byte contract as the single net (all liquids are izh): the
     # per-step bytes over the per-step time of the timed trials
     peak, peak_kind = load_peaks()
@@ -587,7 +654,8 @@ def bench_batched(nb, torch, scrub, steps: int, warmup: int, serial_sample: int 
             "neuron_updates_per_s": neurons * trial * steps / (total_ms / 1000.0),
             "synaptic_events_per_s": events / (total_ms / 1000.0 / steps),
             "firing_rate_hz": spikes / (neurons * trial * 1e-4),
-            "serial_trials_per_s": serial_tps, "serial_sample": serial_sample,
+            "kick_hz": kick_hz, "serial_trials_per_s": serial_tps, "serial_sample": len(sample),
+            "serial_sample_mean_neurons": sample_neurons, "batch_mean_neurons": neurons / len(nets),
             "batched_vs_serial": batched_tps / serial_tps}
 
 
@@ -720,26 +788,29 @@ def cpu_model() -> str:
     return "unknown"
 
 
-REF_SAMPLE = 500  # reference arm: steps per bench step (50 ms of the 1000 ms trial)
+REF_SAMPLE = 500  # reference arm: steps of the trial per bench step (its first 50 ms, from reset)
 REF_MAX_COPIES = 64  # one 100k oracle net (~130 MB) per copy
 
 
 def _reference_copy(steps: int, warmup: int, barrier, out):
-    """One host core's copy of the trial: the oracle (the single-threaded
-    reference CpuSim restated in C) on the 100k net; the timed region starts
-    together with the other copies."""
+    """One host core's copy of the workload: the oracle (the single-threaded
+    reference CpuSim restated in C) on the 100k net, each bench step a reset
+    followed by the first REF_SAMPLE steps of the trial; the timed region
+    starts together with the other copies."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as O
 
     onet = O.ONet.random_kout(N, K_OUT, SEED)
     sim = O.OSim(onet, O.cfg(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0, seed=SEED))
     for _ in range(warmup):
+        sim.reset_state()
         sim.run_steps(REF_SAMPLE // 5)
     barrier.wait()
     t0 = time.perf_counter()
     for _ in range(steps):
+        sim.reset_state()
         sim.run_steps(REF_SAMPLE)
-    out.put(time.perf_counter() - t0)
+    out.put((time.perf_counter() - t0, sim.ring_depth()))
 
 
 def run_reference(args):
@@ -764,9 +835,10 @@ def run_reference(args):
     procs = [ctx.Process(target=_reference_copy, args=(args.steps, args.warmup, barrier, out)) for _ in range(copies)]
     for p in procs:
         p.start()
-    times = [out.get() for _ in range(copies)]
+    res = [out.get() for _ in range(copies)]
     for p in procs:
         p.join()
+    times = [r[0] for r in res]
     dt = max(times)
     sample = REF_SAMPLE
     value = copies * N * sample * args.steps / dt
@@ -777,13 +849,13 @@ def run_reference(args):
         "ms_per_step": dt * 1000.0 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 state, int32 fixed-point ring",
         "data": "synthetic: seeded generator of the 100k configuration (random K=100, distance delays)",
-        "config": {"workload": "100k izh random K=100, 1000 ms trial at dt 0.1 ms, Gaussian noise sd 1, "
-                               "tau_syn 5 ms, int32 ring", "neurons": N, "synapses": N * K_OUT},
+        "config": headline_config(res[0][1], ws),
         "cpu_baseline": {"value": value, "unit": "neuron-updates/s", "cores": copies, "kind": "port",
-                         "sample": f"{sample} steps of the 100k trial per bench step in each of {copies} "
-                                   f"independent copies, one per host core (of {cores}; at most "
-                                   f"{REF_MAX_COPIES}), timed together; the C restatement of the "
-                                   "single-threaded reference CpuSim (the Rust reference cannot be built here)",
+                         "sample": f"each bench step: reset, then the first {sample} of the trial's "
+                                   f"{TRIAL_STEPS} steps, in each of {copies} independent copies, one per host "
+                                   f"core (of {cores}; at most {REF_MAX_COPIES}), timed together; the C "
+                                   "restatement of the single-threaded reference CpuSim (the Rust reference "
+                                   "cannot be built here)",
                          "per_copy_s": times, "cpu": cpu_model()},
         "e2e": {"value": value, "unit": "neuron-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -797,6 +869,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the 1M, batched and serving measurements")
+    ap.add_argument("--extras", default="",
+                    help="comma-separated subset of the extras (c1m_izh, c1m_adex, fp32_ring_100k, batched_256, "
+                         "batched_256_active, serving)")
     ap.add_argument("--serving-requests", type=int, default=200)
     ap.add_argument("--admission-threads", type=int, default=4,
                     help="serving: host threads that build admitted requests while the device steps")
@@ -816,15 +891,7 @@ def main():
                     help="--profile the first N liquids of the batched workload stepped as one batch")
     ap.add_argument("--no-inputs", action="store_true",
                     help="with --batched-liquids: build the liquids without input streams")
-    ap.add_argument("--floors", action="store_true",
-                    help="print the measured launch / streaming / atomic floors (neuro_edit_v2_b200/_lib/probe_floors)")
     args = ap.parse_args()
-    if args.floors:
-        sys.path.insert(0, ROOT)
-        from neuro_edit_v2_b200 import build as B
-
-        B.build()
-        sys.exit(subprocess.run([B.PROBE]).returncode)
     if args.warmup < 3:
         args.warmup = 3
     if args.profile:

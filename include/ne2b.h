@@ -3,8 +3,7 @@
  *
  * This is the drop-in boundary for the reference's `sim::Backend` trait
  * (sim/src/lib.rs:119-184).  A Rust `impl Backend for B200Sim` binds these
- * entry points one-to-one (the binding is written out in INTEGRATION.md);
- * every other caller (the Python mirror in neuro_edit_v2_b200, the batch
+ * entry points one-to-one; every other caller (the Python mirror in neuro_edit_v2_b200, the batch
  * runner, the serving loop) uses the same symbols.
  *
  * Conventions
@@ -147,8 +146,10 @@ ne2b_status ne2b_spike_row(ne2b_sim *sim, uint32_t back, uint64_t *out);
  * not stall on cudaMalloc/cudaFree, which synchronise the device.  Same
  * window rules and results as ne2b_spike_counts; the scratch is a 4 MiB
  * array compiled into the library (held by every GPU that loads it until
- * exit), so n above 1,048,576 neurons is NE2B_EINVAL.  Calls share that
- * array: calls whose work overlaps on the GPU race. */
+ * exit), so a sim of more than 1,048,576 neurons gets NE2B_EINVAL whenever
+ * its counts need the device (recording on and t > 0).  The array's device
+ * address is looked up when the first sim on a device is created.  Calls
+ * share that array: calls whose work overlaps on the GPU race. */
 ne2b_status ne2b_spike_counts_noalloc(ne2b_sim *sim, uint64_t rows, uint32_t *out);
 ne2b_status ne2b_spikes_total(ne2b_sim *sim, uint64_t *total);             /* Backend::spikes_total */
 ne2b_status ne2b_mean_rate_hz(ne2b_sim *sim, double *hz);                  /* Backend::mean_rate_hz */

@@ -4,9 +4,7 @@ Compiles the CUDA kernels ahead of time for sm_100a only
 (`-gencode arch=compute_100a,code=sm_100a`) with `-fmad=false`, so no float
 operation of the step is contracted into an FMA, and the host sources with
 `-ffp-contract=off`.  The library is built in-tree so it travels with the
-repository; nothing is installed.  `_lib/probe_floors` (csrc/probe_floors.cu)
-is a standalone program that measures the launch, streaming and atomic floors
-that bound the step kernel (`python bench.py --floors`).
+repository; nothing is installed.
 """
 from __future__ import annotations
 
@@ -49,9 +47,6 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-PROBE = os.path.join(OUT_DIR, "probe_floors")
-
-
 def _run_all(cmds, verbose: bool) -> None:
     """Run the compiler commands concurrently; raise on the first failure."""
     procs = []
@@ -65,32 +60,25 @@ def _run_all(cmds, verbose: bool) -> None:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    probe_src = os.path.join(CSRC, "probe_floors.cu")
-    probe_stale = not os.path.exists(PROBE) or os.path.getmtime(probe_src) > os.path.getmtime(PROBE)
-    if not force and not _stale() and not probe_stale:
+    if not force and not _stale():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     cmds = []
     objs = []
-    if force or _stale():
-        for src in SOURCES:
-            obj = os.path.join(OUT_DIR, src + ".o")
-            cmds.append([nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj])
-            objs.append(obj)
-    if force or probe_stale:
-        cmds.append([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", probe_src, "-o",
-                     PROBE])
+    for src in SOURCES:
+        obj = os.path.join(OUT_DIR, src + ".o")
+        cmds.append([nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj])
+        objs.append(obj)
     _run_all(cmds, verbose)
-    if objs:
-        tmp = LIB + ".tmp"
-        cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp, "-lcudart",
-               "-Xcompiler", "-pthread"]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        os.replace(tmp, LIB)
-        for o in objs:
-            os.remove(o)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp, "-lcudart",
+           "-Xcompiler", "-pthread"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    for o in objs:
+        os.remove(o)
     return LIB
 
 

@@ -114,12 +114,12 @@ ne2b_status Engine::init(int device, bool int_ring, uint32_t max_nets) {
     device_ = device;
     int_ring_ = int_ring;
     NE2B_CUDA(cudaSetDevice(device));
-    NE2B_TRY(noalloc_setup(device));  // scratch address of ne2b_spike_counts_noalloc
     cudaDeviceProp prop;
     NE2B_CUDA(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10)
         return set_error(NE2B_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a", device,
                          prop.major, prop.minor);
+    noalloc_setup(device);  // scratch address of ne2b_spike_counts_noalloc; a failure only disables that entry point
     sm_count_ = prop.multiProcessorCount;
     NE2B_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     stager_.set_stream(stream_);

@@ -215,6 +215,7 @@ class Engine {
     int device() const { return device_; }
     bool int_ring() const { return int_ring_; }
     uint64_t launches() const { return launches_; }
+    void count_launches(uint64_t k) { launches_ += k; }  // kernels launched by entry points outside the engine
     bool resident() const { return resident_; }
     int mode() const { return mode_; }
     ne2b_status set_mode(int m);

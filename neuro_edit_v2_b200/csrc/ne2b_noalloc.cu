@@ -13,7 +13,9 @@
 // loads this library, until the process exits.  Its device address is looked
 // up once per device, with that device current, when the first engine on the
 // device is created (noalloc_setup, called from Engine::init), so the entry
-// point itself does no set-up.  Every call shares the one array and leaves
+// point itself does no set-up.  A failed look-up (or a device ordinal past
+// kNoAllocMaxDevices) leaves the address unset: engine creation goes on, and
+// only this entry point reports the missing scratch.  Every call shares the one array and leaves
 // the last call's counts in it; each call overwrites entries [0, n) before
 // reading them, so nothing has to start at zero.  Calls whose kernels overlap
 // on the GPU (two host threads, two sims on one device) race on the array.
@@ -39,14 +41,18 @@ static __device__ __align__(256) uint32_t g_noalloc_counts[kNoAllocMaxNeurons];
 static uint32_t *g_noalloc_ptr[kNoAllocMaxDevices] = {};
 static std::mutex g_noalloc_mu;
 
+// Returns NE2B_OK or the look-up's error; the caller may ignore it, since a
+// device without the address only refuses ne2b_spike_counts_noalloc.
 ne2b_status noalloc_setup(int device) {
-    if (device < 0 || device >= kNoAllocMaxDevices)
-        return set_error(NE2B_UNSUPPORTED, "device ordinal %d beyond %d", device, kNoAllocMaxDevices);
+    if (device < 0 || device >= kNoAllocMaxDevices) return NE2B_OK;  // entry point unavailable there
     std::lock_guard<std::mutex> g(g_noalloc_mu);
     if (g_noalloc_ptr[device]) return NE2B_OK;
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_counts);
-    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(spike-count scratch)");
+    if (e != cudaSuccess) {
+        cudaGetLastError();  // clear the (non-sticky) error so that the engine's next runtime call does not return it
+        return cuda_error(e, "cudaGetSymbolAddress(spike-count scratch)");
+    }
     g_noalloc_ptr[device] = (uint32_t *)p;
     return NE2B_OK;
 }
@@ -80,11 +86,10 @@ extern "C" ne2b_status ne2b_spike_counts_noalloc(ne2b_sim *sim, uint64_t rows, u
     NetHost *h = sim->eng.net(sim->slot);
     if (!h) return set_error(NE2B_EINVAL, "sim has no network");
     const uint32_t n = h->n;
-    if (n > kNoAllocMaxNeurons)
-        return set_error(NE2B_EINVAL, "spike_counts_noalloc: %u neurons exceed the %u-neuron scratch array", n,
-                         kNoAllocMaxNeurons);
     if (!out && n) return set_error(NE2B_EINVAL, "null out");
-    // window rules of Backend::spike_counts (sim/src/cpu.rs:424-458)
+    // window rules of Backend::spike_counts (sim/src/cpu.rs:424-458), in the
+    // order Engine::spike_counts applies them: no recording or no step yet
+    // gives zeros at any size
     if (!h->dev.rec_rows || h->t == 0) {
         if (n) memset(out, 0, sizeof(uint32_t) * n);
         return NE2B_OK;
@@ -93,6 +98,9 @@ extern "C" ne2b_status ne2b_spike_counts_noalloc(ne2b_sim *sim, uint64_t rows, u
         return set_error(NE2B_EWINDOW, "spike_counts window %llu exceeds the recorded %u steps",
                          (unsigned long long)rows, h->dev.rec_rows);
     if (n == 0) return NE2B_OK;
+    if (n > kNoAllocMaxNeurons)
+        return set_error(NE2B_EINVAL, "spike_counts_noalloc: %u neurons exceed the %u-neuron scratch array", n,
+                         kNoAllocMaxNeurons);
     const int device = sim->eng.device();
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
@@ -104,8 +112,8 @@ extern "C" ne2b_status ne2b_spike_counts_noalloc(ne2b_sim *sim, uint64_t rows, u
     else noalloc_window_count_kernel<<<grid, 256, 0, st>>>(h->dev.rec_bits, h->dev.rec_rows, h->n_pad, n, h->t,
                                                               (uint32_t)rows, scratch);
     e = cudaGetLastError();
+    sim->eng.count_launches(1);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, scratch, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_error(e, "spike_counts_noalloc");
-    return sim->eng.check_err();
+    return cuda_error(e, "spike_counts_noalloc");
 }

@@ -85,3 +85,51 @@ def assert_state_bits_equal(g: nb.B200Sim, o: O.OSim):
         assert bad.size == 0, f"{name}: {bad.size} neurons differ, first {bad[:5]}"
     assert g.spikes_total() == o.spikes_total()
     assert np.array_equal(g.spike_counts(2**63), o.spike_counts(2**63))
+
+
+def lockstep_many(onet: O.ONet, steps: int, variants, int_weights: bool = True, chunk: int = 100,
+                  exp_mode: int = 1, drive=None, **cfg_kw):
+    """One oracle run against several GPU sims of the same net and config.
+
+    `variants` is a list of dicts: {"mode": kernel mode or None, "records":
+    True/False}.  A sim with records off runs the step instance without the
+    optional features (when nothing else is switched on); its spike totals
+    and every state bit are compared after each chunk.  A sim with records on
+    has every raster row compared as well.  Stops at the first difference;
+    returns (gpu sims, oracle, first divergent step or -1 per sim)."""
+    flat = onet.flat(cfg_kw.get("dt_ms", 0.1))
+    _, oc = configs(int_weights, chunk, exp_mode, **cfg_kw)
+    o = O.OSim(onet, oc)
+    gs = []
+    for v in variants:
+        gc, _ = configs(int_weights, chunk, exp_mode, **cfg_kw)
+        if not v.get("records", True):
+            gc.record_spikes = 0
+        g = nb.B200Sim(flat, gc)
+        if v.get("mode") is not None:
+            g.set_kernel_mode(v["mode"])
+        gs.append(g)
+    if drive:
+        drive(o)
+        for g in gs:
+            drive(g)
+    firsts = [-1] * len(gs)
+    done = 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        o.run_steps(k)
+        for j, (g, v) in enumerate(zip(gs, variants)):
+            if firsts[j] >= 0:
+                continue
+            g.run_steps(k)
+            if v.get("records", True):
+                bad = rows_equal(g, o, k)
+                if bad >= 0:
+                    firsts[j] = done + (k - 1 - bad)
+                    continue
+            if g.spikes_total() != o.spikes_total():
+                firsts[j] = done + k - 1
+        if int_weights and all(f >= 0 for f in firsts):
+            break
+        done += k
+    return gs, o, firsts

@@ -1,0 +1,99 @@
+"""Fixed-point parity at the benchmark configurations' full lengths.
+
+The 10k and 100k configurations run their whole 1000 ms (10,000 steps at
+dt 0.1 ms); the 1M-neuron configuration runs 1000 steps in an active regime
+(Poisson kicks, ~20 Hz, ~2e5 synaptic events per step); AdEx runs at 100k.
+Every GPU variant (streaming kernel, resident kernel, the step instance
+without optional features) is compared with ONE oracle run: every raster row
+where records are on, spike totals after every chunk, and every state bit
+(v, u/w, s, trace) at the end.  The configurations' own drive (Gaussian
+current noise sd 1) never reaches threshold, so each runs once as stated
+(state bits only, no spikes) and once with activity added: a constant drive
+on a fixed subset (as in tests/test_gpu_parity.py) or Poisson kicks."""
+import numpy as np
+import pytest
+
+import pyoracle as O
+import neuro_edit_v2_b200 as nb
+from helpers import lockstep_many, set_ext
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+ADEX_TONIC = [281.0, 30.0, -70.6, -50.4, 2.0, 4.0, 144.0, 80.5, -70.6, 20.0]
+STREAM = {"mode": nb.KERNEL_STREAM}
+RESIDENT = {"mode": nb.KERNEL_RESIDENT}
+PLAIN = {"mode": nb.KERNEL_STREAM, "records": False}
+
+
+def check(gs, o, firsts, variants, spikes=True):
+    """No divergence, then every state bit, the spike totals and (records on)
+    the lifetime per-neuron counts equal the oracle's."""
+    for g, f, v in zip(gs, firsts, variants):
+        assert f < 0, f"{v}: diverged at step {f}"
+        assert g.step_count() == o.t()
+        if spikes:
+            assert g.spikes_total() > 0
+        assert g.spikes_total() == o.spikes_total()
+        for name, a, b in (("v", g.state(0), o.state(0)), ("u", g.state(1), o.state(1)),
+                           ("s", g.syn_current(), o.syn_current()), ("trace", g.trace(), o.trace())):
+            bad = np.flatnonzero(a.view(np.uint32) != b.view(np.uint32))
+            assert bad.size == 0, f"{v} {name}: {bad.size} neurons differ, first {bad[:5]}"
+        if v.get("records", True):
+            assert np.array_equal(g.spike_counts(2**63), o.spike_counts(2**63))
+
+
+@pytest.mark.parametrize("n", [10_000, 100_000])
+def test_config_as_stated_full_1000_ms(n):
+    """Gaussian noise sd 1, tau_syn 5 ms, int ring, 10,000 steps: no neuron
+    reaches threshold; every state bit is the oracle's at the end."""
+    variants = [STREAM, RESIDENT, PLAIN]
+    gs, o, firsts = lockstep_many(O.ONet.random_kout(n, 100, 1), 10_000, variants, chunk=1000, gauss_sd=1.0,
+                                  synapse_tau_ms=5.0)
+    check(gs, o, firsts, variants, spikes=False)
+
+
+@pytest.mark.parametrize("n", [10_000, 100_000])
+def test_config_driven_full_1000_ms_bit_exact(n):
+    """The same nets with a constant drive on every 7th (10k) or 11th (100k)
+    neuron, every raster row of all 10,000 steps."""
+    stride = 7 if n == 10_000 else 11
+    amp = 6.0 if n == 10_000 else 8.0
+    variants = [STREAM, RESIDENT]
+    gs, o, firsts = lockstep_many(O.ONet.random_kout(n, 100, 1), 10_000, variants, chunk=500, gauss_sd=1.0,
+                                  synapse_tau_ms=5.0, drive=lambda s: set_ext(s, n, range(0, n, stride), amp))
+    check(gs, o, firsts, variants)
+
+
+def test_100k_active_regime_full_1000_ms_bit_exact():
+    """The bench's active 100k regime: Gaussian noise sd 1 plus Poisson kicks
+    100 Hz x 20 mV (~23 Hz firing, ~2e4 events per step), all 10,000 rows."""
+    variants = [STREAM, PLAIN]
+    gs, o, firsts = lockstep_many(O.ONet.random_kout(100_000, 100, 1), 10_000, variants, chunk=500, gauss_sd=1.0,
+                                  synapse_tau_ms=5.0, noise_rate_hz=100.0, noise_kick_mv=20.0, seed=1)
+    check(gs, o, firsts, variants)
+    rate = o.mean_rate_hz()
+    assert 10.0 < rate < 60.0, rate
+
+
+def test_1m_active_regime_1000_steps_bit_exact():
+    """1,000,000 neurons x K=100 (~1e8 synapses, a ~670 MB ring), Gaussian
+    noise sd 1 plus Poisson kicks 100 Hz x 20 mV: ~2e5 synaptic events per
+    step into the HBM-resident ring.  Records on (every raster row of 1000
+    steps) and off (the plain instance the bench times)."""
+    variants = [STREAM, PLAIN]
+    gs, o, firsts = lockstep_many(O.ONet.random_kout(1_000_000, 100, 1), 1000, variants, chunk=250, gauss_sd=1.0,
+                                  synapse_tau_ms=5.0, noise_rate_hz=100.0, noise_kick_mv=20.0, seed=1)
+    check(gs, o, firsts, variants)
+    assert o.spikes_total() > 1000 * 1000  # > 10 Hz
+
+
+def test_adex_100k_bit_exact():
+    """100,000 AdEx neurons (TONIC parameters, weights x C), Gaussian noise
+    sd 1 and Poisson kicks, 2000 steps, deterministic exp on both sides."""
+    onet = O.ONet.random_kout(100_000, 100, 3, w_scale=0.7 * 281.0)
+    for i in range(onet.n):
+        onet.set_model(i, O.ADEX, ADEX_TONIC)
+    variants = [STREAM, RESIDENT, PLAIN]
+    gs, o, firsts = lockstep_many(onet, 2000, variants, chunk=250, gauss_sd=1.0, synapse_tau_ms=5.0,
+                                  noise_rate_hz=100.0, noise_kick_mv=20.0, seed=2)
+    check(gs, o, firsts, variants)

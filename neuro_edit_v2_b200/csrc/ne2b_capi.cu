@@ -916,14 +916,14 @@ ne2b_status ne2b_server_step(ne2b_server *s, uint32_t *active_out, uint32_t *fin
                 continue;
             }
             // retire, stream-ordered after the launch that finished it: the
-            // spike total is summed from the neurons' counts, the window
-            // counts stay allocated until the result is taken
+            // spike total is copied out of the shared counter array, the
+            // window counts stay allocated until the result is taken
             r.d_win = h->dev.win_out;
             cudaStream_t st_main = s->eng.stream();
             st = ne2b::cuda_error(cudaMallocAsync((void **)&r.d_spk, sizeof(unsigned long long), st_main), "result");
             if (st == NE2B_OK)
-                st = ne2b::cuda_error(ne2b::launch_pn_sum(h->dev.pn_total, h->n, r.d_spk, st_main), "result");
-            s->eng.count_launches(h->n ? 1 : 0);
+                st = ne2b::cuda_error(cudaMemcpyAsync(r.d_spk, s->eng.counter_ptr(r.slot), sizeof(unsigned long long),
+                                                      cudaMemcpyDeviceToDevice, st_main), "result");
             if (st == NE2B_OK) st = s->eng.remove_net(r.slot, false, r.d_win);
             if (st == NE2B_OK) st = ne2b::cuda_error(cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming), "event");
             if (st == NE2B_OK) st = ne2b::cuda_error(cudaEventRecord(r.ev, st_main), "event");

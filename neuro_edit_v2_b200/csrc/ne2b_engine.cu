@@ -650,55 +650,6 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         NET_TRY(alloc(&p, sizeof(float) * nx)); d.xsyn = (float *)p;
         NET_TRY(alloc(&p, sizeof(uint32_t) * (size_t)h->D * d.xwords)); d.xpend = (uint32_t *)p;
     }
-    // deferred delivery (nets without custom-tau synapses): the spike words
-    // of the last two steps, and the delay-1 synapses again in a table of
-    // their own (they cannot wait a step: they land in the next step's slot)
-    if (!any_tau) {
-        const size_t words = np / 32;
-        NET_TRY(alloc(&p, sizeof(uint32_t) * 2 * words)); d.sbits = (uint32_t *)p;
-        NET_TRY(cuda_error(cudaMemsetAsync(d.sbits, 0, sizeof(uint32_t) * 2 * words, bst), "memset spike words"));
-        if (h->e && (dc || mind <= 1)) {
-            uint32_t *cnt = nullptr, *cursor = nullptr, *sums = nullptr;
-            unsigned long long *tot = nullptr, e1 = 0;
-            auto tmp = [&](void **q, size_t bytes) {
-                return cuda_error(cudaMallocAsync(q, bytes, bst), "cudaMallocAsync (delay-1 table scratch)");
-            };
-            auto drop = [&]() {
-                for (void *q : {(void *)cnt, (void *)cursor, (void *)sums, (void *)tot})
-                    if (q) cudaFreeAsync(q, bst);
-            };
-            ne2b_status st = tmp((void **)&cnt, sizeof(uint32_t) * n);
-            if (st == NE2B_OK) st = tmp((void **)&tot, sizeof(unsigned long long));
-            if (st == NE2B_OK)
-                st = cuda_error(launch_d1_count(d.rowptr, d.delay, d16, n, cnt, tot, bst), "delay-1 counts");
-            if (st == NE2B_OK)
-                st = cuda_error(cudaMemcpyAsync(&e1, tot, sizeof e1, cudaMemcpyDeviceToHost, bst), "delay-1 total");
-            if (st == NE2B_OK) st = cuda_error(cudaStreamSynchronize(bst), "delay-1 total");
-            h->build_launches += 1;
-            if (st == NE2B_OK && e1 > 0) {
-                st = alloc(&p, sizeof(uint32_t) * words);
-                d.d1bits = (const uint32_t *)p;
-                if (st == NE2B_OK) st = alloc(&p, sizeof(uint32_t) * ((size_t)n + 1));
-                d.d1ptr = (const uint32_t *)p;
-                if (st == NE2B_OK) st = alloc(&p, sizeof(uint32_t) * e1);
-                d.d1tgt = (const uint32_t *)p;
-                if (st == NE2B_OK) st = alloc(&p, sizeof(uint32_t) * e1);
-                d.d1w = (const uint32_t *)p;
-                if (st == NE2B_OK) st = tmp((void **)&cursor, sizeof(uint32_t) * n);
-                if (st == NE2B_OK) st = tmp((void **)&sums, sizeof(uint32_t) * csr_scan_blocks(n));
-                if (st == NE2B_OK)
-                    st = cuda_error(csr_scan(cnt, n, (uint32_t)e1, (uint32_t *)d.d1ptr, cursor, sums, bst),
-                                    "delay-1 table: row pointers");
-                if (st == NE2B_OK)
-                    st = cuda_error(launch_d1_fill(d.rowptr, d.tgt, (const uint32_t *)d.w, d.delay, d16, n, np, d.d1ptr,
-                                                   (uint32_t *)d.d1tgt, (uint32_t *)d.d1w, (uint32_t *)d.d1bits, bst),
-                                    "delay-1 table");
-                h->build_launches += 4;
-            }
-            drop();
-            NET_TRY(st);
-        }
-    }
     tp[4] = now_ms();
     // stimulus routing
     const bool has_stim = n > 0 && net->n_inputs > 0 && net->stim_ptr && net->stim_ptr[n] > 0;
@@ -1019,8 +970,6 @@ ne2b_status Engine::reset_net(uint32_t slot) {
         NE2B_CUDA(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h.nx, stream_));
         NE2B_CUDA(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h.D * d.xwords, stream_));
     }
-    // no spike of an earlier step is left to deliver
-    if (d.sbits) NE2B_CUDA(cudaMemsetAsync(d.sbits, 0, sizeof(uint32_t) * 2 * (h.n_pad / 32), stream_));
     // cpu.rs:176-183: the watch history and the grid marks start over
     h.watch_t0 = 0;
     if (d.gw_ls) NE2B_CUDA(cudaMemsetAsync(d.gw_ls, 0xFF, sizeof(uint32_t) * std::max<uint32_t>(h.gw_ptr.back(), 1), stream_));
@@ -1279,10 +1228,6 @@ ne2b_status Engine::spike_row(NetHost &h, uint32_t back, uint64_t *out) {
 }
 
 ne2b_status Engine::spikes_total(NetHost &h, uint64_t *out) {
-    // the sum of the neurons' lifetime counts (the step kernel keeps no
-    // per-net counter: that would be one same-address atomic per spiking tile)
-    NE2B_CUDA(launch_pn_sum(h.dev.pn_total, h.n, &d_counters_[h.slot].spikes_total, stream_));
-    launches_ += h.n ? 1 : 0;
     NE2B_CUDA(cudaMemcpyAsync(out, &d_counters_[h.slot].spikes_total, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream_));
     NE2B_CUDA(cudaStreamSynchronize(stream_));
     return NE2B_OK;
@@ -1482,7 +1427,6 @@ ne2b_status Engine::snapshot(EngineSnapshot &snap) {
         NE2B_TRY(grab(d.watch_ring, d.watch_ring ? 8 * (size_t)d.watch_n * kWatchCap : 0));
         NE2B_TRY(grab(d.gw_ls, d.gw_ls ? 4 * (size_t)std::max<uint32_t>(h->gw_ptr.back(), 1) : 0));
         NE2B_TRY(grab(d.xpend, 4 * (size_t)h->D * d.xwords));
-        NE2B_TRY(grab(d.sbits, d.sbits ? 4 * 2 * (np / 32) : 0));
         snap.hosts.push_back({h->slot, h->t, h->dev});
     }
     return NE2B_OK;

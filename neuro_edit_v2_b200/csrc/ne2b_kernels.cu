@@ -4,8 +4,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <algorithm>
-
 #include "ne2b_kernels.h"
 #include "ne2b_step.cuh"
 
@@ -64,54 +62,6 @@ __global__ void pn_total_kernel(const unsigned long long *pn, uint32_t n, uint32
     if (i >= n) return;
     const unsigned long long c = pn[i];
     out[i] = c > 0xffffffffull ? 0xffffffffu : (uint32_t)c;
-}
-
-// Spike total of a net: the sum of its neurons' lifetime counts, added into
-// *out (zeroed by the caller).
-__global__ void pn_sum_kernel(const unsigned long long *pn, uint32_t n, unsigned long long *out) {
-    unsigned long long c = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c += pn[i];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
-}
-
-// The delay-1 table of deferred delivery, step 1: delay-1 synapses per
-// source neuron (thread per neuron) and their total.
-__global__ void d1_count_kernel(const uint32_t *rowptr, const void *delay, bool d16, uint32_t n, uint32_t *cnt,
-                                unsigned long long *total) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t c = 0;
-    if (i < n)
-        for (uint32_t j = rowptr[i], je = rowptr[i + 1]; j < je; ++j)
-            c += (d16 ? ((const uint16_t *)delay)[j] : ((const uint8_t *)delay)[j]) == 1u;
-    if (i < n) cnt[i] = c;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(total, (unsigned long long)c);
-}
-
-// Step 2 (after the scan of the counts into d1ptr): each neuron's delay-1
-// synapses in CSR order, and the flag words (one thread per padded neuron,
-// whole warps).
-__global__ void d1_fill_kernel(const uint32_t *rowptr, const uint32_t *tgt, const uint32_t *wbits, const void *delay,
-                               bool d16, uint32_t n, uint32_t n_pad, const uint32_t *d1ptr, uint32_t *d1tgt,
-                               uint32_t *d1w, uint32_t *d1bits) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_pad) return;  // n_pad is a multiple of 64: warps stay whole
-    bool any = false;
-    if (i < n) {
-        uint32_t pos = d1ptr[i];
-        for (uint32_t j = rowptr[i], je = rowptr[i + 1]; j < je; ++j)
-            if ((d16 ? ((const uint16_t *)delay)[j] : ((const uint8_t *)delay)[j]) == 1u) {
-                d1tgt[pos] = tgt[j];
-                d1w[pos] = wbits[j];
-                ++pos;
-            }
-        any = pos > d1ptr[i];
-    }
-    const uint32_t m = __ballot_sync(0xffffffffu, any);
-    if ((threadIdx.x & 31) == 0) d1bits[i >> 5] = m;
 }
 
 // Self-test of the bounded grid barrier: every block but `absent` arrives,
@@ -184,31 +134,6 @@ cudaError_t launch_barrier_selftest(unsigned int *counter, unsigned int *err, ui
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st) {
     if (n_nets == 0) return cudaSuccess;
     return launch_pdl(advance_kernel, (n_nets + 127) / 128, 128, st, true, nets, n_nets, steps);
-}
-
-cudaError_t launch_pn_sum(const unsigned long long *pn, uint32_t n, unsigned long long *out, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long), st);
-    if (e != cudaSuccess || n == 0) return e;
-    const uint32_t blocks = std::min<uint32_t>((n + 255) / 256, 1184);
-    pn_sum_kernel<<<blocks, 256, 0, st>>>(pn, n, out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_d1_count(const uint32_t *rowptr, const void *delay, bool d16, uint32_t n, uint32_t *cnt,
-                            unsigned long long *total, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(total, 0, sizeof(unsigned long long), st);
-    if (e != cudaSuccess || n == 0) return e;
-    d1_count_kernel<<<(n + 255) / 256, 256, 0, st>>>(rowptr, delay, d16, n, cnt, total);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_d1_fill(const uint32_t *rowptr, const uint32_t *tgt, const uint32_t *wbits, const void *delay,
-                           bool d16, uint32_t n, uint32_t n_pad, const uint32_t *d1ptr, uint32_t *d1tgt, uint32_t *d1w,
-                           uint32_t *d1bits, cudaStream_t st) {
-    if (n_pad == 0) return cudaSuccess;
-    d1_fill_kernel<<<(n_pad + 255) / 256, 256, 0, st>>>(rowptr, tgt, wbits, delay, d16, n, n_pad, d1ptr, d1tgt, d1w,
-                                                         d1bits);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st) {

@@ -35,15 +35,5 @@ cudaError_t launch_trace(const uint16_t *tk, const float *tab, uint32_t n, float
 cudaError_t launch_window_count(const uint32_t *rec_bits, uint32_t rec_rows, uint32_t n_pad, uint32_t n,
                                 unsigned long long t, uint32_t rows, uint32_t *out, cudaStream_t st);
 cudaError_t launch_pn_total(const unsigned long long *pn, uint32_t n, uint32_t *out, cudaStream_t st);
-// *out = sum of pn[0..n) (the net's spike total; *out is zeroed first).
-cudaError_t launch_pn_sum(const unsigned long long *pn, uint32_t n, unsigned long long *out, cudaStream_t st);
-// Delay-1 table of deferred delivery: per-source counts and their total
-// (zeroed first), then, after the counts are scanned into d1ptr, the
-// targets, weight bits and flag words [n_pad / 32].
-cudaError_t launch_d1_count(const uint32_t *rowptr, const void *delay, bool d16, uint32_t n, uint32_t *cnt,
-                            unsigned long long *total, cudaStream_t st);
-cudaError_t launch_d1_fill(const uint32_t *rowptr, const uint32_t *tgt, const uint32_t *wbits, const void *delay,
-                           bool d16, uint32_t n, uint32_t n_pad, const uint32_t *d1ptr, uint32_t *d1tgt, uint32_t *d1w,
-                           uint32_t *d1bits, cudaStream_t st);
 
 }  // namespace ne2b

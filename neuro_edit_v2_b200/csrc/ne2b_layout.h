@@ -16,11 +16,6 @@
 //   stimulus: neuron-major (input, weight) rows and a [steps x n_inputs] f32
 //     value buffer; spike record: rows x n_pad/32 u32 words; window counts:
 //     max_windows x n_pad u16.
-//   deferred delivery (every net without custom-tau synapses): the spike
-//     words of the last two steps, 2 x n_pad/32 u32 (row t & 1 = step t's
-//     ballots), and the delay-1 synapses again in a small CSR of their own
-//     (d1bits: neurons that have any; d1ptr/d1tgt/d1w), delivered in the
-//     step of the spike because they land in the next step's slot.
 #pragma once
 #include <stdint.h>
 
@@ -111,15 +106,6 @@ struct alignas(16) NetDev {
     const uint32_t *gw_off;     // [gw_n + 1] group ranges in gw_ls
     uint32_t *gw_ls;            // last spike step per texel (min(t, 2^32-2)), kNeverSpiked
     uint32_t watch_n, gw_n;
-    // deferred delivery (nets without kNetXsyn): spikes of step t are
-    // delivered by step t + 1's launch, overlapping its neuron pass, except
-    // their delay-1 synapses (slot t + 1 is read by that launch), which are
-    // delivered at once from the d1 table
-    uint32_t *sbits;            // [2 x n_pad/32] step t's spike words in row t & 1
-    const uint32_t *d1bits;     // [n_pad/32] neurons with delay-1 synapses, or null if the net has none
-    const uint32_t *d1ptr;      // [n+1] each neuron's range of d1tgt / d1w
-    const uint32_t *d1tgt;      // [E1] targets of the delay-1 synapses, CSR order
-    const uint32_t *d1w;        // [E1] their weight bits (as w)
     // scalars
     unsigned long long t;       // step index of the next launch group's k = 0
     unsigned long long t_end;   // steps at or beyond this are skipped (serving)

@@ -16,26 +16,14 @@
 //      the tile's spikes by their CSR rows with block prefix sums over
 //      (spikes, synapses) into shared memory (replaces the global atomicAdd
 //      slot of kernels.rs:150-156);
-//   5. deliver the spikes: the block strides the flat range of all their
-//      synapses, a no-return atomic add into ring[(t_spike + delay) % D][tgt]
-//      per synapse (cpu.rs:264-278, kernels.rs:174-204).
-//
-// Deferred delivery (every net without custom-tau synapses): a spike of step
-// t needs its synapses in the ring only by step t + d, d >= 1.  So step t
-// only stores its ballot words (sbits row t & 1) and delivers the delay-1
-// synapses of its spikes at once (from the small d1 table: their slot t + 1
-// is the next step's), and step t + 1 delivers everything else: each tile
-// reads its neurons' spike words of step t with its state, lists their rows
-// and issues their CSR loads and ring adds before and beside its own neuron
-// pass.  The CSR round trip and the drain of the adds, which ended every
-// spiking step's critical path, now overlap the next step's state loads.
-// Integer ring sums do not depend on the order of the adds, so the rasters
-// are unchanged; the f32 ring adds in an arbitrary order either way.
+//   5. deliver its own spikes: the block strides the flat range of all its
+//      spikes' synapses, a no-return atomic add into
+//      ring[(t + delay) % D][tgt] per synapse (cpu.rs:264-278,
+//      kernels.rs:174-204).
 //
 // Within a step no cross-block ordering is needed: step t reads slot t % D and
-// every delivery of step t lands in slot (t + d) % D, 1 <= d < D (the deferred
-// ones of step t - 1's spikes in (t - 1 + d) % D with d >= 2, never slot
-// t % D).  Between steps, step t's deliveries must land before step t+1 reads:
+// every delivery of step t lands in slot (t + d) % D, 1 <= d < D.  Between
+// steps, step t's deliveries must land before step t+1 reads:
 //   * step_kernel (streaming): one launch per step, the kernel boundary orders
 //     the steps; state is streamed from HBM every step.
 //   * resident_kernel (persistent, cooperative): each block owns a fixed set
@@ -73,135 +61,6 @@ __device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, u
     return SmemLists{base, base + tile, base + 2 * tile + 1, base + 2 * tile + 1 + nw, base + 2 * tile + 1 + 2 * nw};
 }
 
-// One no-return atomic add of weight bits `wb` into ring word `idx`.
-template <bool INT>
-__device__ __forceinline__ void ring_add(uint32_t *ringw, size_t idx, uint32_t wb) {
-    if (INT) atomicAdd((int *)ringw + idx, (int)wb);
-    else atomicAdd((float *)ringw + idx, __uint_as_float(wb));
-}
-
-// CSR index of flat synapse f of the listed rows (binary search of off[]).
-__device__ __forceinline__ uint32_t row_synapse(const SmemLists &sl, uint32_t total, uint32_t f) {
-    uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (sl.off[mid] <= f) lo = mid;
-        else hi = mid;
-    }
-    return sl.lo[lo] + (f - sl.off[lo]);
-}
-
-// Lists the CSR rows [rlo, rhi) of the neurons a thread flags in `has` in
-// shared memory, by block prefix sums over (rows, synapses).  A block with
-// no flagged neuron returns false after one block barrier; otherwise every
-// thread returns true with `total` rows and `nsyn` synapses listed.
-template <int BLOCK, int NPT>
-__device__ __forceinline__ bool list_rows(const bool (&has)[NPT], const uint32_t (&rlo)[NPT],
-                                          const uint32_t (&rhi)[NPT], const SmemLists &sl, uint32_t &total,
-                                          uint32_t &nsyn) {
-    constexpr int NW = BLOCK / 32;
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    uint32_t cnt = 0, syn = 0;
-#pragma unroll
-    for (int q = 0; q < NPT; ++q)
-        if (has[q]) {
-            ++cnt;
-            syn += rhi[q] - rlo[q];
-        }
-    if (!__syncthreads_or(cnt != 0u)) return false;
-    uint32_t ic = cnt, is = syn;  // inclusive warp scans
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t yc = __shfl_up_sync(0xffffffffu, ic, o);
-        const uint32_t ys = __shfl_up_sync(0xffffffffu, is, o);
-        if (lane >= o) {
-            ic += yc;
-            is += ys;
-        }
-    }
-    if (lane == 31) {
-        sl.woff[warp] = ic;
-        sl.wsyn[warp] = is;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t c = lane < NW ? sl.woff[lane] : 0u, y = lane < NW ? sl.wsyn[lane] : 0u;
-        uint32_t jc = c, js = y;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t a = __shfl_up_sync(0xffffffffu, jc, o);
-            const uint32_t b = __shfl_up_sync(0xffffffffu, js, o);
-            if (lane >= o) {
-                jc += a;
-                js += b;
-            }
-        }
-        if (lane < NW) {
-            sl.woff[lane] = jc - c;
-            sl.wsyn[lane] = js - y;
-        }
-        if (lane == 31) {
-            sl.total[0] = jc;
-            sl.total[1] = js;
-        }
-    }
-    __syncthreads();
-    {
-        uint32_t pos = sl.woff[warp] + ic - cnt;
-        uint32_t so = sl.wsyn[warp] + is - syn;
-#pragma unroll
-        for (int q = 0; q < NPT; ++q)
-            if (has[q]) {
-                sl.lo[pos] = rlo[q];
-                sl.off[pos] = so;
-                ++pos;
-                so += rhi[q] - rlo[q];
-            }
-    }
-    total = sl.total[0];
-    nsyn = sl.total[1];
-    if (threadIdx.x == 0) sl.off[total] = nsyn;
-    __syncthreads();
-    return true;
-}
-
-// Deferred delivery of the listed rows, spikes of the step whose slot is
-// `pslot`: the block strides the flat synapse range, U synapses per thread
-// and pass with all their CSR loads issued before any add (a thread past the
-// end repeats its first synapse's loads, cheaper in registers than
-// predicated loads, and skips the add); delay-1 synapses were delivered in
-// the spike's own step and are skipped.  Ends with a block barrier (the next
-// tile reuses the lists).
-template <bool INT, int BLOCK>
-__device__ __forceinline__ void deliver_rows(const NetDev &nd, uint32_t *ringw, const SmemLists &sl, uint32_t total,
-                                             uint32_t nsyn, uint32_t pslot) {
-    constexpr int U = kDeliverUnroll<INT>;
-    const uint32_t *__restrict__ tgt = nd.tgt;
-    const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
-    const bool d16 = nd.flags & kNetDelay16;
-    const uint32_t D = nd.D, n_pad = nd.n_pad;
-    for (uint32_t f = threadIdx.x; f < nsyn; f += U * BLOCK) {
-        uint32_t j[U], tg[U], d[U], wb[U];
-        j[0] = row_synapse(sl, total, f);
-#pragma unroll
-        for (int q = 1; q < U; ++q) j[q] = f + q * BLOCK < nsyn ? row_synapse(sl, total, f + q * BLOCK) : j[0];
-#pragma unroll
-        for (int q = 0; q < U; ++q) {
-            tg[q] = tgt[j[q]];
-            d[q] = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j[q]] : (uint32_t)((const uint8_t *)nd.delay)[j[q]];
-            wb[q] = wbits[j[q]];
-        }
-#pragma unroll
-        for (int q = 0; q < U; ++q)
-            if (f + q * BLOCK < nsyn && d[q] != 1u) {
-                const uint32_t slot = pslot + d[q] >= D ? pslot + d[q] - D : pslot + d[q];
-                ring_add<INT>(ringw, (size_t)slot * n_pad + tg[q], wb[q]);
-            }
-    }
-    __syncthreads();
-}
-
 // `nd` is the tile's net descriptor (global memory, or a shared-memory copy
 // staged before the launch's dependency wait); `t` is the absolute step,
 // `tmod` = t % D and `k` = t - nd.t (the step within the launch group).
@@ -218,6 +77,7 @@ template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool L
 __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
                                              const Tile &tile, uint64_t t, uint32_t tmod, uint32_t k, float *vs, float *us,
                                              float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
+    constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const uint32_t flags = nd.flags;
@@ -290,49 +150,9 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         }
     }
 
-    const uint32_t *__restrict__ rowptr = nd.rowptr;
-    // ---- deferred delivery of step t - 1's spikes in this tile (their
-    // words in sbits row (t - 1) & 1; reset zeroes both rows, so step 0
-    // finds none), while the state loads above are in flight; with it the
-    // delay-1 table rows of this step's flagged neurons and their first
-    // synapse, so a spike among them can deliver at once
-    uint32_t d1lo[NPT], d1hi[NPT], d1t0[NPT], d1w0[NPT];
-    if (!xsyn_on) {
-        const uint32_t words32 = n_pad >> 5;
-        const uint32_t *prow = nd.sbits + (size_t)((t - 1u) & 1u) * words32;
-        bool pb[NPT];
-        uint32_t plo[NPT], phi[NPT];
-#pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-            const uint32_t off = q * BLOCK + warp * 32;
-            const uint32_t wi = (tile.start + off) >> 5;
-            const uint32_t word = off < tile.count ? (RES ? __ldcg(prow + wi) : prow[wi]) : 0u;
-            pb[q] = valid[q] && ((word >> lane) & 1u);
-            plo[q] = phi[q] = 0u;
-            if (pb[q]) {
-                plo[q] = rowptr[li[q]];
-                phi[q] = rowptr[li[q] + 1];
-            }
-            d1lo[q] = d1hi[q] = d1t0[q] = d1w0[q] = 0u;
-            if (nd.d1bits) {
-                const uint32_t fw = off < tile.count ? nd.d1bits[wi] : 0u;
-                if (valid[q] && ((fw >> lane) & 1u)) {
-                    d1lo[q] = nd.d1ptr[li[q]];
-                    d1hi[q] = nd.d1ptr[li[q] + 1];
-                    if (d1lo[q] < d1hi[q]) {
-                        d1t0[q] = nd.d1tgt[d1lo[q]];
-                        d1w0[q] = nd.d1w[d1lo[q]];
-                    }
-                }
-            }
-        }
-        uint32_t total, nsyn;
-        if (list_rows<BLOCK, NPT>(pb, plo, phi, sl, total, nsyn))
-            deliver_rows<INT, BLOCK>(nd, ringw, sl, total, nsyn, tmod == 0u ? D - 1u : tmod - 1u);
-    }
-
     bool spk[NPT];
-    uint32_t rlo[NPT], rhi[NPT];  // custom-tau nets: CSR row of a spiking neuron, loaded as soon as it spikes
+    uint32_t rlo[NPT], rhi[NPT];  // CSR row of a spiking neuron, loaded as soon as it spikes
+    const uint32_t *__restrict__ rowptr = nd.rowptr;
 #pragma unroll
     for (int q = 0; q < NPT; ++q) {
         spk[q] = false;
@@ -415,10 +235,8 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         if (__float_as_uint(snew) != __float_as_uint(s[q])) ss[off] = snew;
         if (k != k0) tks[off] = (uint16_t)k;
         if (sp) {
-            if (xsyn_on) {
-                rlo[q] = rowptr[i];
-                rhi[q] = rowptr[i + 1];
-            }
+            rlo[q] = rowptr[i];
+            rhi[q] = rowptr[i + 1];
             nd.pn_total[i] += 1ull;
             if (!LEAN && (flags & kNetGridWatch)) {  // cpu.rs:293-304
                 const uint32_t t32 = t < 0xFFFFFFFEull ? (uint32_t)t : 0xFFFFFFFEu;
@@ -448,61 +266,149 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         spk[q] = sp;
     }
 
-    // ---- spike words: one ballot per warp and q, for the record row and
-    // (deferred delivery) the step's row of sbits
-    const uint32_t words32 = n_pad >> 5;
-    uint32_t row = 0;
+    // ---- spike record: one ballot word per warp and q
     if (!LEAN && (flags & kNetRecord)) {
+        uint32_t row;
         if constexpr (PHASES) {
             row = nd.rphase + k;
             if (row >= nd.rec_rows) row %= nd.rec_rows;
         } else {
             row = mod_steps(t, nd.rec_rows);
         }
-    }
+        const uint32_t words32 = n_pad >> 5;
 #pragma unroll
-    for (int q = 0; q < NPT; ++q) {
-        const uint32_t mask = __ballot_sync(0xffffffffu, spk[q]);
-        const uint32_t off = q * BLOCK + warp * 32;
-        if (lane == 0 && off < tile.count) {
-            const uint32_t word = (tile.start + off) >> 5;
-            if (!LEAN && (flags & kNetRecord)) nd.rec_bits[(size_t)row * words32 + word] = mask;
-            if (!xsyn_on) nd.sbits[(size_t)(t & 1u) * words32 + word] = mask;
+        for (int q = 0; q < NPT; ++q) {
+            const uint32_t mask = __ballot_sync(0xffffffffu, spk[q]);
+            const uint32_t off = q * BLOCK + warp * 32;
+            if (lane == 0 && off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask;
         }
     }
-    if (!xsyn_on) {
-        // delay-1 synapses of this step's spikes: their slot is the next
-        // step's, so they cannot wait (the first one was loaded before the
-        // neuron pass)
-        const uint32_t nslot = tmod + 1u == D ? 0u : tmod + 1u;
+    // ---- compaction: per-thread (spikes, synapses), block prefix sums
+    uint32_t cnt = 0, syn = 0;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+        if (spk[q]) {
+            ++cnt;
+            syn += rhi[q] - rlo[q];
+        }
+    // quiet tile: one block barrier, no scan, no delivery
+    if (!__syncthreads_or(cnt != 0u)) return;
+    uint32_t ic = cnt, is = syn;  // inclusive warp scans
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t yc = __shfl_up_sync(0xffffffffu, ic, o);
+        const uint32_t ys = __shfl_up_sync(0xffffffffu, is, o);
+        if (lane >= o) {
+            ic += yc;
+            is += ys;
+        }
+    }
+    if (lane == 31) {
+        sl.woff[warp] = ic;
+        sl.wsyn[warp] = is;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t c = lane < NW ? sl.woff[lane] : 0u, y = lane < NW ? sl.wsyn[lane] : 0u;
+        uint32_t jc = c, js = y;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t a = __shfl_up_sync(0xffffffffu, jc, o);
+            const uint32_t b = __shfl_up_sync(0xffffffffu, js, o);
+            if (lane >= o) {
+                jc += a;
+                js += b;
+            }
+        }
+        if (lane < NW) {
+            sl.woff[lane] = jc - c;
+            sl.wsyn[lane] = js - y;
+        }
+        if (lane == 31) {
+            sl.total[0] = jc;
+            sl.total[1] = js;
+        }
+    }
+    __syncthreads();
+    {
+        uint32_t pos = sl.woff[warp] + ic - cnt;
+        uint32_t so = sl.wsyn[warp] + is - syn;
 #pragma unroll
         for (int q = 0; q < NPT; ++q)
-            if (spk[q] && d1lo[q] < d1hi[q]) {
-                ring_add<INT>(ringw, (size_t)nslot * n_pad + d1t0[q], d1w0[q]);
-                for (uint32_t j = d1lo[q] + 1u; j < d1hi[q]; ++j)
-                    ring_add<INT>(ringw, (size_t)nslot * n_pad + nd.d1tgt[j], nd.d1w[j]);
+            if (spk[q]) {
+                sl.lo[pos] = rlo[q];
+                sl.off[pos] = so;
+                ++pos;
+                so += rhi[q] - rlo[q];
             }
-        return;
     }
-    // ---- custom-tau nets: compaction and immediate delivery
-    uint32_t total, nsyn;
-    if (!list_rows<BLOCK, NPT>(spk, rlo, rhi, sl, total, nsyn)) return;
+    const uint32_t total = sl.total[0], nsyn = sl.total[1];
+    if (threadIdx.x == 0) sl.off[total] = nsyn;
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
+    // ---- delivery: the block strides the flat synapse range; a thread
+    // finds its row by binary search over off[], then adds the weight into
+    // ring[(t + d) % D][tgt] with a no-return atomic
     const uint32_t *__restrict__ tgt = nd.tgt;
     const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
     const bool d16 = flags & kNetDelay16;
-    for (uint32_t f = threadIdx.x; f < nsyn; f += BLOCK) {
-        const uint32_t j = row_synapse(sl, total, f);
-        const uint32_t tg = tgt[j];
+    auto syn_at = [&](uint32_t f) {
+        uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sl.off[mid] <= f) lo = mid;
+            else hi = mid;
+        }
+        return sl.lo[lo] + (f - sl.off[lo]);
+    };
+    auto slot_of = [&](uint32_t j) {
         const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
-        const uint32_t slot = tmod + d >= D ? tmod + d - D : tmod + d;
+        const uint32_t slot = tmod + d;
+        return slot >= D ? slot - D : slot;
+    };
+    auto add = [&](uint32_t slot, uint32_t tg, uint32_t wb) {
+        const size_t idx = (size_t)slot * n_pad + tg;
+        if (INT) atomicAdd((int *)ringw + idx, (int)wb);
+        else atomicAdd((float *)ringw + idx, __uint_as_float(wb));
+    };
+    if (!xsyn_on) {
+        // U synapses per thread and pass, all their loads issued before any
+        // add, so a tile with more synapses than threads pays one round trip
+        // to the CSR per U block-widths
+        constexpr int U = kDeliverUnroll<INT>;
+        for (uint32_t f = threadIdx.x; f < nsyn; f += U * BLOCK) {
+            // a thread past the end repeats its first synapse's loads (same
+            // lines; cheaper in registers than predicated loads) and skips
+            // the add
+            uint32_t j[U], tg[U], sl_[U], wb[U];
+            j[0] = syn_at(f);
+#pragma unroll
+            for (int q = 1; q < U; ++q) j[q] = f + q * BLOCK < nsyn ? syn_at(f + q * BLOCK) : j[0];
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                tg[q] = tgt[j[q]];
+                sl_[q] = slot_of(j[q]);
+                wb[q] = wbits[j[q]];
+            }
+#pragma unroll
+            for (int q = 0; q < U; ++q)
+                if (f + q * BLOCK < nsyn) add(sl_[q], tg[q], wb[q]);
+        }
+        __syncthreads();  // the next tile reuses the shared lists
+        return;
+    }
+    for (uint32_t f = threadIdx.x; f < nsyn; f += BLOCK) {
+        const uint32_t j = syn_at(f);
+        const uint32_t tg = tgt[j];
+        const uint32_t slot = slot_of(j);
         {
-            const uint32_t xk = nd.xmap[j];
-            if (xk != kNoXsyn) {  // its own current: mark the arrival (cpu.rs:270-273)
-                atomicOr(nd.xpend + (size_t)slot * nd.xwords + (xk >> 5), 1u << (xk & 31u));
+            const uint32_t k = nd.xmap[j];
+            if (k != kNoXsyn) {  // its own current: mark the arrival (cpu.rs:270-273)
+                atomicOr(nd.xpend + (size_t)slot * nd.xwords + (k >> 5), 1u << (k & 31u));
                 continue;
             }
         }
-        ring_add<INT>(ringw, (size_t)slot * n_pad + tg, wbits[j]);
+        add(slot, tg, wbits[j]);
     }
     // the next tile reuses the shared lists
     __syncthreads();

@@ -238,9 +238,10 @@ def barrier(ws: int):
         dist.barrier()
 
 
-def make_cfg(nb, active: bool):
-    return nb.default_config(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0,
-                             noise_rate_hz=ACTIVE_KICK_HZ if active else 0.0, noise_kick_mv=20.0, seed=SEED)
+def make_cfg(nb, active: bool, adex: bool = False):
+    kick = (ADEX_ACTIVE_KICK_HZ if adex else ACTIVE_KICK_HZ) if active else 0.0
+    return nb.default_config(int_weights=1, gauss_sd=1.0, synapse_tau_ms=5.0, noise_rate_hz=kick,
+                             noise_kick_mv=20.0, seed=SEED)
 
 
 def timed_trials(sim, steps: int, warmup: int, trial_steps: int, ws: int, torch, scrub):
@@ -287,7 +288,7 @@ def run_profile(args):
     net = nb.random_kout(args.profile_neurons, K_OUT, SEED, w_scale=0.7 * (281.0 if args.adex else 1.0))
     if args.adex:  # the AdEx variant of the 1M workload (weights x C = 281 pF)
         nb.to_adex(net)
-    sim = nb.B200Sim(net, make_cfg(nb, args.active))
+    sim = nb.B200Sim(net, make_cfg(nb, args.active, args.adex))
     if args.kernel:
         sim.set_kernel_mode({"stream": nb.KERNEL_STREAM, "resident": nb.KERNEL_RESIDENT}[args.kernel])
     if args.shape:

@@ -24,10 +24,16 @@ from helpers import configs, set_ext
 
 pytestmark = pytest.mark.gpu
 
-DV_TOL = 1e-2   # mV, per step, before the first raster divergence
-DS_TOL = 1e-3   # synaptic current, per step, before the first raster divergence
-COUNT_RTOL = 0.02
-FIRST_DIVERGENCE_MIN = {"10k": 100, "100k": 50, "bench_net": 50}
+# Measured on a B200 (one run each): no raster divergence within 2000 /
+# 1000 / 1500 locked steps, max |dv| 7.6e-6 / 2.3e-5 / 2.2e-4 mV and max
+# |ds| 2.4e-7 / 2.4e-7 / 7.6e-6 (10k / 100k / bench_net), equal spike
+# totals.  The error bounds keep about 10x margin; the divergence step of a
+# float-atomic run varies from run to run, so its bound is those measured
+# step counts, half of the locked windows used here.
+DV_TOL = 2e-3   # mV, per step, before the first raster divergence
+DS_TOL = 1e-4   # synaptic current, per step, before the first raster divergence
+COUNT_RTOL = 0.01
+FIRST_DIVERGENCE_MIN = {"10k": 2000, "100k": 1000, "bench_net": 1500}
 
 
 def run_case(onet, steps, lock_steps, drive=None, **cfg_kw):
@@ -56,11 +62,11 @@ def run_case(onet, steps, lock_steps, drive=None, **cfg_kw):
 
 
 CASES = {
-    "10k": dict(net=lambda: O.ONet.random_kout(10_000, 100, 1), steps=4000, lock=2000, gauss_sd=1.0,
+    "10k": dict(net=lambda: O.ONet.random_kout(10_000, 100, 1), steps=6000, lock=4000, gauss_sd=1.0,
                 synapse_tau_ms=5.0, drive=lambda s: set_ext(s, 10_000, range(0, 10_000, 7), 6.0)),
-    "100k": dict(net=lambda: O.ONet.random_kout(100_000, 100, 1), steps=2000, lock=1000, gauss_sd=1.0,
+    "100k": dict(net=lambda: O.ONet.random_kout(100_000, 100, 1), steps=3000, lock=2000, gauss_sd=1.0,
                  synapse_tau_ms=5.0, drive=lambda s: set_ext(s, 100_000, range(0, 100_000, 11), 8.0)),
-    "bench_net": dict(net=lambda: O.ONet.bench_net(4000, 100, 5, 0.7, 5.0), steps=3000, lock=1500,
+    "bench_net": dict(net=lambda: O.ONet.bench_net(4000, 100, 5, 0.7, 5.0), steps=4000, lock=3000,
                       noise_rate_hz=500.0, noise_kick_mv=20.0, seed=3),
 }
 

@@ -30,7 +30,7 @@ def check(gs, o, firsts, variants, spikes=True):
     the lifetime per-neuron counts equal the oracle's."""
     for g, f, v in zip(gs, firsts, variants):
         assert f < 0, f"{v}: diverged at step {f}"
-        assert g.step_count() == o.t()
+        assert g.step_count() == o.t
         if spikes:
             assert g.spikes_total() > 0
         assert g.spikes_total() == o.spikes_total()

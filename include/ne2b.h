@@ -173,7 +173,13 @@ ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd);                 /* ne
  * streaming kernel; the other two force one (RESIDENT fails with
  * NE2B_UNSUPPORTED when the nets do not fit).  *resident reports which
  * kernel runs.  The environment variable NE2B_KERNEL=stream|resident sets
- * the initial mode of every handle. */
+ * the initial mode of every handle.
+ *
+ * Delivery into a ring larger than 128 MB (D x n_pad x 4 bytes) goes through
+ * per-step event queues (arrivals appended per arrival step, added into the
+ * ring the step before they are read) instead of random adds into the ring;
+ * results are identical.  NE2B_EVQ=0 / 1, set when a net is created, turns
+ * the queues off / on for that net regardless of its size. */
 enum { NE2B_KERNEL_AUTO = 0, NE2B_KERNEL_STREAM = 1, NE2B_KERNEL_RESIDENT = 2 };
 ne2b_status ne2b_set_kernel_mode(ne2b_sim *sim, int32_t mode);
 ne2b_status ne2b_kernel_mode(ne2b_sim *sim, int32_t *mode, int32_t *resident);

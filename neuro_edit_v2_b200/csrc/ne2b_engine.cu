@@ -343,6 +343,15 @@ ne2b_status Stager::close() {
     return NE2B_OK;
 }
 
+// Event queues pay where the ring misses L2: a net's ring of at least this
+// many bytes uses them.  NE2B_EVQ=0 / 1 turns them off / on for every net.
+constexpr uint64_t kEvqMinRingBytes = 128ull << 20;
+static bool evq_wanted(uint64_t ring_bytes) {
+    const char *e = getenv("NE2B_EVQ");
+    if (e && *e) return e[0] == '1';
+    return ring_bytes >= kEvqMinRingBytes;
+}
+
 static double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -726,9 +735,20 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         d.trace_last = (uint32_t)tab.size() - 1;
     }
     fill_noise(d, *cfg);
+    // event queues for a ring too large for L2 (custom-tau nets keep the
+    // direct adds): D buckets of n_pad events, room for one arrival per
+    // neuron per step (~100 Hz at 100 synapses per neuron); an append past
+    // that is added into the ring directly
+    const bool use_evq = !h->nx && h->e > 0 && h->D >= 3 && evq_wanted((uint64_t)h->D * np * 4u);
+    if (use_evq) {
+        d.evq_cap = np;
+        NET_TRY(alloc(&p, sizeof(uint2) * (size_t)h->D * np)); d.evq = (uint2 *)p;
+        NET_TRY(alloc(&p, sizeof(uint32_t) * h->D)); d.evq_cnt = (uint32_t *)p;
+        NET_TRY(cuda_error(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h->D, bst), "memset event queues"));
+    }
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
               (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u) | (h->nx ? kNetXsyn : 0u) |
-              (d.trace_f ? kNetTraceF32 : 0u);
+              (d.trace_f ? kNetTraceF32 : 0u) | (use_evq ? kNetEvq : 0u);
     tp[5] = now_ms();
     // initial state (cpu.rs:158-183), on the build stream
     NET_TRY(cuda_error(launch_reset_neurons(d, bst), "reset kernel"));
@@ -970,6 +990,7 @@ ne2b_status Engine::reset_net(uint32_t slot) {
         NE2B_CUDA(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h.nx, stream_));
         NE2B_CUDA(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h.D * d.xwords, stream_));
     }
+    if (d.evq_cnt) NE2B_CUDA(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h.D, stream_));  // queues emptied
     // cpu.rs:176-183: the watch history and the grid marks start over
     h.watch_t0 = 0;
     if (d.gw_ls) NE2B_CUDA(cudaMemsetAsync(d.gw_ls, 0xFF, sizeof(uint32_t) * std::max<uint32_t>(h.gw_ptr.back(), 1), stream_));
@@ -1427,6 +1448,8 @@ ne2b_status Engine::snapshot(EngineSnapshot &snap) {
         NE2B_TRY(grab(d.watch_ring, d.watch_ring ? 8 * (size_t)d.watch_n * kWatchCap : 0));
         NE2B_TRY(grab(d.gw_ls, d.gw_ls ? 4 * (size_t)std::max<uint32_t>(h->gw_ptr.back(), 1) : 0));
         NE2B_TRY(grab(d.xpend, 4 * (size_t)h->D * d.xwords));
+        NE2B_TRY(grab(d.evq_cnt, d.evq_cnt ? 4 * (size_t)h->D : 0));
+        NE2B_TRY(grab(d.evq, d.evq ? sizeof(uint2) * (size_t)h->D * d.evq_cap : 0));
         snap.hosts.push_back({h->slot, h->t, h->dev});
     }
     return NE2B_OK;

@@ -16,8 +16,14 @@
 //   stimulus: neuron-major (input, weight) rows and a [steps x n_inputs] f32
 //     value buffer; spike record: rows x n_pad/32 u32 words; window counts:
 //     max_windows x n_pad u16.
+//   event queues (nets whose ring is too large for L2): D buckets of
+//     evq_cap events {target, weight bits} and D append counters; bucket b
+//     holds the arrivals due at steps = b (mod D) delivered with a delay of
+//     2 or more, appended in order of arrival and added into ring slot b by
+//     the step before it is read.
 #pragma once
 #include <stdint.h>
+#include <vector_types.h>  // uint2
 
 namespace ne2b {
 
@@ -35,6 +41,7 @@ enum NetFlags : uint32_t {
     kNetWatch = 1u << 7,    // watched neurons record their state every step
     kNetGridWatch = 1u << 8,  // grid groups record each member's last spike step
     kNetTraceF32 = 1u << 9,   // readout trace kept as f32 (its step table would be too long)
+    kNetEvq = 1u << 10,       // delays >= 2 are queued per arrival step (event queues), not added into the ring
 };
 
 enum TileFlags : uint32_t {
@@ -106,6 +113,11 @@ struct alignas(16) NetDev {
     const uint32_t *gw_off;     // [gw_n + 1] group ranges in gw_ls
     uint32_t *gw_ls;            // last spike step per texel (min(t, 2^32-2)), kNeverSpiked
     uint32_t watch_n, gw_n;
+    // event queues (kNetEvq only)
+    uint2 *evq;                 // [D x evq_cap] bucket b's events {target, weight bits}
+    uint32_t *evq_cnt;          // [D] appends to bucket b since it was last drained (may pass evq_cap:
+                                // an append past the cap adds straight into the ring)
+    uint32_t evq_cap, evq_pad[3];
     // scalars
     unsigned long long t;       // step index of the next launch group's k = 0
     unsigned long long t_end;   // steps at or beyond this are skipped (serving)

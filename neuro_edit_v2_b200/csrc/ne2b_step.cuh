@@ -21,6 +21,20 @@
 //      ring[(t + delay) % D][tgt] per synapse (cpu.rs:264-278,
 //      kernels.rs:174-204).
 //
+// Event queues (kNetEvq: nets whose D-slot ring does not fit in L2).  A
+// random add into a ring of hundreds of MB costs a DRAM read and write of a
+// 32-byte sector per event; instead, an arrival with delay d >= 2 is
+// appended as {target, weight} to bucket (t + d) % D (a returning atomic on
+// the bucket's counter, then an 8-byte store: the appends of a step to one
+// bucket fill consecutive entries, so they reach DRAM as whole sectors),
+// and during step t - 1 the net's tiles add bucket t's events into ring
+// slot t, which is in L2 then (it is also the slot prefetched for the next
+// step).  Bucket t is complete by then: its last appends came from step
+// t - 2 (delay 2); delay-1 arrivals are added straight into the ring.  The
+// counter of bucket t is reset during step t, when nothing appends to it.
+// Integer sums do not depend on the order of the adds, so rasters and
+// state are the direct path's bit for bit.
+//
 // Within a step no cross-block ordering is needed: step t reads slot t % D and
 // every delivery of step t lands in slot (t + d) % D, 1 <= d < D.  Between
 // steps, step t's deliveries must land before step t+1 reads:
@@ -147,6 +161,26 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             if (rel >= 0 && rel < (long long)nd.stim_len)
                 for (uint32_t c = threadIdx.x * 8u; c < nd.n_inputs; c += BLOCK * 8u)
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(nd.stim_buf + (size_t)rel * nd.n_inputs + c));
+        }
+    }
+
+    // ---- event queues: this tile's slice of bucket t + 1 into ring slot
+    // t + 1 (read by the next launch); bucket t's counter starts over
+    const bool evq = (flags & kNetEvq) != 0u;
+    const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;
+    if (evq) {
+        constexpr uint32_t kTile = BLOCK * NPT;
+        if (tile.start == 0u && threadIdx.x == 0u) nd.evq_cnt[tmod] = 0u;
+        const uint32_t c = RES ? __ldcg(nd.evq_cnt + b1) : nd.evq_cnt[b1];
+        const uint32_t qn = c < nd.evq_cap ? c : nd.evq_cap;
+        const uint32_t per = (qn + (n_pad + kTile - 1) / kTile - 1) / ((n_pad + kTile - 1) / kTile);
+        const uint32_t lo = (tile.start / kTile) * per, hi = lo + per < qn ? lo + per : qn;
+        const uint2 *q = nd.evq + (size_t)b1 * nd.evq_cap;
+        for (uint32_t e = lo + threadIdx.x; e < hi; e += BLOCK) {
+            const uint2 ev = RES ? __ldcg(q + e) : q[e];
+            const size_t idx = (size_t)b1 * n_pad + ev.x;
+            if (INT) atomicAdd((int *)ringw + idx, (int)ev.y);
+            else atomicAdd((float *)ringw + idx, __uint_as_float(ev.y));
         }
     }
 
@@ -392,7 +426,18 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             }
 #pragma unroll
             for (int q = 0; q < U; ++q)
-                if (f + q * BLOCK < nsyn) add(sl_[q], tg[q], wb[q]);
+                if (f + q * BLOCK < nsyn) {
+                    // event queues: delays >= 2 are appended to their
+                    // bucket (past its cap, added into the ring as below)
+                    if (evq && sl_[q] != b1) {
+                        const uint32_t pos = atomicAdd(nd.evq_cnt + sl_[q], 1u);
+                        if (pos < nd.evq_cap) {
+                            nd.evq[(size_t)sl_[q] * nd.evq_cap + pos] = make_uint2(tg[q], wb[q]);
+                            continue;
+                        }
+                    }
+                    add(sl_[q], tg[q], wb[q]);
+                }
         }
         __syncthreads();  // the next tile reuses the shared lists
         return;

@@ -344,11 +344,13 @@ ne2b_status Stager::close() {
 }
 
 // Event queues pay where the ring misses L2: a net's ring of at least this
-// many bytes uses them.  NE2B_EVQ=0 / 1 turns them off / on for every net.
+// many bytes uses them, unless the engine decides for all its nets (mode 0
+// / 1).  NE2B_EVQ=0 / 1 turns them off / on for every net.
 constexpr uint64_t kEvqMinRingBytes = 128ull << 20;
-static bool evq_wanted(uint64_t ring_bytes) {
+static bool evq_wanted(uint64_t ring_bytes, int mode) {
     const char *e = getenv("NE2B_EVQ");
     if (e && *e) return e[0] == '1';
+    if (mode >= 0) return mode == 1;
     return ring_bytes >= kEvqMinRingBytes;
 }
 
@@ -739,7 +741,7 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     // direct adds): D buckets of n_pad events, room for one arrival per
     // neuron per step (~100 Hz at 100 synapses per neuron); an append past
     // that is added into the ring directly
-    const bool use_evq = !h->nx && h->e > 0 && h->D >= 3 && evq_wanted((uint64_t)h->D * np * 4u);
+    const bool use_evq = !h->nx && h->e > 0 && h->D >= 3 && evq_wanted((uint64_t)h->D * np * 4u, evq_mode);
     if (use_evq) {
         d.evq_cap = np;
         NET_TRY(alloc(&p, sizeof(uint2) * (size_t)h->D * np)); d.evq = (uint2 *)p;

@@ -221,6 +221,7 @@ class Engine {
     ne2b_status set_mode(int m);
     bool fixed_grid = false;  // grid independent of the tile count (serving)
     bool multi_net = false;   // many nets (batch, server): the streaming kernel stages tiles ahead
+    int evq_mode = -1;        // event queues for nets built from now on: -1 by the net's ring size, 0 off, 1 on
     uint32_t graph_steps = 256;
     uint32_t resident_steps = 4096;  // max steps per resident launch
     uint64_t stim_chunk = 2048;

@@ -743,10 +743,11 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     // that is added into the ring directly
     const bool use_evq = !h->nx && h->e > 0 && h->D >= 3 && evq_wanted((uint64_t)h->D * np * 4u, evq_mode);
     if (use_evq) {
-        d.evq_cap = np;
+        d.evq_nseg = np / kNeuronAlign;  // tiles are at least 64 neurons
         NET_TRY(alloc(&p, sizeof(uint2) * (size_t)h->D * np)); d.evq = (uint2 *)p;
-        NET_TRY(alloc(&p, sizeof(uint32_t) * h->D)); d.evq_cnt = (uint32_t *)p;
-        NET_TRY(cuda_error(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h->D, bst), "memset event queues"));
+        NET_TRY(alloc(&p, sizeof(uint32_t) * h->D * (size_t)d.evq_nseg)); d.evq_cnt = (uint32_t *)p;
+        NET_TRY(cuda_error(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h->D * (size_t)d.evq_nseg, bst),
+                           "memset event queues"));
     }
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
               (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u) | (h->nx ? kNetXsyn : 0u) |
@@ -968,9 +969,23 @@ ne2b_status Engine::set_mode(int m) {
     return st;
 }
 
+// Event-queue segments belong to tile positions: drain them into the ring
+// (for the tile size they were filled under) before the tile size changes
+// or a snapshot is taken.
+ne2b_status Engine::flush_queues() {
+    const uint32_t tile = shape_.block * shape_.npt;
+    for (NetHost *h : nets_) {
+        if (!h || !h->dev.evq) continue;
+        NE2B_CUDA(launch_evq_flush(h->dev, int_ring_, tile, stream_));
+        launches_ += 1;
+    }
+    return NE2B_OK;
+}
+
 ne2b_status Engine::set_shape(const TileShape &s) {
     if (!shape_supported(s.block, s.npt))
         return set_error(NE2B_EINVAL, "tile shape block=%u npt=%u is not compiled in", s.block, s.npt);
+    if (s.block * s.npt != shape_.block * shape_.npt) NE2B_TRY(flush_queues());
     NE2B_CUDA(cudaStreamSynchronize(stream_));
     shape_ = s;
     clear_graphs();
@@ -992,7 +1007,8 @@ ne2b_status Engine::reset_net(uint32_t slot) {
         NE2B_CUDA(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h.nx, stream_));
         NE2B_CUDA(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h.D * d.xwords, stream_));
     }
-    if (d.evq_cnt) NE2B_CUDA(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h.D, stream_));  // queues emptied
+    if (d.evq_cnt)  // queues emptied
+        NE2B_CUDA(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h.D * (size_t)d.evq_nseg, stream_));
     // cpu.rs:176-183: the watch history and the grid marks start over
     h.watch_t0 = 0;
     if (d.gw_ls) NE2B_CUDA(cudaMemsetAsync(d.gw_ls, 0xFF, sizeof(uint32_t) * std::max<uint32_t>(h.gw_ptr.back(), 1), stream_));
@@ -1420,6 +1436,7 @@ ne2b_status Engine::grid_traces(NetHost &h, float tau_ms, float *out) {
 // Snapshot of every mutable device array (state, ring, record, windows,
 // descriptors, counters) in device memory, for the autotuner's trials.
 ne2b_status Engine::snapshot(EngineSnapshot &snap) {
+    NE2B_TRY(flush_queues());  // a restore may run under another tile size
     snap.items.clear();
     snap.hosts.clear();
     auto grab = [&](void *live, size_t bytes) -> ne2b_status {
@@ -1450,8 +1467,9 @@ ne2b_status Engine::snapshot(EngineSnapshot &snap) {
         NE2B_TRY(grab(d.watch_ring, d.watch_ring ? 8 * (size_t)d.watch_n * kWatchCap : 0));
         NE2B_TRY(grab(d.gw_ls, d.gw_ls ? 4 * (size_t)std::max<uint32_t>(h->gw_ptr.back(), 1) : 0));
         NE2B_TRY(grab(d.xpend, 4 * (size_t)h->D * d.xwords));
-        NE2B_TRY(grab(d.evq_cnt, d.evq_cnt ? 4 * (size_t)h->D : 0));
-        NE2B_TRY(grab(d.evq, d.evq ? sizeof(uint2) * (size_t)h->D * d.evq_cap : 0));
+        // the event queues are drained before a snapshot (flush_queues):
+        // their counters, all zero, are the whole of their state
+        NE2B_TRY(grab(d.evq_cnt, d.evq_cnt ? 4 * (size_t)h->D * d.evq_nseg : 0));
         snap.hosts.push_back({h->slot, h->t, h->dev});
     }
     return NE2B_OK;

@@ -189,6 +189,7 @@ class Engine {
     ne2b_status read_f32(const float *dev, uint32_t n, float *out);
     ne2b_status read_trace(NetHost &h, float *out);
     ne2b_status check_err();
+    ne2b_status flush_queues();  // event queues into the ring (before a tile-size change or a snapshot)
     ne2b_status spike_counts(NetHost &h, uint64_t rows, uint32_t *out);
     ne2b_status spike_row(NetHost &h, uint32_t back, uint64_t *out);
     ne2b_status spikes_total(NetHost &h, uint64_t *out);

@@ -64,6 +64,29 @@ __global__ void pn_total_kernel(const unsigned long long *pn, uint32_t n, uint32
     out[i] = c > 0xffffffffull ? 0xffffffffu : (uint32_t)c;
 }
 
+// Event queues: add every segment of every bucket into its ring slot and
+// empty it (the segments of tile size `tile`), so the queues can be refilled
+// under another tile size.  Pending arrivals reach their slots early, which
+// changes nothing: the slot of bucket b is next read at the step they are due.
+template <bool INT>
+__global__ void evq_flush_kernel(NetDev nd, uint32_t tile) {
+    const uint32_t nseg = (nd.n_pad + tile - 1) / tile;
+    for (uint32_t s = blockIdx.x; s < nseg * nd.D; s += gridDim.x) {
+        const uint32_t b = s / nseg, k = s - b * nseg;
+        const uint32_t cnt = nd.evq_cnt[(size_t)b * nd.evq_nseg + k];
+        const uint32_t size = nd.n_pad - k * tile < tile ? nd.n_pad - k * tile : tile;
+        const uint32_t ne = cnt < size ? cnt : size;
+        const uint2 *q = nd.evq + (size_t)b * nd.n_pad + (size_t)k * tile;
+        for (uint32_t e = threadIdx.x; e < ne; e += blockDim.x) {
+            const size_t idx = (size_t)b * nd.n_pad + q[e].x;
+            if (INT) atomicAdd((int *)nd.ring + idx, (int)q[e].y);
+            else atomicAdd((float *)nd.ring + idx, __uint_as_float(q[e].y));
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) nd.evq_cnt[(size_t)b * nd.evq_nseg + k] = 0u;
+    }
+}
+
 // Self-test of the bounded grid barrier: every block but `absent` arrives,
 // so the others give up after `limit_ns`, set the error flag and return
 // (a wait that cannot end, ended by its limit, with no fault).
@@ -134,6 +157,15 @@ cudaError_t launch_barrier_selftest(unsigned int *counter, unsigned int *err, ui
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st) {
     if (n_nets == 0) return cudaSuccess;
     return launch_pdl(advance_kernel, (n_nets + 127) / 128, 128, st, true, nets, n_nets, steps);
+}
+
+cudaError_t launch_evq_flush(const NetDev &nd, bool int_ring, uint32_t tile, cudaStream_t st) {
+    if (!nd.evq || tile == 0) return cudaSuccess;
+    const uint32_t segs = (nd.n_pad + tile - 1) / tile * nd.D;
+    const uint32_t grid = segs < 4096 ? segs : 4096;
+    if (int_ring) evq_flush_kernel<true><<<grid, 256, 0, st>>>(nd, tile);
+    else evq_flush_kernel<false><<<grid, 256, 0, st>>>(nd, tile);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st) {

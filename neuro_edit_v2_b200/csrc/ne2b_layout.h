@@ -16,11 +16,12 @@
 //   stimulus: neuron-major (input, weight) rows and a [steps x n_inputs] f32
 //     value buffer; spike record: rows x n_pad/32 u32 words; window counts:
 //     max_windows x n_pad u16.
-//   event queues (nets whose ring is too large for L2): D buckets of
-//     evq_cap events {target, weight bits} and D append counters; bucket b
-//     holds the arrivals due at steps = b (mod D) delivered with a delay of
-//     2 or more, appended in order of arrival and added into ring slot b by
-//     the step before it is read.
+//   event queues (nets whose ring is too large for L2): D buckets of n_pad
+//     events {target, weight bits}; bucket b holds the arrivals due at steps
+//     = b (mod D) delivered with a delay of 2 or more, in one segment per
+//     tile (the tile's neuron range of the bucket, with its own append
+//     counter), and is added into ring slot b by the step before it is
+//     read.
 #pragma once
 #include <stdint.h>
 #include <vector_types.h>  // uint2
@@ -114,10 +115,11 @@ struct alignas(16) NetDev {
     uint32_t *gw_ls;            // last spike step per texel (min(t, 2^32-2)), kNeverSpiked
     uint32_t watch_n, gw_n;
     // event queues (kNetEvq only)
-    uint2 *evq;                 // [D x evq_cap] bucket b's events {target, weight bits}
-    uint32_t *evq_cnt;          // [D] appends to bucket b since it was last drained (may pass evq_cap:
-                                // an append past the cap adds straight into the ring)
-    uint32_t evq_cap, evq_pad[3];
+    uint2 *evq;                 // [D x n_pad] {target, weight bits}; tile k's segment of bucket b is
+                                // [b * n_pad + k * tile, + the tile's neuron count)
+    uint32_t *evq_cnt;          // [D x evq_nseg] tile k's appends to bucket b at [b * evq_nseg + k] since
+                                // it was drained (may pass the segment's size: those added into the ring)
+    uint32_t evq_nseg, evq_pad[3];  // evq_nseg = n_pad / 64: segments at the smallest tile
     // scalars
     unsigned long long t;       // step index of the next launch group's k = 0
     unsigned long long t_end;   // steps at or beyond this are skipped (serving)

@@ -24,14 +24,18 @@
 // Event queues (kNetEvq: nets whose D-slot ring does not fit in L2).  A
 // random add into a ring of hundreds of MB costs a DRAM read and write of a
 // 32-byte sector per event; instead, an arrival with delay d >= 2 is
-// appended as {target, weight} to bucket (t + d) % D (a returning atomic on
-// the bucket's counter, then an 8-byte store: the appends of a step to one
-// bucket fill consecutive entries, so they reach DRAM as whole sectors),
-// and during step t - 1 the net's tiles add bucket t's events into ring
-// slot t, which is in L2 then (it is also the slot prefetched for the next
-// step).  Bucket t is complete by then: its last appends came from step
-// t - 2 (delay 2); delay-1 arrivals are added straight into the ring.  The
-// counter of bucket t is reset during step t, when nothing appends to it.
+// appended as {target, weight} to the delivering tile's segment of bucket
+// (t + d) % D (a returning atomic on that segment's counter, which only
+// this tile's block touches, so it is uncontended; then an 8-byte store:
+// a segment fills front to back, and the ~n/8 open fronts stay in L2 until
+// their sectors are whole), and during step t - 1 each tile adds its
+// segment of bucket t into ring slot t, which is in L2 then (it is also the
+// slot prefetched for the next step).  Bucket t is complete by then: its
+// last appends came from step t - 2 (delay 2); delay-1 arrivals, and
+// appends past a segment's size (one per neuron of the tile), are added
+// straight into the ring.  A segment's counter is reset during step t, when
+// nothing appends to bucket t.  Segments belong to tile positions, so the
+// host drains the queues into the ring before the tile size changes.
 // Integer sums do not depend on the order of the adds, so rasters and
 // state are the direct path's bit for bit.
 //
@@ -166,17 +170,14 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
 
     // ---- event queues: this tile's slice of bucket t + 1 into ring slot
     // t + 1 (read by the next launch); bucket t's counter starts over
-    const bool evq = (flags & kNetEvq) != 0u;
-    const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;
-    if (evq) {
-        constexpr uint32_t kTile = BLOCK * NPT;
-        if (tile.start == 0u && threadIdx.x == 0u) nd.evq_cnt[tmod] = 0u;
-        const uint32_t c = RES ? __ldcg(nd.evq_cnt + b1) : nd.evq_cnt[b1];
-        const uint32_t qn = c < nd.evq_cap ? c : nd.evq_cap;
-        const uint32_t per = (qn + (n_pad + kTile - 1) / kTile - 1) / ((n_pad + kTile - 1) / kTile);
-        const uint32_t lo = (tile.start / kTile) * per, hi = lo + per < qn ? lo + per : qn;
-        const uint2 *q = nd.evq + (size_t)b1 * nd.evq_cap;
-        for (uint32_t e = lo + threadIdx.x; e < hi; e += BLOCK) {
+    if (flags & kNetEvq) {
+        const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;
+        uint32_t *const seg_cnt = nd.evq_cnt + tile.start / (BLOCK * NPT);  // [b * evq_nseg]
+        if (threadIdx.x == 0u) seg_cnt[(size_t)tmod * nd.evq_nseg] = 0u;
+        const uint32_t c = RES ? __ldcg(seg_cnt + (size_t)b1 * nd.evq_nseg) : seg_cnt[(size_t)b1 * nd.evq_nseg];
+        const uint32_t ne = c < tile.count ? c : tile.count;
+        const uint2 *q = nd.evq + (size_t)b1 * n_pad + tile.start;
+        for (uint32_t e = threadIdx.x; e < ne; e += BLOCK) {
             const uint2 ev = RES ? __ldcg(q + e) : q[e];
             const size_t idx = (size_t)b1 * n_pad + ev.x;
             if (INT) atomicAdd((int *)ringw + idx, (int)ev.y);
@@ -386,6 +387,11 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     const uint32_t *__restrict__ tgt = nd.tgt;
     const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
     const bool d16 = flags & kNetDelay16;
+    // event queues: the next step's slot (delay 1: added at once) and this
+    // tile's append counters
+    const bool evq = (flags & kNetEvq) != 0u;
+    const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;
+    uint32_t *const seg_cnt = nd.evq_cnt + tile.start / (BLOCK * NPT);  // [b * evq_nseg]
     auto syn_at = [&](uint32_t f) {
         uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
         while (hi - lo > 1) {
@@ -430,9 +436,9 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
                     // event queues: delays >= 2 are appended to their
                     // bucket (past its cap, added into the ring as below)
                     if (evq && sl_[q] != b1) {
-                        const uint32_t pos = atomicAdd(nd.evq_cnt + sl_[q], 1u);
-                        if (pos < nd.evq_cap) {
-                            nd.evq[(size_t)sl_[q] * nd.evq_cap + pos] = make_uint2(tg[q], wb[q]);
+                        const uint32_t pos = atomicAdd(seg_cnt + (size_t)sl_[q] * nd.evq_nseg, 1u);
+                        if (pos < tile.count) {
+                            nd.evq[(size_t)sl_[q] * n_pad + tile.start + pos] = make_uint2(tg[q], wb[q]);
                             continue;
                         }
                     }

@@ -64,16 +64,19 @@ __global__ void pn_total_kernel(const unsigned long long *pn, uint32_t n, uint32
     out[i] = c > 0xffffffffull ? 0xffffffffu : (uint32_t)c;
 }
 
-// Event queues: add every segment of every bucket into its ring slot and
-// empty it (the segments of tile size `tile`), so the queues can be refilled
-// under another tile size.  Pending arrivals reach their slots early, which
-// changes nothing: the slot of bucket b is next read at the step they are due.
+// Event queues: add every segment of every pending bucket into its ring slot
+// and empty it (the segments of tile size `tile`), so the queues can be
+// refilled under another tile size.  Pending arrivals reach their slots
+// early, which changes nothing: the slot of bucket b is next read at the
+// step they are due.  Bucket tmod (the next step's) was added into its slot
+// during the last step and only awaits its counter reset: it is emptied
+// without adding.
 template <bool INT>
 __global__ void evq_flush_kernel(NetDev nd, uint32_t tile) {
     const uint32_t nseg = (nd.n_pad + tile - 1) / tile;
     for (uint32_t s = blockIdx.x; s < nseg * nd.D; s += gridDim.x) {
         const uint32_t b = s / nseg, k = s - b * nseg;
-        const uint32_t cnt = nd.evq_cnt[(size_t)b * nd.evq_nseg + k];
+        const uint32_t cnt = b == nd.tmod ? 0u : nd.evq_cnt[(size_t)b * nd.evq_nseg + k];
         const uint32_t size = nd.n_pad - k * tile < tile ? nd.n_pad - k * tile : tile;
         const uint32_t ne = cnt < size ? cnt : size;
         const uint2 *q = nd.evq + (size_t)b * nd.n_pad + (size_t)k * tile;

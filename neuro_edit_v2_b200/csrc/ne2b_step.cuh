@@ -74,82 +74,9 @@ struct SmemLists {
     uint32_t *woff;   // [warps] spike prefix per warp
     uint32_t *wsyn;   // [warps] synapse prefix per warp
     uint32_t *total;  // [2] spikes, synapses
-    uint32_t *seg;    // [tile size] row k's tile position in its net (its event-queue segment)
-    uint32_t *acc;    // [2] rows and synapses listed so far (batched delivery)
 };
 __device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, uint32_t nw) {
-    uint32_t *w = base + 2 * tile + 1;
-    return SmemLists{base, base + tile, w, w + nw, w + 2 * nw, w + 2 * nw + 2, w + 2 * nw + 2 + tile};
-}
-
-// Delivery of the listed rows (spikes of the step whose slot is tmod; nets
-// without custom-tau synapses): the block strides the flat synapse range; a
-// thread finds its row by binary search over off[], then adds the weight
-// into ring[(tmod + d) % D][tgt] with a no-return atomic, or (event queues,
-// delay >= 2) appends it to the row's tile segment of its bucket.  U
-// synapses per thread and pass, all their loads issued before any add, so
-// rows with more synapses than threads pay one round trip to the CSR per U
-// block-widths; a thread past the end repeats its first synapse's loads
-// (same lines; cheaper in registers than predicated loads) and skips the
-// add.  `tsize` is the tile size (segment k holds tile k's appends).  Ends
-// with a block barrier (the lists are reused).
-template <bool INT, int BLOCK>
-__device__ __forceinline__ void deliver_list(const NetDev &nd, const SmemLists &sl, uint32_t total, uint32_t nsyn,
-                                             uint32_t tmod, uint32_t tsize) {
-    const uint32_t *__restrict__ tgt = nd.tgt;
-    const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
-    uint32_t *__restrict__ ringw = (uint32_t *)nd.ring;
-    const uint32_t D = nd.D, n_pad = nd.n_pad;
-    const bool d16 = nd.flags & kNetDelay16;
-    const bool evq = (nd.flags & kNetEvq) != 0u;
-    const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;  // delay 1: added at once
-    auto row_of = [&](uint32_t f) {
-        uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (sl.off[mid] <= f) lo = mid;
-            else hi = mid;
-        }
-        return lo;
-    };
-    constexpr int U = kDeliverUnroll<INT>;
-    for (uint32_t f = threadIdx.x; f < nsyn; f += U * BLOCK) {
-        uint32_t r[U], j[U], tg[U], sl_[U], wb[U];
-        r[0] = row_of(f);
-#pragma unroll
-        for (int q = 1; q < U; ++q) r[q] = f + q * BLOCK < nsyn ? row_of(f + q * BLOCK) : r[0];
-#pragma unroll
-        for (int q = 0; q < U; ++q) {
-            const uint32_t fq = f + q * BLOCK < nsyn ? f + q * BLOCK : f;
-            j[q] = sl.lo[r[q]] + (fq - sl.off[r[q]]);
-        }
-#pragma unroll
-        for (int q = 0; q < U; ++q) {
-            tg[q] = tgt[j[q]];
-            const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j[q]] : (uint32_t)((const uint8_t *)nd.delay)[j[q]];
-            sl_[q] = tmod + d >= D ? tmod + d - D : tmod + d;
-            wb[q] = wbits[j[q]];
-        }
-#pragma unroll
-        for (int q = 0; q < U; ++q)
-            if (f + q * BLOCK < nsyn) {
-                if (evq && sl_[q] != b1) {
-                    // the row's tile segment of the bucket; past its size
-                    // (the tile's neuron count), added into the ring
-                    const uint32_t k = sl.seg[r[q]];
-                    const uint32_t size = n_pad - k * tsize < tsize ? n_pad - k * tsize : tsize;
-                    const uint32_t pos = atomicAdd(nd.evq_cnt + (size_t)sl_[q] * nd.evq_nseg + k, 1u);
-                    if (pos < size) {
-                        nd.evq[(size_t)sl_[q] * n_pad + (size_t)k * tsize + pos] = make_uint2(tg[q], wb[q]);
-                        continue;
-                    }
-                }
-                const size_t idx = (size_t)sl_[q] * n_pad + tg[q];
-                if (INT) atomicAdd((int *)ringw + idx, (int)wb[q]);
-                else atomicAdd((float *)ringw + idx, __uint_as_float(wb[q]));
-            }
-    }
-    __syncthreads();
+    return SmemLists{base, base + tile, base + 2 * tile + 1, base + 2 * tile + 1 + nw, base + 2 * tile + 1 + 2 * nw};
 }
 
 // `nd` is the tile's net descriptor (global memory, or a shared-memory copy
@@ -164,11 +91,7 @@ __device__ __forceinline__ void deliver_list(const NetDev &nd, const SmemLists &
 // trace or watches; NOIO: nor an external current, a stimulus or windows.
 // Their code is compiled out (the engine launches such an instance only
 // then).
-// BATCH: the caller (the single-net streaming kernel) delivers the block's
-// listed rows once, after its last tile; this tile's rows are appended to
-// the list (which is delivered first if they would not fit).
-template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool LEAN = false, bool NOIO = false,
-          bool BATCH = false>
+template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool LEAN = false, bool NOIO = false>
 __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
                                              const Tile &tile, uint64_t t, uint32_t tmod, uint32_t k, float *vs, float *us,
                                              float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
@@ -442,56 +365,33 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         }
     }
     __syncthreads();
-    // batched: the rows go after those already listed by this block's
-    // earlier tiles of the step (the list is delivered first when it would
-    // overflow); otherwise the list starts empty
-    uint32_t base_s = 0, base_y = 0;
-    if (BATCH && !xsyn_on) {
-        base_s = sl.acc[0];
-        base_y = sl.acc[1];
-        if (base_s + sl.total[0] > (uint32_t)(BLOCK * NPT)) {
-            if (threadIdx.x == 0) sl.off[base_s] = base_y;
-            __syncthreads();
-            deliver_list<INT, BLOCK>(nd, sl, base_s, base_y, tmod, BLOCK * NPT);
-            base_s = base_y = 0;
-        }
-    }
     {
-        uint32_t pos = base_s + sl.woff[warp] + ic - cnt;
-        uint32_t so = base_y + sl.wsyn[warp] + is - syn;
-        const uint32_t k = tile.start / (BLOCK * NPT);
+        uint32_t pos = sl.woff[warp] + ic - cnt;
+        uint32_t so = sl.wsyn[warp] + is - syn;
 #pragma unroll
         for (int q = 0; q < NPT; ++q)
             if (spk[q]) {
                 sl.lo[pos] = rlo[q];
                 sl.off[pos] = so;
-                sl.seg[pos] = k;
                 ++pos;
                 so += rhi[q] - rlo[q];
             }
     }
-    const uint32_t total = base_s + sl.total[0], nsyn = base_y + sl.total[1];
-    if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)sl.total[0]);
-    if (BATCH && !xsyn_on) {
-        __syncthreads();  // every thread has read acc and total
-        if (threadIdx.x == 0) {
-            sl.acc[0] = total;
-            sl.acc[1] = nsyn;
-        }
-        __syncthreads();
-        return;
-    }
+    const uint32_t total = sl.total[0], nsyn = sl.total[1];
     if (threadIdx.x == 0) sl.off[total] = nsyn;
     __syncthreads();
-    if (!xsyn_on) {
-        deliver_list<INT, BLOCK>(nd, sl, total, nsyn, tmod, BLOCK * NPT);
-        return;
-    }
-    // ---- custom-tau nets: the block strides the flat synapse range, one
-    // synapse per thread and pass
+    if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
+    // ---- delivery: the block strides the flat synapse range; a thread
+    // finds its row by binary search over off[], then adds the weight into
+    // ring[(t + d) % D][tgt] with a no-return atomic
     const uint32_t *__restrict__ tgt = nd.tgt;
     const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
     const bool d16 = flags & kNetDelay16;
+    // event queues: the next step's slot (delay 1: added at once) and this
+    // tile's append counters
+    const bool evq = (flags & kNetEvq) != 0u;
+    const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;
+    uint32_t *const seg_cnt = nd.evq_cnt + tile.start / (BLOCK * NPT);  // [b * evq_nseg]
     auto syn_at = [&](uint32_t f) {
         uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
         while (hi - lo > 1) {
@@ -511,6 +411,43 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         if (INT) atomicAdd((int *)ringw + idx, (int)wb);
         else atomicAdd((float *)ringw + idx, __uint_as_float(wb));
     };
+    if (!xsyn_on) {
+        // U synapses per thread and pass, all their loads issued before any
+        // add, so a tile with more synapses than threads pays one round trip
+        // to the CSR per U block-widths
+        constexpr int U = kDeliverUnroll<INT>;
+        for (uint32_t f = threadIdx.x; f < nsyn; f += U * BLOCK) {
+            // a thread past the end repeats its first synapse's loads (same
+            // lines; cheaper in registers than predicated loads) and skips
+            // the add
+            uint32_t j[U], tg[U], sl_[U], wb[U];
+            j[0] = syn_at(f);
+#pragma unroll
+            for (int q = 1; q < U; ++q) j[q] = f + q * BLOCK < nsyn ? syn_at(f + q * BLOCK) : j[0];
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                tg[q] = tgt[j[q]];
+                sl_[q] = slot_of(j[q]);
+                wb[q] = wbits[j[q]];
+            }
+#pragma unroll
+            for (int q = 0; q < U; ++q)
+                if (f + q * BLOCK < nsyn) {
+                    // event queues: delays >= 2 are appended to their
+                    // bucket (past its cap, added into the ring as below)
+                    if (evq && sl_[q] != b1) {
+                        const uint32_t pos = atomicAdd(seg_cnt + (size_t)sl_[q] * nd.evq_nseg, 1u);
+                        if (pos < tile.count) {
+                            nd.evq[(size_t)sl_[q] * n_pad + tile.start + pos] = make_uint2(tg[q], wb[q]);
+                            continue;
+                        }
+                    }
+                    add(sl_[q], tg[q], wb[q]);
+                }
+        }
+        __syncthreads();  // the next tile reuses the shared lists
+        return;
+    }
     for (uint32_t f = threadIdx.x; f < nsyn; f += BLOCK) {
         const uint32_t j = syn_at(f);
         const uint32_t tg = tgt[j];
@@ -595,48 +532,32 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
     const SmemLists sl = smem_lists(s_lists, BLOCK * NPT, BLOCK / 32);
     const uint32_t n_tiles = eng->n_tiles;
     if constexpr (!MULTI) {
-        // the block's tiles list their spikes' rows as they go, and the
-        // block delivers them once, after its last tile (one delivery chain
-        // per block and step instead of one per spiking tile)
         uint32_t tix = blockIdx.x;
         if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
         Tile tile = eng->tiles[tix];
         stage_net(eng, tile.net, &s_nd);
         const ParamRow *ptab = stage_params<BLOCK>(eng, s_ptab);
-        if (threadIdx.x == 0) sl.acc[0] = sl.acc[1] = 0u;
         __syncthreads();
         pdl_wait();
-        auto deliver_listed = [&]() {  // every thread; ends with a barrier
-            __syncthreads();
-            const uint32_t ns = sl.acc[0], ny = sl.acc[1];
-            if (ns == 0u) return;
-            uint32_t tmod = s_nd.tmod + k_step;
-            if (tmod >= s_nd.D) tmod %= s_nd.D;
-            if (threadIdx.x == 0) sl.off[ns] = ny;
-            __syncthreads();
-            deliver_list<INT, BLOCK>(s_nd, sl, ns, ny, tmod, BLOCK * NPT);
-            if (threadIdx.x == 0) sl.acc[0] = sl.acc[1] = 0u;
-            __syncthreads();
-        };
         for (;;) {
             const uint32_t nx = tix + gridDim.x;
             const uint64_t t = s_nd.t + k_step;
             uint32_t tmod = s_nd.tmod + k_step;
             if (tmod >= s_nd.D) tmod %= s_nd.D;
-            process_tile<INT, BLOCK, NPT, false, ADEX, false, PLAIN, PLAIN, true>(
-                eng, ptab, s_nd, tile, t, tmod, k_step, s_nd.v + tile.start, s_nd.u + tile.start,
-                s_nd.s + tile.start, s_nd.tk + tile.start, s_nd.pidx + tile.start, sl);
+            process_tile<INT, BLOCK, NPT, false, ADEX, false, PLAIN, PLAIN>(eng, ptab, s_nd, tile, t, tmod, k_step,
+                                                             s_nd.v + tile.start, s_nd.u + tile.start,
+                                                             s_nd.s + tile.start, s_nd.tk + tile.start,
+                                                             s_nd.pidx + tile.start, sl);
             if (nx >= n_tiles) break;
             const Tile next = eng->tiles[nx];
             if (next.net != tile.net) {
-                deliver_listed();  // the list belongs to this net
+                __syncthreads();  // every thread is done with the staged descriptor
                 stage_net(eng, next.net, &s_nd);
                 __syncthreads();
             }
             tix = nx;
             tile = next;
         }
-        deliver_listed();
     } else {
         __shared__ __align__(16) NetDev s_stage[kStageTiles];  // slot j: tile j's net, where it changes
         __shared__ __align__(16) Tile s_tile[kStageTiles];

@@ -20,7 +20,7 @@ bool pdl_enabled();  // programmatic dependent launch of the streaming kernels (
 // 32-bit words of the delivery phase's shared lists (SmemLists).
 template <int BLOCK, int NPT>
 __host__ __device__ constexpr uint32_t smem_lists_words() {
-    return 3 * BLOCK * NPT + 1 + 2 * (BLOCK / 32) + 4;
+    return 2 * BLOCK * NPT + 1 + 2 * (BLOCK / 32) + 2;
 }
 
 // Resident kernel shared memory: [delivery lists][flag u32], 16-byte aligned,

@@ -146,6 +146,10 @@ ne2b_status Engine::init(int device, bool int_ring, uint32_t max_nets) {
     NE2B_CUDA(cudaMemset(d_barrier_, 0, 2 * sizeof(unsigned int)));
     d_err_ = d_barrier_ + 1;
     if (const char *pdl = getenv("NE2B_PDL")) set_pdl(strcmp(pdl, "0") != 0);
+    if (const char *sp = getenv("NE2B_SPLIT")) {
+        if (*sp) split_env_ = sp[0] == '1' ? 1 : 0;
+        split_ = split_env_ == 1;
+    }
     if (const char *m = getenv("NE2B_KERNEL")) {
         if (!strcmp(m, "stream")) mode_ = kModeStream;
         else if (!strcmp(m, "resident")) mode_ = kModeResident;
@@ -167,6 +171,8 @@ ne2b_status Engine::upload_eng() {
     e.n_params = ptab_rows_dev_;
     e.barrier = d_barrier_;
     e.err = d_err_;
+    e.split = split_ ? 1u : 0u;
+    e.pad_[0] = e.pad_[1] = e.pad_[2] = 0u;
     // pageable source: the runtime copies it to staging before returning, so
     // the stack frame may go away without waiting for the device
     NE2B_CUDA(cudaMemcpyAsync(d_eng_, &e, sizeof e, cudaMemcpyHostToDevice, stream_));
@@ -749,6 +755,13 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         NET_TRY(cuda_error(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h->D * (size_t)d.evq_nseg, bst),
                            "memset event queues"));
     }
+    // split delivery lists (custom-tau nets deliver in the step kernel)
+    if (!h->nx && np) {
+        NET_TRY(alloc(&p, sizeof(uint32_t) * np)); d.spk_ids = (uint32_t *)p;
+        NET_TRY(alloc(&p, sizeof(uint32_t) * (np / kNeuronAlign))); d.spk_cnt = (uint32_t *)p;
+        NET_TRY(cuda_error(cudaMemsetAsync(d.spk_cnt, 0, sizeof(uint32_t) * (np / kNeuronAlign), bst),
+                           "memset spike lists"));
+    }
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
               (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u) | (h->nx ? kNetXsyn : 0u) |
               (d.trace_f ? kNetTraceF32 : 0u) | (use_evq ? kNetEvq : 0u);
@@ -1007,6 +1020,7 @@ ne2b_status Engine::reset_net(uint32_t slot) {
         NE2B_CUDA(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h.nx, stream_));
         NE2B_CUDA(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h.D * d.xwords, stream_));
     }
+    if (d.spk_cnt) NE2B_CUDA(cudaMemsetAsync(d.spk_cnt, 0, sizeof(uint32_t) * (h.n_pad / kNeuronAlign), stream_));
     if (d.evq_cnt)  // queues emptied
         NE2B_CUDA(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h.D * (size_t)d.evq_nseg, stream_));
     // cpu.rs:176-183: the watch history and the grid marks start over
@@ -1137,8 +1151,10 @@ ne2b_status Engine::launch_group(uint32_t steps) {
             cudaGraph_t gr;
             NE2B_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
             cudaError_t err = cudaSuccess;
-            for (uint32_t k = 0; k < steps && err == cudaSuccess; ++k)
+            for (uint32_t k = 0; k < steps && err == cudaSuccess; ++k) {
                 err = launch_step(int_ring_, adex_, var, shape_.block, shape_.npt, d_eng_, k, g, stream_);
+                if (err == cudaSuccess && split_) err = launch_split_delivery(k);
+            }
             if (err == cudaSuccess) err = launch_advance(d_nets_, nets_cap_, steps, stream_);
             cudaError_t e2 = cudaStreamEndCapture(stream_, &gr);
             if (err != cudaSuccess) return cuda_error(err, "step launch during capture");
@@ -1150,13 +1166,34 @@ ne2b_status Engine::launch_group(uint32_t steps) {
             it = graphs_.emplace(steps, ex).first;
         }
         NE2B_CUDA(cudaGraphLaunch(it->second, stream_));
-        launches_ += steps + 1;
+        launches_ += (split_ ? 2 * (uint64_t)steps : steps) + 1;
         return NE2B_OK;
     }
-    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, adex_, var, shape_.block, shape_.npt, d_eng_, k, g, stream_));
+    for (uint32_t k = 0; k < steps; ++k) {
+        NE2B_CUDA(launch_step(int_ring_, adex_, var, shape_.block, shape_.npt, d_eng_, k, g, stream_));
+        if (split_) NE2B_CUDA(launch_split_delivery(k));
+    }
     NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
-    launches_ += steps + 1;
+    launches_ += (split_ ? 2 * (uint64_t)steps : steps) + 1;
     return NE2B_OK;
+}
+
+// The delivery kernel of split delivery for step k of a launch group: one
+// warp per tile, as many blocks as the tiles need (8 warps each), at most
+// what the SMs hold at once.
+cudaError_t Engine::launch_split_delivery(uint32_t k) {
+    return launch_deliver(int_ring_, d_eng_, n_tiles_, k, shape_.block * shape_.npt, (uint32_t)sm_count_ * 8u, stream_);
+}
+
+// Split or fused delivery (resident launches always deliver themselves).
+// NE2B_SPLIT=0 / 1, read when the engine is created, fixes the choice.
+ne2b_status Engine::set_split(bool on) {
+    if (split_env_ >= 0) on = split_env_ == 1;
+    if (on == split_) return NE2B_OK;
+    NE2B_CUDA(cudaStreamSynchronize(stream_));  // every listed spike was delivered by its step's launch
+    split_ = on;
+    clear_graphs();
+    return upload_eng();
 }
 
 ne2b_status Engine::run_steps(uint64_t steps) {
@@ -1522,19 +1559,25 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
     const int saved_mode = mode_;
     TileShape best = shape_;
     int best_mode = mode_ == kModeAuto ? (resident_ ? kModeResident : kModeStream) : mode_;
+    bool best_split = split_;
     float best_ms = 1e30f;
     for (int m : {(int)kModeStream, (int)kModeResident}) {
         if (saved_mode != kModeAuto && m != saved_mode) continue;  // a forced kernel keeps its mode
         for (uint32_t c = 0; c < count; ++c) {
             const int occ = step_occupancy(int_ring_, adex_, step_variant(), blocks[c], npts[c]);
-            for (int half = 0; half < 2; ++half) {
+            for (int cand = 0; cand < 4; ++cand) {
+                const int half = cand & 1;
+                const bool sp = (cand >> 1) != 0;  // split delivery (streaming only)
                 if (half && (m == kModeResident || occ < 2)) continue;
+                if (sp && m == kModeResident) continue;
+                if (split_env_ >= 0 && sp != (split_env_ == 1)) continue;
                 TileShape s;
                 s.block = blocks[c];
                 s.npt = npts[c];
                 s.blocks_per_sm = half ? (uint32_t)std::max(1, occ / 2) : 0;
                 mode_ = m;
                 shape_ = s;
+                split_ = sp;
                 clear_graphs();
                 if (rebuild_tiles() != NE2B_OK) continue;  // resident plan does not fit
                 NE2B_TRY(restore(snap));
@@ -1555,12 +1598,14 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
                     best_ms = ms;
                     best = s;
                     best_mode = m;
+                    best_split = sp;
                 }
             }
         }
     }
     mode_ = saved_mode == kModeAuto ? best_mode : saved_mode;
     shape_ = best;
+    split_ = best_split;
     clear_graphs();
     NE2B_TRY(rebuild_tiles());
     NE2B_TRY(restore(snap));

@@ -190,6 +190,9 @@ class Engine {
     ne2b_status read_trace(NetHost &h, float *out);
     ne2b_status check_err();
     ne2b_status flush_queues();  // event queues into the ring (before a tile-size change or a snapshot)
+    ne2b_status set_split(bool on);  // split (step kernel + delivery kernel) or fused delivery
+    bool split() const { return split_; }
+    cudaError_t launch_split_delivery(uint32_t k);
     ne2b_status spike_counts(NetHost &h, uint64_t rows, uint32_t *out);
     ne2b_status spike_row(NetHost &h, uint32_t back, uint64_t *out);
     ne2b_status spikes_total(NetHost &h, uint64_t *out);
@@ -268,6 +271,8 @@ class Engine {
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     float last_ms_ = 0.0f;
     uint64_t launches_ = 0;  // kernels launched (graph nodes counted per replay)
+    bool split_ = false;     // split delivery (streaming launches only)
+    int split_env_ = -1;     // NE2B_SPLIT: -1 unset, else the fixed choice
     // resident kernel
     int mode_ = kModeAuto;
     bool resident_ = false;

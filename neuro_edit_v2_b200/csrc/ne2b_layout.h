@@ -120,6 +120,11 @@ struct alignas(16) NetDev {
     uint32_t *evq_cnt;          // [D x evq_nseg] tile k's appends to bucket b at [b * evq_nseg + k] since
                                 // it was drained (may pass the segment's size: those added into the ring)
     uint32_t evq_nseg, evq_pad[3];  // evq_nseg = n_pad / 64: segments at the smallest tile
+    // split delivery (nets without custom-tau synapses): the step kernel
+    // lists each tile's spiking neurons, the delivery kernel that follows it
+    // delivers them and empties the list
+    uint32_t *spk_ids;          // [n_pad] tile k's spiking neurons at [k * tile, + count)
+    uint32_t *spk_cnt;          // [n_pad / 64] tile k's count (0 when nothing is listed)
     // scalars
     unsigned long long t;       // step index of the next launch group's k = 0
     unsigned long long t_end;   // steps at or beyond this are skipped (serving)
@@ -176,6 +181,8 @@ struct EngineDev {
     uint32_t n_params;       // rows of ptab on the device
     unsigned int *barrier;   // grid-barrier arrival counter (zeroed before each launch)
     unsigned int *err;       // nonzero: a grid barrier timed out
+    uint32_t split;          // the streaming kernel lists spikes for the delivery kernel instead of delivering
+    uint32_t pad_[3];
 };
 
 }  // namespace ne2b

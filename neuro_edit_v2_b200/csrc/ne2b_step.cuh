@@ -39,6 +39,16 @@
 // Integer sums do not depend on the order of the adds, so rasters and
 // state are the direct path's bit for bit.
 //
+// Split delivery (EngineDev::split; nets without custom-tau synapses): the
+// streaming kernel only lists each tile's spiking neurons (ids at the
+// tile's range of spk_ids, the count in spk_cnt), and deliver_kernel, launched
+// right after it, delivers every listed spike with one warp per tile across
+// the whole GPU.  Fused, a block that walks several tiles pays one
+// dependent delivery chain (row bounds, scans, CSR loads, adds) per spiking
+// tile in sequence; split, the neuron pass ends at its ballots and all
+// chains run at once in one wave of warps, for one more launch per step.
+// The engine (autotune) picks whichever is faster for the workload.
+//
 // Within a step no cross-block ordering is needed: step t reads slot t % D and
 // every delivery of step t lands in slot (t + d) % D, 1 <= d < D.  Between
 // steps, step t's deliveries must land before step t+1 reads:
@@ -94,7 +104,8 @@ __device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, u
 template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool LEAN = false, bool NOIO = false>
 __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
                                              const Tile &tile, uint64_t t, uint32_t tmod, uint32_t k, float *vs, float *us,
-                                             float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
+                                             float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl,
+                                             bool split = false) {
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -270,8 +281,10 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         if (__float_as_uint(snew) != __float_as_uint(s[q])) ss[off] = snew;
         if (k != k0) tks[off] = (uint16_t)k;
         if (sp) {
-            rlo[q] = rowptr[i];
-            rhi[q] = rowptr[i + 1];
+            if (!split || xsyn_on) {  // split: the delivery kernel loads the row
+                rlo[q] = rowptr[i];
+                rhi[q] = rowptr[i + 1];
+            }
             nd.pn_total[i] += 1ull;
             if (!LEAN && (flags & kNetGridWatch)) {  // cpu.rs:293-304
                 const uint32_t t32 = t < 0xFFFFFFFEull ? (uint32_t)t : 0xFFFFFFFEu;
@@ -365,6 +378,18 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         }
     }
     __syncthreads();
+    if (split && !xsyn_on) {
+        // split delivery: list the tile's spiking neurons for deliver_kernel
+        uint32_t pos = sl.woff[warp] + ic - cnt;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q)
+            if (spk[q]) nd.spk_ids[tile.start + pos++] = li[q];
+        if (threadIdx.x == 0) {
+            nd.spk_cnt[tile.start / (BLOCK * NPT)] = sl.total[0];
+            atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)sl.total[0]);
+        }
+        return;  // the next tile writes the shared lists only after its first barrier
+    }
     {
         uint32_t pos = sl.woff[warp] + ic - cnt;
         uint32_t so = sl.wsyn[warp] + is - syn;
@@ -531,6 +556,7 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
     static_assert(kNetWords <= BLOCK && kStageTiles <= BLOCK, "one 16-byte word per thread");
     const SmemLists sl = smem_lists(s_lists, BLOCK * NPT, BLOCK / 32);
     const uint32_t n_tiles = eng->n_tiles;
+    const bool split = eng->split != 0u;
     if constexpr (!MULTI) {
         uint32_t tix = blockIdx.x;
         if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
@@ -547,7 +573,7 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
             process_tile<INT, BLOCK, NPT, false, ADEX, false, PLAIN, PLAIN>(eng, ptab, s_nd, tile, t, tmod, k_step,
                                                              s_nd.v + tile.start, s_nd.u + tile.start,
                                                              s_nd.s + tile.start, s_nd.tk + tile.start,
-                                                             s_nd.pidx + tile.start, sl);
+                                                             s_nd.pidx + tile.start, sl, split);
             if (nx >= n_tiles) break;
             const Tile next = eng->tiles[nx];
             if (next.net != tile.net) {
@@ -598,7 +624,7 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
             process_tile<INT, BLOCK, NPT, false, ADEX, true, PLAIN>(eng, ptab, s_nd, tile, t, tmod, k_step,
                                                             s_nd.v + tile.start, s_nd.u + tile.start,
                                                             s_nd.s + tile.start, s_nd.tk + tile.start,
-                                                            s_nd.pidx + tile.start, sl);
+                                                            s_nd.pidx + tile.start, sl, split);
         }
     }
 }

@@ -173,13 +173,7 @@ ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd);                 /* ne
  * streaming kernel; the other two force one (RESIDENT fails with
  * NE2B_UNSUPPORTED when the nets do not fit).  *resident reports which
  * kernel runs.  The environment variable NE2B_KERNEL=stream|resident sets
- * the initial mode of every handle.
- *
- * Delivery into a ring larger than 128 MB (D x n_pad x 4 bytes) goes through
- * per-step event queues (arrivals appended per arrival step, added into the
- * ring the step before they are read) instead of random adds into the ring;
- * results are identical.  NE2B_EVQ=0 / 1, set when a net is created, turns
- * the queues off / on for that net regardless of its size. */
+ * the initial mode of every handle. */
 enum { NE2B_KERNEL_AUTO = 0, NE2B_KERNEL_STREAM = 1, NE2B_KERNEL_RESIDENT = 2 };
 ne2b_status ne2b_set_kernel_mode(ne2b_sim *sim, int32_t mode);
 ne2b_status ne2b_kernel_mode(ne2b_sim *sim, int32_t *mode, int32_t *resident);
@@ -194,13 +188,6 @@ ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *neurons_pe
                             uint32_t *blocks_per_sm);
 ne2b_status ne2b_set_tile_shape(ne2b_sim *sim, uint32_t block, uint32_t neurons_per_thread,
                                 uint32_t blocks_per_sm);
-/* Delivery (new): fused (0: each tile of the streaming kernel delivers its
- * spikes itself) or split (1: the streaming kernel lists them and a second
- * kernel per step delivers them, one warp per tile across the GPU).  Results
- * are identical; autotune picks the faster; the environment variable
- * NE2B_SPLIT=0|1 fixes the choice for every handle created while it is set. */
-ne2b_status ne2b_split_delivery(ne2b_sim *sim, int32_t *split);
-ne2b_status ne2b_set_split_delivery(ne2b_sim *sim, int32_t split);
 
 /* Instrumentation (new): the CUDA stream the handle launches on (a
  * cudaStream_t, for timing with events on the launching stream) and the
@@ -252,8 +239,6 @@ ne2b_status ne2b_batch_tile_shape(ne2b_batch *b, uint32_t *block, uint32_t *neur
                                   uint32_t *blocks_per_sm);
 ne2b_status ne2b_batch_set_tile_shape(ne2b_batch *b, uint32_t block, uint32_t neurons_per_thread,
                                       uint32_t blocks_per_sm);
-ne2b_status ne2b_batch_split_delivery(ne2b_batch *b, int32_t *split);
-ne2b_status ne2b_batch_set_split_delivery(ne2b_batch *b, int32_t split);
 ne2b_status ne2b_batch_dev_mem_bytes(ne2b_batch *b, uint64_t *bytes);
 ne2b_status ne2b_batch_last_step_ms(ne2b_batch *b, float *ms);
 ne2b_status ne2b_batch_set_kernel_mode(ne2b_batch *b, int32_t mode);

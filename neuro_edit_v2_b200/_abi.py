@@ -177,10 +177,6 @@ _SIGS = {
     "ne2b_batch_kernel_mode": (C.c_int, [_p, C.POINTER(_i32), C.POINTER(_i32)]),
     "ne2b_autotune": (C.c_int, [_p, _u32]),
     "ne2b_tile_shape": (C.c_int, [_p, _pu32, _pu32, _pu32]),
-    "ne2b_split_delivery": (C.c_int, [_p, C.POINTER(C.c_int32)]),
-    "ne2b_set_split_delivery": (C.c_int, [_p, _i32]),
-    "ne2b_batch_split_delivery": (C.c_int, [_p, C.POINTER(C.c_int32)]),
-    "ne2b_batch_set_split_delivery": (C.c_int, [_p, _i32]),
     "ne2b_set_tile_shape": (C.c_int, [_p, _u32, _u32, _u32]),
     "ne2b_stream": (C.c_int, [_p, C.POINTER(_p)]),
     "ne2b_kernel_launches": (C.c_int, [_p, _pu64]),

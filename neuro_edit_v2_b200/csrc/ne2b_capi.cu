@@ -465,17 +465,6 @@ ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *npt, uint3
     return NE2B_OK;
 }
 
-ne2b_status ne2b_split_delivery(ne2b_sim *sim, int32_t *split) {
-    if (!sim || !split) return set_error(NE2B_EINVAL, "null argument");
-    *split = sim->eng.split() ? 1 : 0;
-    return NE2B_OK;
-}
-
-ne2b_status ne2b_set_split_delivery(ne2b_sim *sim, int32_t split) {
-    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
-    GUARD(sim->eng.set_split(split != 0));
-}
-
 ne2b_status ne2b_stream(ne2b_sim *sim, void **stream) {
     if (!sim || !stream) return set_error(NE2B_EINVAL, "null argument");
     *stream = (void *)sim->eng.stream();
@@ -609,17 +598,6 @@ ne2b_status ne2b_batch_read_state(ne2b_batch *b, uint32_t net, uint32_t slot, fl
 ne2b_status ne2b_batch_autotune(ne2b_batch *b, uint32_t steps_per_trial) {
     if (!b) return set_error(NE2B_EINVAL, "null batch handle");
     GUARD(b->eng.autotune(steps_per_trial));
-}
-
-ne2b_status ne2b_batch_split_delivery(ne2b_batch *b, int32_t *split) {
-    if (!b || !split) return set_error(NE2B_EINVAL, "null argument");
-    *split = b->eng.split() ? 1 : 0;
-    return NE2B_OK;
-}
-
-ne2b_status ne2b_batch_set_split_delivery(ne2b_batch *b, int32_t split) {
-    if (!b) return set_error(NE2B_EINVAL, "null batch handle");
-    GUARD(b->eng.set_split(split != 0));
 }
 
 ne2b_status ne2b_batch_tile_shape(ne2b_batch *b, uint32_t *block, uint32_t *npt, uint32_t *bps) {

@@ -146,10 +146,6 @@ ne2b_status Engine::init(int device, bool int_ring, uint32_t max_nets) {
     NE2B_CUDA(cudaMemset(d_barrier_, 0, 2 * sizeof(unsigned int)));
     d_err_ = d_barrier_ + 1;
     if (const char *pdl = getenv("NE2B_PDL")) set_pdl(strcmp(pdl, "0") != 0);
-    if (const char *sp = getenv("NE2B_SPLIT")) {
-        if (*sp) split_env_ = sp[0] == '1' ? 1 : 0;
-        split_ = split_env_ == 1;
-    }
     if (const char *m = getenv("NE2B_KERNEL")) {
         if (!strcmp(m, "stream")) mode_ = kModeStream;
         else if (!strcmp(m, "resident")) mode_ = kModeResident;
@@ -171,8 +167,6 @@ ne2b_status Engine::upload_eng() {
     e.n_params = ptab_rows_dev_;
     e.barrier = d_barrier_;
     e.err = d_err_;
-    e.split = split_ ? 1u : 0u;
-    e.pad_[0] = e.pad_[1] = e.pad_[2] = 0u;
     // pageable source: the runtime copies it to staging before returning, so
     // the stack frame may go away without waiting for the device
     NE2B_CUDA(cudaMemcpyAsync(d_eng_, &e, sizeof e, cudaMemcpyHostToDevice, stream_));
@@ -347,17 +341,6 @@ ne2b_status Stager::close() {
     open_.clear();
     cur_ = -1;
     return NE2B_OK;
-}
-
-// Event queues pay where the ring misses L2: a net's ring of at least this
-// many bytes uses them, unless the engine decides for all its nets (mode 0
-// / 1).  NE2B_EVQ=0 / 1 turns them off / on for every net.
-constexpr uint64_t kEvqMinRingBytes = 128ull << 20;
-static bool evq_wanted(uint64_t ring_bytes, int mode) {
-    const char *e = getenv("NE2B_EVQ");
-    if (e && *e) return e[0] == '1';
-    if (mode >= 0) return mode == 1;
-    return ring_bytes >= kEvqMinRingBytes;
 }
 
 static double now_ms() {
@@ -743,28 +726,9 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         d.trace_last = (uint32_t)tab.size() - 1;
     }
     fill_noise(d, *cfg);
-    // event queues for a ring too large for L2 (custom-tau nets keep the
-    // direct adds): D buckets of n_pad events, room for one arrival per
-    // neuron per step (~100 Hz at 100 synapses per neuron); an append past
-    // that is added into the ring directly
-    const bool use_evq = !h->nx && h->e > 0 && h->D >= 3 && evq_wanted((uint64_t)h->D * np * 4u, evq_mode);
-    if (use_evq) {
-        d.evq_nseg = np / kNeuronAlign;  // tiles are at least 64 neurons
-        NET_TRY(alloc(&p, sizeof(uint2) * (size_t)h->D * np)); d.evq = (uint2 *)p;
-        NET_TRY(alloc(&p, sizeof(uint32_t) * h->D * (size_t)d.evq_nseg)); d.evq_cnt = (uint32_t *)p;
-        NET_TRY(cuda_error(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h->D * (size_t)d.evq_nseg, bst),
-                           "memset event queues"));
-    }
-    // split delivery lists (custom-tau nets deliver in the step kernel)
-    if (!h->nx && np) {
-        NET_TRY(alloc(&p, sizeof(uint32_t) * np)); d.spk_ids = (uint32_t *)p;
-        NET_TRY(alloc(&p, sizeof(uint32_t) * (np / kNeuronAlign))); d.spk_cnt = (uint32_t *)p;
-        NET_TRY(cuda_error(cudaMemsetAsync(d.spk_cnt, 0, sizeof(uint32_t) * (np / kNeuronAlign), bst),
-                           "memset spike lists"));
-    }
     d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
               (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u) | (h->nx ? kNetXsyn : 0u) |
-              (d.trace_f ? kNetTraceF32 : 0u) | (use_evq ? kNetEvq : 0u);
+              (d.trace_f ? kNetTraceF32 : 0u);
     tp[5] = now_ms();
     // initial state (cpu.rs:158-183), on the build stream
     NET_TRY(cuda_error(launch_reset_neurons(d, bst), "reset kernel"));
@@ -982,23 +946,9 @@ ne2b_status Engine::set_mode(int m) {
     return st;
 }
 
-// Event-queue segments belong to tile positions: drain them into the ring
-// (for the tile size they were filled under) before the tile size changes
-// or a snapshot is taken.
-ne2b_status Engine::flush_queues() {
-    const uint32_t tile = shape_.block * shape_.npt;
-    for (NetHost *h : nets_) {
-        if (!h || !h->dev.evq) continue;
-        NE2B_CUDA(launch_evq_flush(h->dev, int_ring_, tile, stream_));
-        launches_ += 1;
-    }
-    return NE2B_OK;
-}
-
 ne2b_status Engine::set_shape(const TileShape &s) {
     if (!shape_supported(s.block, s.npt))
         return set_error(NE2B_EINVAL, "tile shape block=%u npt=%u is not compiled in", s.block, s.npt);
-    if (s.block * s.npt != shape_.block * shape_.npt) NE2B_TRY(flush_queues());
     NE2B_CUDA(cudaStreamSynchronize(stream_));
     shape_ = s;
     clear_graphs();
@@ -1020,9 +970,6 @@ ne2b_status Engine::reset_net(uint32_t slot) {
         NE2B_CUDA(cudaMemsetAsync(d.xsyn, 0, sizeof(float) * h.nx, stream_));
         NE2B_CUDA(cudaMemsetAsync(d.xpend, 0, sizeof(uint32_t) * (size_t)h.D * d.xwords, stream_));
     }
-    if (d.spk_cnt) NE2B_CUDA(cudaMemsetAsync(d.spk_cnt, 0, sizeof(uint32_t) * (h.n_pad / kNeuronAlign), stream_));
-    if (d.evq_cnt)  // queues emptied
-        NE2B_CUDA(cudaMemsetAsync(d.evq_cnt, 0, sizeof(uint32_t) * h.D * (size_t)d.evq_nseg, stream_));
     // cpu.rs:176-183: the watch history and the grid marks start over
     h.watch_t0 = 0;
     if (d.gw_ls) NE2B_CUDA(cudaMemsetAsync(d.gw_ls, 0xFF, sizeof(uint32_t) * std::max<uint32_t>(h.gw_ptr.back(), 1), stream_));
@@ -1151,10 +1098,8 @@ ne2b_status Engine::launch_group(uint32_t steps) {
             cudaGraph_t gr;
             NE2B_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
             cudaError_t err = cudaSuccess;
-            for (uint32_t k = 0; k < steps && err == cudaSuccess; ++k) {
+            for (uint32_t k = 0; k < steps && err == cudaSuccess; ++k)
                 err = launch_step(int_ring_, adex_, var, shape_.block, shape_.npt, d_eng_, k, g, stream_);
-                if (err == cudaSuccess && split_) err = launch_split_delivery(k);
-            }
             if (err == cudaSuccess) err = launch_advance(d_nets_, nets_cap_, steps, stream_);
             cudaError_t e2 = cudaStreamEndCapture(stream_, &gr);
             if (err != cudaSuccess) return cuda_error(err, "step launch during capture");
@@ -1166,34 +1111,13 @@ ne2b_status Engine::launch_group(uint32_t steps) {
             it = graphs_.emplace(steps, ex).first;
         }
         NE2B_CUDA(cudaGraphLaunch(it->second, stream_));
-        launches_ += (split_ ? 2 * (uint64_t)steps : steps) + 1;
+        launches_ += steps + 1;
         return NE2B_OK;
     }
-    for (uint32_t k = 0; k < steps; ++k) {
-        NE2B_CUDA(launch_step(int_ring_, adex_, var, shape_.block, shape_.npt, d_eng_, k, g, stream_));
-        if (split_) NE2B_CUDA(launch_split_delivery(k));
-    }
+    for (uint32_t k = 0; k < steps; ++k) NE2B_CUDA(launch_step(int_ring_, adex_, var, shape_.block, shape_.npt, d_eng_, k, g, stream_));
     NE2B_CUDA(launch_advance(d_nets_, nets_cap_, steps, stream_));
-    launches_ += (split_ ? 2 * (uint64_t)steps : steps) + 1;
+    launches_ += steps + 1;
     return NE2B_OK;
-}
-
-// The delivery kernel of split delivery for step k of a launch group: one
-// warp per tile, as many blocks as the tiles need (8 warps each), at most
-// what the SMs hold at once.
-cudaError_t Engine::launch_split_delivery(uint32_t k) {
-    return launch_deliver(int_ring_, d_eng_, n_tiles_, k, shape_.block * shape_.npt, (uint32_t)sm_count_ * 8u, stream_);
-}
-
-// Split or fused delivery (resident launches always deliver themselves).
-// NE2B_SPLIT=0 / 1, read when the engine is created, fixes the choice.
-ne2b_status Engine::set_split(bool on) {
-    if (split_env_ >= 0) on = split_env_ == 1;
-    if (on == split_) return NE2B_OK;
-    NE2B_CUDA(cudaStreamSynchronize(stream_));  // every listed spike was delivered by its step's launch
-    split_ = on;
-    clear_graphs();
-    return upload_eng();
 }
 
 ne2b_status Engine::run_steps(uint64_t steps) {
@@ -1473,7 +1397,6 @@ ne2b_status Engine::grid_traces(NetHost &h, float tau_ms, float *out) {
 // Snapshot of every mutable device array (state, ring, record, windows,
 // descriptors, counters) in device memory, for the autotuner's trials.
 ne2b_status Engine::snapshot(EngineSnapshot &snap) {
-    NE2B_TRY(flush_queues());  // a restore may run under another tile size
     snap.items.clear();
     snap.hosts.clear();
     auto grab = [&](void *live, size_t bytes) -> ne2b_status {
@@ -1504,9 +1427,6 @@ ne2b_status Engine::snapshot(EngineSnapshot &snap) {
         NE2B_TRY(grab(d.watch_ring, d.watch_ring ? 8 * (size_t)d.watch_n * kWatchCap : 0));
         NE2B_TRY(grab(d.gw_ls, d.gw_ls ? 4 * (size_t)std::max<uint32_t>(h->gw_ptr.back(), 1) : 0));
         NE2B_TRY(grab(d.xpend, 4 * (size_t)h->D * d.xwords));
-        // the event queues are drained before a snapshot (flush_queues):
-        // their counters, all zero, are the whole of their state
-        NE2B_TRY(grab(d.evq_cnt, d.evq_cnt ? 4 * (size_t)h->D * d.evq_nseg : 0));
         snap.hosts.push_back({h->slot, h->t, h->dev});
     }
     return NE2B_OK;
@@ -1559,25 +1479,19 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
     const int saved_mode = mode_;
     TileShape best = shape_;
     int best_mode = mode_ == kModeAuto ? (resident_ ? kModeResident : kModeStream) : mode_;
-    bool best_split = split_;
     float best_ms = 1e30f;
     for (int m : {(int)kModeStream, (int)kModeResident}) {
         if (saved_mode != kModeAuto && m != saved_mode) continue;  // a forced kernel keeps its mode
         for (uint32_t c = 0; c < count; ++c) {
             const int occ = step_occupancy(int_ring_, adex_, step_variant(), blocks[c], npts[c]);
-            for (int cand = 0; cand < 4; ++cand) {
-                const int half = cand & 1;
-                const bool sp = (cand >> 1) != 0;  // split delivery (streaming only)
+            for (int half = 0; half < 2; ++half) {
                 if (half && (m == kModeResident || occ < 2)) continue;
-                if (sp && m == kModeResident) continue;
-                if (split_env_ >= 0 && sp != (split_env_ == 1)) continue;
                 TileShape s;
                 s.block = blocks[c];
                 s.npt = npts[c];
                 s.blocks_per_sm = half ? (uint32_t)std::max(1, occ / 2) : 0;
                 mode_ = m;
                 shape_ = s;
-                split_ = sp;
                 clear_graphs();
                 if (rebuild_tiles() != NE2B_OK) continue;  // resident plan does not fit
                 NE2B_TRY(restore(snap));
@@ -1598,14 +1512,12 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
                     best_ms = ms;
                     best = s;
                     best_mode = m;
-                    best_split = sp;
                 }
             }
         }
     }
     mode_ = saved_mode == kModeAuto ? best_mode : saved_mode;
     shape_ = best;
-    split_ = best_split;
     clear_graphs();
     NE2B_TRY(rebuild_tiles());
     NE2B_TRY(restore(snap));

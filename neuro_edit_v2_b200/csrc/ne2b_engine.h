@@ -189,10 +189,6 @@ class Engine {
     ne2b_status read_f32(const float *dev, uint32_t n, float *out);
     ne2b_status read_trace(NetHost &h, float *out);
     ne2b_status check_err();
-    ne2b_status flush_queues();  // event queues into the ring (before a tile-size change or a snapshot)
-    ne2b_status set_split(bool on);  // split (step kernel + delivery kernel) or fused delivery
-    bool split() const { return split_; }
-    cudaError_t launch_split_delivery(uint32_t k);
     ne2b_status spike_counts(NetHost &h, uint64_t rows, uint32_t *out);
     ne2b_status spike_row(NetHost &h, uint32_t back, uint64_t *out);
     ne2b_status spikes_total(NetHost &h, uint64_t *out);
@@ -225,7 +221,6 @@ class Engine {
     ne2b_status set_mode(int m);
     bool fixed_grid = false;  // grid independent of the tile count (serving)
     bool multi_net = false;   // many nets (batch, server): the streaming kernel stages tiles ahead
-    int evq_mode = -1;        // event queues for nets built from now on: -1 by the net's ring size, 0 off, 1 on
     uint32_t graph_steps = 256;
     uint32_t resident_steps = 4096;  // max steps per resident launch
     uint64_t stim_chunk = 2048;
@@ -271,8 +266,6 @@ class Engine {
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     float last_ms_ = 0.0f;
     uint64_t launches_ = 0;  // kernels launched (graph nodes counted per replay)
-    bool split_ = false;     // split delivery (streaming launches only)
-    int split_env_ = -1;     // NE2B_SPLIT: -1 unset, else the fixed choice
     // resident kernel
     int mode_ = kModeAuto;
     bool resident_ = false;

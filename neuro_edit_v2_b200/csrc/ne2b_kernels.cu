@@ -64,111 +64,6 @@ __global__ void pn_total_kernel(const unsigned long long *pn, uint32_t n, uint32
     out[i] = c > 0xffffffffull ? 0xffffffffu : (uint32_t)c;
 }
 
-// Split delivery, the second launch of a step: one warp per tile delivers
-// the spikes the step kernel listed for it (ids in the tile's range of
-// spk_ids, count in spk_cnt, emptied here).  For each spike the warp loads
-// the row bounds and strides the row, U synapses per lane and pass with all
-// their CSR loads issued before any add; an arrival goes into
-// ring[(t + d) % D][tgt] by a no-return atomic, or, with event queues and
-// d >= 2, is appended to the tile's segment of its bucket (cpu.rs:264-278,
-// kernels.rs:174-204).  `tile` is the tile size of the step kernel.
-template <bool INT>
-__global__ void __launch_bounds__(256) deliver_kernel(const EngineDev *__restrict__ eng, uint32_t k_step,
-                                                      uint32_t tile_size) {
-    pdl_trigger();
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t n_tiles = eng->n_tiles;
-    pdl_wait();  // the step kernel's lists are complete
-    for (uint32_t tix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tix < n_tiles; tix += warps) {
-        const Tile tile = eng->tiles[tix];
-        const NetDev &nd = eng->nets[tile.net];
-        uint32_t *const cntp = nd.spk_cnt;
-        if (!cntp) continue;  // a custom-tau net: delivered by the step kernel
-        const uint32_t k = tile.start / tile_size;
-        const uint32_t cnt = cntp[k];
-        if (cnt == 0u) continue;
-        __syncwarp();
-        if (lane == 0) cntp[k] = 0u;
-        const uint32_t D = nd.D, n_pad = nd.n_pad;
-        uint32_t tmod = nd.tmod + k_step;
-        if (tmod >= D) tmod %= D;
-        const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;
-        const bool evq = (nd.flags & kNetEvq) != 0u;
-        const bool d16 = (nd.flags & kNetDelay16) != 0u;
-        const uint32_t *__restrict__ rowptr = nd.rowptr;
-        const uint32_t *__restrict__ tgt = nd.tgt;
-        const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
-        uint32_t *__restrict__ ringw = (uint32_t *)nd.ring;
-        for (uint32_t b0 = 0; b0 < cnt; b0 += 32) {
-            uint32_t lo = 0, hi = 0;
-            if (b0 + lane < cnt) {
-                const uint32_t id = nd.spk_ids[tile.start + b0 + lane];
-                lo = rowptr[id];
-                hi = rowptr[id + 1];
-            }
-            const uint32_t m = cnt - b0 < 32u ? cnt - b0 : 32u;
-            for (uint32_t r = 0; r < m; ++r) {
-                const uint32_t rl = __shfl_sync(0xffffffffu, lo, r), rh = __shfl_sync(0xffffffffu, hi, r);
-                constexpr int U = 4;
-                for (uint32_t j0 = rl; j0 < rh; j0 += 32u * U) {
-                    uint32_t tg[U], sl_[U], wb[U];
-#pragma unroll
-                    for (int q = 0; q < U; ++q) {
-                        const uint32_t j0q = j0 + 32u * q + lane;
-                        const uint32_t j = j0q < rh ? j0q : rl;  // past the end: the row's first synapse again
-                        tg[q] = tgt[j];
-                        const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j]
-                                               : (uint32_t)((const uint8_t *)nd.delay)[j];
-                        sl_[q] = tmod + d >= D ? tmod + d - D : tmod + d;
-                        wb[q] = wbits[j];
-                    }
-#pragma unroll
-                    for (int q = 0; q < U; ++q) {
-                        if (j0 + 32u * q + lane >= rh) continue;
-                        if (evq && sl_[q] != b1) {
-                            const uint32_t pos = atomicAdd(nd.evq_cnt + (size_t)sl_[q] * nd.evq_nseg + k, 1u);
-                            if (pos < tile.count) {
-                                nd.evq[(size_t)sl_[q] * n_pad + tile.start + pos] = make_uint2(tg[q], wb[q]);
-                                continue;
-                            }
-                        }
-                        const size_t idx = (size_t)sl_[q] * n_pad + tg[q];
-                        if (INT) atomicAdd((int *)ringw + idx, (int)wb[q]);
-                        else atomicAdd((float *)ringw + idx, __uint_as_float(wb[q]));
-                    }
-                }
-            }
-        }
-    }
-}
-
-// Event queues: add every segment of every pending bucket into its ring slot
-// and empty it (the segments of tile size `tile`), so the queues can be
-// refilled under another tile size.  Pending arrivals reach their slots
-// early, which changes nothing: the slot of bucket b is next read at the
-// step they are due.  Bucket tmod (the next step's) was added into its slot
-// during the last step and only awaits its counter reset: it is emptied
-// without adding.
-template <bool INT>
-__global__ void evq_flush_kernel(NetDev nd, uint32_t tile) {
-    const uint32_t nseg = (nd.n_pad + tile - 1) / tile;
-    for (uint32_t s = blockIdx.x; s < nseg * nd.D; s += gridDim.x) {
-        const uint32_t b = s / nseg, k = s - b * nseg;
-        const uint32_t cnt = b == nd.tmod ? 0u : nd.evq_cnt[(size_t)b * nd.evq_nseg + k];
-        const uint32_t size = nd.n_pad - k * tile < tile ? nd.n_pad - k * tile : tile;
-        const uint32_t ne = cnt < size ? cnt : size;
-        const uint2 *q = nd.evq + (size_t)b * nd.n_pad + (size_t)k * tile;
-        for (uint32_t e = threadIdx.x; e < ne; e += blockDim.x) {
-            const size_t idx = (size_t)b * nd.n_pad + q[e].x;
-            if (INT) atomicAdd((int *)nd.ring + idx, (int)q[e].y);
-            else atomicAdd((float *)nd.ring + idx, __uint_as_float(q[e].y));
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) nd.evq_cnt[(size_t)b * nd.evq_nseg + k] = 0u;
-    }
-}
-
 // Self-test of the bounded grid barrier: every block but `absent` arrives,
 // so the others give up after `limit_ns`, set the error flag and return
 // (a wait that cannot end, ended by its limit, with no fault).
@@ -239,24 +134,6 @@ cudaError_t launch_barrier_selftest(unsigned int *counter, unsigned int *err, ui
 cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaStream_t st) {
     if (n_nets == 0) return cudaSuccess;
     return launch_pdl(advance_kernel, (n_nets + 127) / 128, 128, st, true, nets, n_nets, steps);
-}
-
-cudaError_t launch_deliver(bool int_ring, const EngineDev *eng, uint32_t n_tiles, uint32_t k_step, uint32_t tile,
-                           uint32_t max_blocks, cudaStream_t st) {
-    uint32_t grid = (n_tiles + 7) / 8;  // 8 warps per block, one tile per warp
-    if (grid > max_blocks) grid = max_blocks;
-    if (grid == 0) grid = 1;
-    return int_ring ? launch_pdl(deliver_kernel<true>, grid, 256, st, true, eng, k_step, tile)
-                    : launch_pdl(deliver_kernel<false>, grid, 256, st, true, eng, k_step, tile);
-}
-
-cudaError_t launch_evq_flush(const NetDev &nd, bool int_ring, uint32_t tile, cudaStream_t st) {
-    if (!nd.evq || tile == 0) return cudaSuccess;
-    const uint32_t segs = (nd.n_pad + tile - 1) / tile * nd.D;
-    const uint32_t grid = segs < 4096 ? segs : 4096;
-    if (int_ring) evq_flush_kernel<true><<<grid, 256, 0, st>>>(nd, tile);
-    else evq_flush_kernel<false><<<grid, 256, 0, st>>>(nd, tile);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st) {

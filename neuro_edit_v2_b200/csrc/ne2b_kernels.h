@@ -31,12 +31,6 @@ cudaError_t launch_advance(NetDev *nets, uint32_t n_nets, uint32_t steps, cudaSt
 cudaError_t launch_barrier_selftest(unsigned int *counter, unsigned int *err, uint32_t blocks, uint32_t absent,
                                     unsigned long long limit_ns, cudaStream_t st);
 cudaError_t launch_reset_neurons(const NetDev &nd, cudaStream_t st);
-// Split delivery after step k_step's step kernel (programmatic launch):
-// one warp per tile, at most max_blocks blocks of 8 warps.
-cudaError_t launch_deliver(bool int_ring, const EngineDev *eng, uint32_t n_tiles, uint32_t k_step, uint32_t tile,
-                           uint32_t max_blocks, cudaStream_t st);
-// Event queues of `nd` (filled under tile size `tile`) added into the ring and emptied.
-cudaError_t launch_evq_flush(const NetDev &nd, bool int_ring, uint32_t tile, cudaStream_t st);
 cudaError_t launch_trace(const uint16_t *tk, const float *tab, uint32_t n, float *out, cudaStream_t st);
 cudaError_t launch_window_count(const uint32_t *rec_bits, uint32_t rec_rows, uint32_t n_pad, uint32_t n,
                                 unsigned long long t, uint32_t rows, uint32_t *out, cudaStream_t st);

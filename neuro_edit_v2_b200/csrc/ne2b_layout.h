@@ -16,15 +16,8 @@
 //   stimulus: neuron-major (input, weight) rows and a [steps x n_inputs] f32
 //     value buffer; spike record: rows x n_pad/32 u32 words; window counts:
 //     max_windows x n_pad u16.
-//   event queues (nets whose ring is too large for L2): D buckets of n_pad
-//     events {target, weight bits}; bucket b holds the arrivals due at steps
-//     = b (mod D) delivered with a delay of 2 or more, in one segment per
-//     tile (the tile's neuron range of the bucket, with its own append
-//     counter), and is added into ring slot b by the step before it is
-//     read.
 #pragma once
 #include <stdint.h>
-#include <vector_types.h>  // uint2
 
 namespace ne2b {
 
@@ -42,7 +35,6 @@ enum NetFlags : uint32_t {
     kNetWatch = 1u << 7,    // watched neurons record their state every step
     kNetGridWatch = 1u << 8,  // grid groups record each member's last spike step
     kNetTraceF32 = 1u << 9,   // readout trace kept as f32 (its step table would be too long)
-    kNetEvq = 1u << 10,       // delays >= 2 are queued per arrival step (event queues), not added into the ring
 };
 
 enum TileFlags : uint32_t {
@@ -114,17 +106,6 @@ struct alignas(16) NetDev {
     const uint32_t *gw_off;     // [gw_n + 1] group ranges in gw_ls
     uint32_t *gw_ls;            // last spike step per texel (min(t, 2^32-2)), kNeverSpiked
     uint32_t watch_n, gw_n;
-    // event queues (kNetEvq only)
-    uint2 *evq;                 // [D x n_pad] {target, weight bits}; tile k's segment of bucket b is
-                                // [b * n_pad + k * tile, + the tile's neuron count)
-    uint32_t *evq_cnt;          // [D x evq_nseg] tile k's appends to bucket b at [b * evq_nseg + k] since
-                                // it was drained (may pass the segment's size: those added into the ring)
-    uint32_t evq_nseg, evq_pad[3];  // evq_nseg = n_pad / 64: segments at the smallest tile
-    // split delivery (nets without custom-tau synapses): the step kernel
-    // lists each tile's spiking neurons, the delivery kernel that follows it
-    // delivers them and empties the list
-    uint32_t *spk_ids;          // [n_pad] tile k's spiking neurons at [k * tile, + count)
-    uint32_t *spk_cnt;          // [n_pad / 64] tile k's count (0 when nothing is listed)
     // scalars
     unsigned long long t;       // step index of the next launch group's k = 0
     unsigned long long t_end;   // steps at or beyond this are skipped (serving)
@@ -181,8 +162,6 @@ struct EngineDev {
     uint32_t n_params;       // rows of ptab on the device
     unsigned int *barrier;   // grid-barrier arrival counter (zeroed before each launch)
     unsigned int *err;       // nonzero: a grid barrier timed out
-    uint32_t split;          // the streaming kernel lists spikes for the delivery kernel instead of delivering
-    uint32_t pad_[3];
 };
 
 }  // namespace ne2b

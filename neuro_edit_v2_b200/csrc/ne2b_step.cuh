@@ -12,42 +12,18 @@
 //      the trace is kept as "steps since the last spike" into a table of the
 //      exact f32 products 1.0 * decay_t * decay_t ..., which reproduces the
 //      reference's repeated multiply bit-for-bit at 2 bytes per neuron;
-//   4. write the spike-record words straight from warp ballots, and compact
-//      the tile's spikes by their CSR rows with block prefix sums over
-//      (spikes, synapses) into shared memory (replaces the global atomicAdd
-//      slot of kernels.rs:150-156);
-//   5. deliver its own spikes: the block strides the flat range of all its
-//      spikes' synapses, a no-return atomic add into
+//   4. write the spike-record words straight from warp ballots;
+//   5. deliver: each warp takes its own spiking lanes from the same ballots
+//      (replacing the global atomicAdd slot of kernels.rs:150-156) and
+//      strides each one's CSR row, four synapses per lane and pass (two
+//      with the f32 ring) with their loads issued together, a no-return
+//      atomic add into
 //      ring[(t + delay) % D][tgt] per synapse (cpu.rs:264-278,
-//      kernels.rs:174-204).
-//
-// Event queues (kNetEvq: nets whose D-slot ring does not fit in L2).  A
-// random add into a ring of hundreds of MB costs a DRAM read and write of a
-// 32-byte sector per event; instead, an arrival with delay d >= 2 is
-// appended as {target, weight} to the delivering tile's segment of bucket
-// (t + d) % D (a returning atomic on that segment's counter, which only
-// this tile's block touches, so it is uncontended; then an 8-byte store:
-// a segment fills front to back, and the ~n/8 open fronts stay in L2 until
-// their sectors are whole), and during step t - 1 each tile adds its
-// segment of bucket t into ring slot t, which is in L2 then (it is also the
-// slot prefetched for the next step).  Bucket t is complete by then: its
-// last appends came from step t - 2 (delay 2); delay-1 arrivals, and
-// appends past a segment's size (one per neuron of the tile), are added
-// straight into the ring.  A segment's counter is reset during step t, when
-// nothing appends to bucket t.  Segments belong to tile positions, so the
-// host drains the queues into the ring before the tile size changes.
-// Integer sums do not depend on the order of the adds, so rasters and
-// state are the direct path's bit for bit.
-//
-// Split delivery (EngineDev::split; nets without custom-tau synapses): the
-// streaming kernel only lists each tile's spiking neurons (ids at the
-// tile's range of spk_ids, the count in spk_cnt), and deliver_kernel, launched
-// right after it, delivers every listed spike with one warp per tile across
-// the whole GPU.  Fused, a block that walks several tiles pays one
-// dependent delivery chain (row bounds, scans, CSR loads, adds) per spiking
-// tile in sequence; split, the neuron pass ends at its ballots and all
-// chains run at once in one wave of warps, for one more launch per step.
-// The engine (autotune) picks whichever is faster for the workload.
+//      kernels.rs:174-204).  No block barrier and no shared memory: a warp
+//      holds a spike in a few percent of steps at tens of Hz, and a
+//      100-synapse row is one pass of the warp.  Nets with custom-tau
+//      synapses compact the tile's spikes by block prefix sums and stride
+//      the tile's flat synapse range instead (their arrivals mark bits).
 //
 // Within a step no cross-block ordering is needed: step t reads slot t % D and
 // every delivery of step t lands in slot (t + d) % D, 1 <= d < D.  Between
@@ -104,8 +80,7 @@ __device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, u
 template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool LEAN = false, bool NOIO = false>
 __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
                                              const Tile &tile, uint64_t t, uint32_t tmod, uint32_t k, float *vs, float *us,
-                                             float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl,
-                                             bool split = false) {
+                                             float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -176,23 +151,6 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             if (rel >= 0 && rel < (long long)nd.stim_len)
                 for (uint32_t c = threadIdx.x * 8u; c < nd.n_inputs; c += BLOCK * 8u)
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(nd.stim_buf + (size_t)rel * nd.n_inputs + c));
-        }
-    }
-
-    // ---- event queues: this tile's slice of bucket t + 1 into ring slot
-    // t + 1 (read by the next launch); bucket t's counter starts over
-    if (flags & kNetEvq) {
-        const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;
-        uint32_t *const seg_cnt = nd.evq_cnt + tile.start / (BLOCK * NPT);  // [b * evq_nseg]
-        if (threadIdx.x == 0u) seg_cnt[(size_t)tmod * nd.evq_nseg] = 0u;
-        const uint32_t c = RES ? __ldcg(seg_cnt + (size_t)b1 * nd.evq_nseg) : seg_cnt[(size_t)b1 * nd.evq_nseg];
-        const uint32_t ne = c < tile.count ? c : tile.count;
-        const uint2 *q = nd.evq + (size_t)b1 * n_pad + tile.start;
-        for (uint32_t e = threadIdx.x; e < ne; e += BLOCK) {
-            const uint2 ev = RES ? __ldcg(q + e) : q[e];
-            const size_t idx = (size_t)b1 * n_pad + ev.x;
-            if (INT) atomicAdd((int *)ringw + idx, (int)ev.y);
-            else atomicAdd((float *)ringw + idx, __uint_as_float(ev.y));
         }
     }
 
@@ -281,10 +239,8 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         if (__float_as_uint(snew) != __float_as_uint(s[q])) ss[off] = snew;
         if (k != k0) tks[off] = (uint16_t)k;
         if (sp) {
-            if (!split || xsyn_on) {  // split: the delivery kernel loads the row
-                rlo[q] = rowptr[i];
-                rhi[q] = rowptr[i + 1];
-            }
+            rlo[q] = rowptr[i];
+            rhi[q] = rowptr[i + 1];
             nd.pn_total[i] += 1ull;
             if (!LEAN && (flags & kNetGridWatch)) {  // cpu.rs:293-304
                 const uint32_t t32 = t < 0xFFFFFFFEull ? (uint32_t)t : 0xFFFFFFFEu;
@@ -331,7 +287,52 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             if (lane == 0 && off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask;
         }
     }
-    // ---- compaction: per-thread (spikes, synapses), block prefix sums
+    // ---- delivery, warp by warp (nets without custom-tau synapses): the
+    // warp's spiking lanes in order, the whole warp on each one's row
+    if (!xsyn_on) {
+        constexpr int U = kDeliverUnroll<INT>;
+        const uint32_t *__restrict__ tgt = nd.tgt;
+        const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
+        const bool d16 = flags & kNetDelay16;
+        uint32_t nspk = 0;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+            uint32_t m = __ballot_sync(0xffffffffu, spk[q]);
+            nspk += __popc(m);
+            while (m) {
+                const int src = __ffs(m) - 1;
+                m &= m - 1u;
+                const uint32_t lo = __shfl_sync(0xffffffffu, rlo[q], src);
+                const uint32_t hi = __shfl_sync(0xffffffffu, rhi[q], src);
+                for (uint32_t j0 = lo; j0 < hi; j0 += 32u * U) {
+                    // a lane past the row's end repeats its first synapse's
+                    // loads (same lines) and skips the add
+                    uint32_t tg[U], sl_[U], wb[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const uint32_t j1 = j0 + 32u * u + lane;
+                        const uint32_t j = j1 < hi ? j1 : lo;
+                        tg[u] = tgt[j];
+                        const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j]
+                                               : (uint32_t)((const uint8_t *)nd.delay)[j];
+                        sl_[u] = tmod + d >= D ? tmod + d - D : tmod + d;
+                        wb[u] = wbits[j];
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        if (j0 + 32u * u + lane < hi) {
+                            const size_t idx = (size_t)sl_[u] * n_pad + tg[u];
+                            if (INT) atomicAdd((int *)ringw + idx, (int)wb[u]);
+                            else atomicAdd((float *)ringw + idx, __uint_as_float(wb[u]));
+                        }
+                }
+            }
+        }
+        if (lane == 0 && nspk) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)nspk);
+        return;
+    }
+    // ---- custom-tau nets: compaction by block prefix sums over (spikes,
+    // synapses) into shared memory
     uint32_t cnt = 0, syn = 0;
 #pragma unroll
     for (int q = 0; q < NPT; ++q)
@@ -378,18 +379,6 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         }
     }
     __syncthreads();
-    if (split && !xsyn_on) {
-        // split delivery: list the tile's spiking neurons for deliver_kernel
-        uint32_t pos = sl.woff[warp] + ic - cnt;
-#pragma unroll
-        for (int q = 0; q < NPT; ++q)
-            if (spk[q]) nd.spk_ids[tile.start + pos++] = li[q];
-        if (threadIdx.x == 0) {
-            nd.spk_cnt[tile.start / (BLOCK * NPT)] = sl.total[0];
-            atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)sl.total[0]);
-        }
-        return;  // the next tile writes the shared lists only after its first barrier
-    }
     {
         uint32_t pos = sl.woff[warp] + ic - cnt;
         uint32_t so = sl.wsyn[warp] + is - syn;
@@ -412,11 +401,6 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     const uint32_t *__restrict__ tgt = nd.tgt;
     const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
     const bool d16 = flags & kNetDelay16;
-    // event queues: the next step's slot (delay 1: added at once) and this
-    // tile's append counters
-    const bool evq = (flags & kNetEvq) != 0u;
-    const uint32_t b1 = tmod + 1u == D ? 0u : tmod + 1u;
-    uint32_t *const seg_cnt = nd.evq_cnt + tile.start / (BLOCK * NPT);  // [b * evq_nseg]
     auto syn_at = [&](uint32_t f) {
         uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
         while (hi - lo > 1) {
@@ -457,18 +441,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             }
 #pragma unroll
             for (int q = 0; q < U; ++q)
-                if (f + q * BLOCK < nsyn) {
-                    // event queues: delays >= 2 are appended to their
-                    // bucket (past its cap, added into the ring as below)
-                    if (evq && sl_[q] != b1) {
-                        const uint32_t pos = atomicAdd(seg_cnt + (size_t)sl_[q] * nd.evq_nseg, 1u);
-                        if (pos < tile.count) {
-                            nd.evq[(size_t)sl_[q] * n_pad + tile.start + pos] = make_uint2(tg[q], wb[q]);
-                            continue;
-                        }
-                    }
-                    add(sl_[q], tg[q], wb[q]);
-                }
+                if (f + q * BLOCK < nsyn) add(sl_[q], tg[q], wb[q]);
         }
         __syncthreads();  // the next tile reuses the shared lists
         return;
@@ -556,7 +529,6 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
     static_assert(kNetWords <= BLOCK && kStageTiles <= BLOCK, "one 16-byte word per thread");
     const SmemLists sl = smem_lists(s_lists, BLOCK * NPT, BLOCK / 32);
     const uint32_t n_tiles = eng->n_tiles;
-    const bool split = eng->split != 0u;
     if constexpr (!MULTI) {
         uint32_t tix = blockIdx.x;
         if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
@@ -573,7 +545,7 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
             process_tile<INT, BLOCK, NPT, false, ADEX, false, PLAIN, PLAIN>(eng, ptab, s_nd, tile, t, tmod, k_step,
                                                              s_nd.v + tile.start, s_nd.u + tile.start,
                                                              s_nd.s + tile.start, s_nd.tk + tile.start,
-                                                             s_nd.pidx + tile.start, sl, split);
+                                                             s_nd.pidx + tile.start, sl);
             if (nx >= n_tiles) break;
             const Tile next = eng->tiles[nx];
             if (next.net != tile.net) {
@@ -624,7 +596,7 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
             process_tile<INT, BLOCK, NPT, false, ADEX, true, PLAIN>(eng, ptab, s_nd, tile, t, tmod, k_step,
                                                             s_nd.v + tile.start, s_nd.u + tile.start,
                                                             s_nd.s + tile.start, s_nd.tk + tile.start,
-                                                            s_nd.pidx + tile.start, sl, split);
+                                                            s_nd.pidx + tile.start, sl);
         }
     }
 }

@@ -306,17 +306,7 @@ class B200Sim:
         a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
         check(lib.ne2b_tile_shape(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return {"kernel": "resident" if self.kernel_mode()[1] else "stream", "block": int(a.value),
-                "neurons_per_thread": int(b.value), "blocks_per_sm": int(c.value),
-                "split_delivery": self.split_delivery()}
-
-    def split_delivery(self) -> bool:
-        """True when a second kernel per step delivers the listed spikes."""
-        v = C.c_int32()
-        check(lib.ne2b_split_delivery(self._h, C.byref(v)))
-        return bool(v.value)
-
-    def set_split_delivery(self, on: bool) -> None:
-        check(lib.ne2b_set_split_delivery(self._h, 1 if on else 0))
+                "neurons_per_thread": int(b.value), "blocks_per_sm": int(c.value)}
 
     # --- instrumentation (new) ------------------------------------------
     def stream_handle(self) -> int:
@@ -434,14 +424,6 @@ class Batch:
 
     def set_tile_shape(self, block: int, npt: int, blocks_per_sm: int = 0) -> None:
         check(lib.ne2b_batch_set_tile_shape(self._h, block, npt, blocks_per_sm))
-
-    def split_delivery(self) -> bool:
-        v = C.c_int32()
-        check(lib.ne2b_batch_split_delivery(self._h, C.byref(v)))
-        return bool(v.value)
-
-    def set_split_delivery(self, on: bool) -> None:
-        check(lib.ne2b_batch_set_split_delivery(self._h, 1 if on else 0))
 
     def dev_mem_bytes(self) -> int:
         b = C.c_uint64()

@@ -12,18 +12,14 @@
 //      the trace is kept as "steps since the last spike" into a table of the
 //      exact f32 products 1.0 * decay_t * decay_t ..., which reproduces the
 //      reference's repeated multiply bit-for-bit at 2 bytes per neuron;
-//   4. write the spike-record words straight from warp ballots;
-//   5. deliver: each warp takes its own spiking lanes from the same ballots
-//      (replacing the global atomicAdd slot of kernels.rs:150-156) and
-//      strides each one's CSR row, four synapses per lane and pass (two
-//      with the f32 ring) with their loads issued together, a no-return
-//      atomic add into
+//   4. write the spike-record words straight from warp ballots, and compact
+//      the tile's spikes by their CSR rows with block prefix sums over
+//      (spikes, synapses) into shared memory (replaces the global atomicAdd
+//      slot of kernels.rs:150-156);
+//   5. deliver its own spikes: the block strides the flat range of all its
+//      spikes' synapses, a no-return atomic add into
 //      ring[(t + delay) % D][tgt] per synapse (cpu.rs:264-278,
-//      kernels.rs:174-204).  No block barrier and no shared memory: a warp
-//      holds a spike in a few percent of steps at tens of Hz, and a
-//      100-synapse row is one pass of the warp.  Nets with custom-tau
-//      synapses compact the tile's spikes by block prefix sums and stride
-//      the tile's flat synapse range instead (their arrivals mark bits).
+//      kernels.rs:174-204).
 //
 // Within a step no cross-block ordering is needed: step t reads slot t % D and
 // every delivery of step t lands in slot (t + d) % D, 1 <= d < D.  Between
@@ -287,52 +283,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             if (lane == 0 && off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask;
         }
     }
-    // ---- delivery, warp by warp (nets without custom-tau synapses): the
-    // warp's spiking lanes in order, the whole warp on each one's row
-    if (!xsyn_on) {
-        constexpr int U = kDeliverUnroll<INT>;
-        const uint32_t *__restrict__ tgt = nd.tgt;
-        const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
-        const bool d16 = flags & kNetDelay16;
-        uint32_t nspk = 0;
-#pragma unroll
-        for (int q = 0; q < NPT; ++q) {
-            uint32_t m = __ballot_sync(0xffffffffu, spk[q]);
-            nspk += __popc(m);
-            while (m) {
-                const int src = __ffs(m) - 1;
-                m &= m - 1u;
-                const uint32_t lo = __shfl_sync(0xffffffffu, rlo[q], src);
-                const uint32_t hi = __shfl_sync(0xffffffffu, rhi[q], src);
-                for (uint32_t j0 = lo; j0 < hi; j0 += 32u * U) {
-                    // a lane past the row's end repeats its first synapse's
-                    // loads (same lines) and skips the add
-                    uint32_t tg[U], sl_[U], wb[U];
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const uint32_t j1 = j0 + 32u * u + lane;
-                        const uint32_t j = j1 < hi ? j1 : lo;
-                        tg[u] = tgt[j];
-                        const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j]
-                                               : (uint32_t)((const uint8_t *)nd.delay)[j];
-                        sl_[u] = tmod + d >= D ? tmod + d - D : tmod + d;
-                        wb[u] = wbits[j];
-                    }
-#pragma unroll
-                    for (int u = 0; u < U; ++u)
-                        if (j0 + 32u * u + lane < hi) {
-                            const size_t idx = (size_t)sl_[u] * n_pad + tg[u];
-                            if (INT) atomicAdd((int *)ringw + idx, (int)wb[u]);
-                            else atomicAdd((float *)ringw + idx, __uint_as_float(wb[u]));
-                        }
-                }
-            }
-        }
-        if (lane == 0 && nspk) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)nspk);
-        return;
-    }
-    // ---- custom-tau nets: compaction by block prefix sums over (spikes,
-    // synapses) into shared memory
+    // ---- compaction: per-thread (spikes, synapses), block prefix sums
     uint32_t cnt = 0, syn = 0;
 #pragma unroll
     for (int q = 0; q < NPT; ++q)

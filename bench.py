@@ -294,6 +294,8 @@ def run_profile(args):
     if args.shape:
         b, npt = (int(x) for x in args.shape.split("x"))
         sim.set_tile_shape(b, npt)
+    if args.delivery_warps:
+        sim.set_delivery_warps(True)
     tiling = sim.autotune(128) if args.autotune else sim.tiling()
     scrub = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
     ms, spikes, launches = timed_trials(sim, 1, 3, args.trial_steps, 1, torch, scrub)
@@ -886,6 +888,8 @@ def main():
     ap.add_argument("--shape", default=None,
                     help="tile shape BLOCKxNPT, e.g. 256x2 (with --kernel: fixes the headline tiling instead of "
                          "autotuning it, e.g. for an ncu launch list)")
+    ap.add_argument("--delivery-warps", action="store_true",
+                    help="--profile with separate delivery warps in the streaming kernel")
     ap.add_argument("--served-mix", type=int, default=0,
                     help="--profile the first N requests of the serving stream stepped as one batch")
     ap.add_argument("--batched-liquids", type=int, default=0,

@@ -188,6 +188,17 @@ ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *neurons_pe
                             uint32_t *blocks_per_sm);
 ne2b_status ne2b_set_tile_shape(ne2b_sim *sim, uint32_t block, uint32_t neurons_per_thread,
                                 uint32_t blocks_per_sm);
+/* Delivery warps (new; no reference counterpart, the reference delivers
+ * with one warp per spike in a second kernel, kernels.rs:174-204): with
+ * `on`, the streaming step kernel of a one-net sim runs separate delivery
+ * warps beside the tile threads, which queue their spiking neurons' rows
+ * in shared memory, so delivery overlaps the neuron pass (tile blocks of
+ * 128, 256 and 512 threads).  ne2b_autotune tries both and keeps the faster.
+ * ne2b_set_tile_shape keeps this setting.  *active reports whether the
+ * kernel that runs uses them.  Results are the same either way (bit for bit
+ * with the int32 ring). */
+ne2b_status ne2b_set_delivery_warps(ne2b_sim *sim, int32_t on);
+ne2b_status ne2b_delivery_warps(ne2b_sim *sim, int32_t *on, int32_t *active);
 
 /* Instrumentation (new): the CUDA stream the handle launches on (a
  * cudaStream_t, for timing with events on the launching stream) and the

@@ -178,6 +178,8 @@ _SIGS = {
     "ne2b_autotune": (C.c_int, [_p, _u32]),
     "ne2b_tile_shape": (C.c_int, [_p, _pu32, _pu32, _pu32]),
     "ne2b_set_tile_shape": (C.c_int, [_p, _u32, _u32, _u32]),
+    "ne2b_set_delivery_warps": (C.c_int, [_p, C.c_int32]),
+    "ne2b_delivery_warps": (C.c_int, [_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ne2b_stream": (C.c_int, [_p, C.POINTER(_p)]),
     "ne2b_kernel_launches": (C.c_int, [_p, _pu64]),
     "ne2b_batch_stream": (C.c_int, [_p, C.POINTER(_p)]),

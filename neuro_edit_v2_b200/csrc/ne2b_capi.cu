@@ -454,6 +454,7 @@ ne2b_status ne2b_set_tile_shape(ne2b_sim *sim, uint32_t block, uint32_t npt, uin
     sh.block = block;
     sh.npt = npt;
     sh.blocks_per_sm = bps;
+    sh.ws = sim->eng.shape().ws;  // the delivery-warp setting is kept
     GUARD(sim->eng.set_shape(sh));
 }
 
@@ -462,6 +463,20 @@ ne2b_status ne2b_tile_shape(ne2b_sim *sim, uint32_t *block, uint32_t *npt, uint3
     *block = sim->eng.shape().block;
     *npt = sim->eng.shape().npt;
     *bps = sim->eng.shape().blocks_per_sm;
+    return NE2B_OK;
+}
+
+ne2b_status ne2b_set_delivery_warps(ne2b_sim *sim, int32_t on) {
+    if (!sim) return set_error(NE2B_EINVAL, "null sim handle");
+    ne2b::TileShape sh = sim->eng.shape();
+    sh.ws = on != 0;
+    GUARD(sim->eng.set_shape(sh));
+}
+
+ne2b_status ne2b_delivery_warps(ne2b_sim *sim, int32_t *on, int32_t *active) {
+    if (!sim || !on || !active) return set_error(NE2B_EINVAL, "null argument");
+    *on = sim->eng.shape().ws ? 1 : 0;
+    *active = (!sim->eng.resident() && sim->eng.ws_applies(sim->eng.shape())) ? 1 : 0;
     return NE2B_OK;
 }
 

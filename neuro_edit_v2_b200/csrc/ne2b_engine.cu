@@ -804,15 +804,25 @@ uint32_t Engine::grid() const {
     return g < nt ? g : nt;
 }
 
-int Engine::step_variant() const {
+int Engine::step_variant() const { return step_variant(shape_); }
+
+// The warp-specialised kernel serves streaming engines of exactly one net
+// (its tile warps never restage a net descriptor) in the shapes it is
+// compiled for.
+bool Engine::ws_applies(const TileShape &s) const {
+    return s.ws && !multi_net && active_nets() == 1 && ws_shape_supported(s.block, s.npt);
+}
+
+int Engine::step_variant(const TileShape &s) const {
     constexpr uint32_t kDebug = kNetRecord | kNetXsyn | kNetWatch | kNetGridWatch | kNetTraceF32;
     constexpr uint32_t kInput = kNetHasExt | kNetWindows;
     uint32_t used = 0;
     for (const NetHost *h : nets_)
         if (h) used |= h->dev.flags;
     if (multi_net) return (used & kDebug) ? kStepMulti : kStepMultiLean;
-    if (stim_tiles_ || (used & (kDebug | kInput))) return kStepSingle;
-    return kStepPlain;
+    const int ws = ws_applies(s) ? kStepWS : 0;
+    if (stim_tiles_ || (used & (kDebug | kInput))) return kStepSingle | ws;
+    return kStepPlain | ws;
 }
 
 // Resident plan: G co-resident blocks, each owning a contiguous range of
@@ -992,6 +1002,8 @@ ne2b_status Engine::check_err() {
     NE2B_CUDA(cudaMemcpy(&e, d_err_, sizeof e, cudaMemcpyDeviceToHost));
     if (e) {
         NE2B_CUDA(cudaMemset(d_err_, 0, sizeof e));
+        if (e == kErrDeliveryQueue)
+            return set_error(NE2B_ECUDA, "step kernel: a delivery-queue wait exceeded its limit; state is invalid");
         return set_error(NE2B_ECUDA, "resident kernel: a grid barrier wait exceeded its limit; state is invalid");
     }
     return NE2B_OK;
@@ -1482,13 +1494,16 @@ ne2b_status Engine::autotune(uint32_t steps_per_trial) {
     float best_ms = 1e30f;
     for (int m : {(int)kModeStream, (int)kModeResident}) {
         if (saved_mode != kModeAuto && m != saved_mode) continue;  // a forced kernel keeps its mode
-        for (uint32_t c = 0; c < count; ++c) {
-            const int occ = step_occupancy(int_ring_, adex_, step_variant(), blocks[c], npts[c]);
+        for (uint32_t c = 0; c < 2 * count; ++c) {
+            // candidates c >= count: the same shapes with delivery warps
+            TileShape s;
+            s.block = blocks[c % count];
+            s.npt = npts[c % count];
+            s.ws = c >= count;
+            if (s.ws && (m == kModeResident || !ws_applies(s))) continue;
+            const int occ = step_occupancy(int_ring_, adex_, step_variant(s), s.block, s.npt);
             for (int half = 0; half < 2; ++half) {
                 if (half && (m == kModeResident || occ < 2)) continue;
-                TileShape s;
-                s.block = blocks[c];
-                s.npt = npts[c];
                 s.blocks_per_sm = half ? (uint32_t)std::max(1, occ / 2) : 0;
                 mode_ = m;
                 shape_ = s;

@@ -145,6 +145,7 @@ struct TileShape {
     uint32_t block = 256;
     uint32_t npt = 2;
     uint32_t blocks_per_sm = 0;  // 0 = occupancy limit
+    bool ws = false;             // separate delivery warps (step_kernel_ws), engines of one net
 };
 
 class Engine {
@@ -219,6 +220,8 @@ class Engine {
     bool resident() const { return resident_; }
     int mode() const { return mode_; }
     ne2b_status set_mode(int m);
+    // the streaming kernel runs separate delivery warps for shape `s`
+    bool ws_applies(const TileShape &s) const;
     bool fixed_grid = false;  // grid independent of the tile count (serving)
     bool multi_net = false;   // many nets (batch, server): the streaming kernel stages tiles ahead
     uint32_t graph_steps = 256;
@@ -235,6 +238,7 @@ class Engine {
     uint32_t grid() const;
     // the streaming kernel instance for the engine's nets (StepVariant)
     int step_variant() const;
+    int step_variant(const TileShape &s) const;  // with `s`'s delivery warps where they apply
     bool plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &block_tiles);
     void clear_graphs();
 

@@ -82,6 +82,13 @@ bool shape_supported(uint32_t block, uint32_t npt) {
     return false;
 }
 
+bool ws_shape_supported(uint32_t block, uint32_t npt) {
+#define X(B, P) if (block == B && npt == P) return true;
+    NE2B_WS_SHAPES(X)
+#undef X
+    return false;
+}
+
 void shape_list(uint32_t *blocks, uint32_t *npts, uint32_t *count) {
     uint32_t c = 0;
 #define X(B, P) blocks[c] = B; npts[c] = P; ++c;

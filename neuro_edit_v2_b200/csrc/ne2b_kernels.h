@@ -8,6 +8,7 @@
 namespace ne2b {
 
 bool shape_supported(uint32_t block, uint32_t npt);
+bool ws_shape_supported(uint32_t block, uint32_t npt);  // step_kernel_ws compiled for this shape
 void set_pdl(bool on);  // programmatic dependent launch of the streaming kernels (default on)
 void shape_list(uint32_t *blocks, uint32_t *npts, uint32_t *count);
 // `adex`: an AdEx row is present in some net (else the Izhikevich-only

@@ -161,7 +161,9 @@ struct EngineDev {
     uint32_t block_neurons;  // shared-memory state capacity per block
     uint32_t n_params;       // rows of ptab on the device
     unsigned int *barrier;   // grid-barrier arrival counter (zeroed before each launch)
-    unsigned int *err;       // nonzero: a grid barrier timed out
+    unsigned int *err;       // nonzero: a device wait gave up (kErrBarrier, kErrDeliveryQueue)
 };
+constexpr unsigned int kErrBarrier = 1u;        // a resident kernel's grid barrier
+constexpr unsigned int kErrDeliveryQueue = 2u;  // a delivery-queue wait of step_kernel_ws
 
 }  // namespace ne2b

@@ -61,6 +61,58 @@ __device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, u
     return SmemLists{base, base + tile, base + 2 * tile + 1, base + 2 * tile + 1 + nw, base + 2 * tile + 1 + 2 * nw};
 }
 
+// Delivery queue of the warp-specialised streaming kernel (step_kernel_ws):
+// the tile warps push one cell per spiking neuron with synapses, and the
+// block's delivery warps take the cells and deliver their rows, so a tile's
+// delivery overlaps the next tiles' neuron passes.  A bounded multi-producer
+// multi-consumer ring in shared memory: cell c holds {turn, row start, row
+// end}; position p (claimed with an atomic counter) uses cell p % kWsCells,
+// whose producer waits for turn == p, writes the row, then publishes turn =
+// p + 1 (release); its consumer waits for turn == p + 1 (acquire), reads the
+// row and hands the cell on with turn = p + kWsCells.  Every wait is bounded
+// by %globaltimer (kWsWaitLimitNs), after which the kernel raises the engine
+// error flag (kErrDeliveryQueue) and stops waiting.
+constexpr uint32_t kWsCells = 256;
+constexpr unsigned long long kWsWaitLimitNs = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ uint32_t ld_acquire_cta(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.cta.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_cta(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.cta.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+struct WsQueue {
+    uint4 *cell;     // [kWsCells] {turn, rlo, rhi, -}
+    uint32_t *ctr;   // [0] positions claimed by producers, [1] by consumers,
+                     // [2] tile warps finished, [3] spikes counted
+};
+
+// Wait (bounded) until cell `turn` reads `want`; false when the wait gave up
+// (the error flag is then set) or another wait of the launch already did.
+__device__ __forceinline__ bool ws_wait_turn(const uint32_t *turn, uint32_t want, unsigned int *err) {
+    unsigned long long t0 = 0;
+    for (uint32_t polls = 1; ld_acquire_cta(turn) != want; ++polls) {
+        if ((polls & 63u) == 0u) {
+            const unsigned long long now = globaltimer_ns();
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > kWsWaitLimitNs || *(volatile unsigned int *)err != 0u) {
+                atomicCAS(err, 0u, kErrDeliveryQueue);
+                return false;
+            }
+        }
+        __nanosleep(32);
+    }
+    return true;
+}
+
 // `nd` is the tile's net descriptor (global memory, or a shared-memory copy
 // staged before the launch's dependency wait); `t` is the absolute step,
 // `tmod` = t % D and `k` = t - nd.t (the step within the launch group).
@@ -73,10 +125,15 @@ __device__ __forceinline__ SmemLists smem_lists(uint32_t *base, uint32_t tile, u
 // trace or watches; NOIO: nor an external current, a stimulus or windows.
 // Their code is compiled out (the engine launches such an instance only
 // then).
-template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool LEAN = false, bool NOIO = false>
+// WSQ (step_kernel_ws): the tile's threads are the producer warps of a
+// delivery queue; they push their spiking neurons' rows into `wq` and count
+// their spikes into *nspk (per warp) instead of compacting and delivering.
+template <bool INT, int BLOCK, int NPT, bool RES, bool ADEX, bool PHASES, bool LEAN = false, bool NOIO = false,
+          bool WSQ = false>
 __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, const ParamRow *ptab, const NetDev &nd,
                                              const Tile &tile, uint64_t t, uint32_t tmod, uint32_t k, float *vs, float *us,
-                                             float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl) {
+                                             float *ss, uint16_t *tks, const uint16_t *pis, const SmemLists &sl,
+                                             const WsQueue *wq = nullptr, uint32_t *nspk = nullptr) {
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -282,6 +339,33 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             const uint32_t off = q * BLOCK + warp * 32;
             if (lane == 0 && off < tile.count) nd.rec_bits[(size_t)row * words32 + ((tile.start + off) >> 5)] = mask;
         }
+    }
+    if constexpr (WSQ) {
+        // ---- push each spiking neuron's CSR row to the block's delivery
+        // warps: one position claim per warp and q, then each spiking lane
+        // fills its cell in turn (no block barrier)
+        const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+            *nspk += __popc(__ballot_sync(0xffffffffu, spk[q]));
+            const bool has = spk[q] && rhi[q] > rlo[q];
+            const uint32_t m = __ballot_sync(0xffffffffu, has);
+            if (m == 0u) continue;
+            const int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&wq->ctr[0], (uint32_t)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (has) {
+                const uint32_t pos = base + __popc(m & lt);
+                uint4 *c = wq->cell + (pos & (kWsCells - 1u));
+                if (ws_wait_turn(&c->x, pos, eng->err)) {
+                    c->y = rlo[q];
+                    c->z = rhi[q];
+                    st_release_cta(&c->x, pos + 1u);
+                }
+            }
+        }
+        return;
     }
     // ---- compaction: per-thread (spikes, synapses), block prefix sums
     uint32_t cnt = 0, syn = 0;
@@ -552,12 +636,150 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
     }
 }
 
-// ------------------------------------------------------- resident kernel
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
+// ------------------------------------------- warp-specialised streaming kernel
+// One net (single-net engines only).  Warps 0 .. BLOCK/32 - 1 are the tile
+// warps: they stride the block's tiles (b, b + G, ...) doing the neuron pass
+// and push each spiking neuron's CSR row into the block's delivery queue,
+// never waiting on a block barrier.  The ws_warps(BLOCK) warps after them
+// take the queued rows one per warp (lanes stride the row, U synapses per
+// lane and pass, all their CSR loads in flight before the adds) and deliver
+// them into the ring, so a tile's delivery overlaps the neuron passes of the
+// block's later tiles.  They stop when every tile warp has finished and the
+// queue is drained.  The last tile warp to finish adds the block's spike
+// count to the net's total.
+template <int BLOCK>
+__host__ __device__ constexpr int ws_warps() {
+    return BLOCK <= 128 ? 2 : 4;
 }
+
+template <bool INT, int BLOCK, int NPT, bool ADEX, bool PLAIN>
+__global__ void __launch_bounds__(BLOCK + 32 * ws_warps<BLOCK>()) step_kernel_ws(const EngineDev *__restrict__ eng,
+                                                                               uint32_t k_step) {
+    pdl_trigger();
+    constexpr int THREADS = BLOCK + 32 * ws_warps<BLOCK>();
+    constexpr uint32_t P = BLOCK / 32;  // tile warps
+    __shared__ __align__(16) NetDev s_nd;
+    __shared__ __align__(16) ParamRow s_ptab[kSmemParamRows];
+    __shared__ __align__(16) uint4 s_cell[kWsCells];
+    __shared__ uint32_t s_ctr[4];
+    static_assert(sizeof(NetDev) / 16 <= BLOCK, "one 16-byte word per thread");
+    const uint32_t n_tiles = eng->n_tiles;
+    uint32_t tix = blockIdx.x;
+    if (tix >= n_tiles) return;  // a fixed grid larger than the tile list
+    Tile tile = eng->tiles[tix];
+    stage_net(eng, tile.net, &s_nd);
+    const ParamRow *ptab = stage_params<THREADS>(eng, s_ptab);
+    for (uint32_t c = threadIdx.x; c < kWsCells; c += THREADS) s_cell[c] = make_uint4(c, 0u, 0u, 0u);
+    if (threadIdx.x < 4) s_ctr[threadIdx.x] = 0u;
+    __syncthreads();
+    pdl_wait();
+    const WsQueue wq{s_cell, s_ctr};
+    const uint64_t t = s_nd.t + k_step;
+    uint32_t tmod = s_nd.tmod + k_step;
+    if (tmod >= s_nd.D) tmod %= s_nd.D;
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < BLOCK) {
+        uint32_t nspk = 0;  // this warp's spikes (warp-uniform)
+        const SmemLists none{};
+        for (;;) {
+            process_tile<INT, BLOCK, NPT, false, ADEX, false, PLAIN, PLAIN, true>(
+                eng, ptab, s_nd, tile, t, tmod, k_step, s_nd.v + tile.start, s_nd.u + tile.start, s_nd.s + tile.start,
+                s_nd.tk + tile.start, s_nd.pidx + tile.start, none, &wq, &nspk);
+            tix += gridDim.x;
+            if (tix >= n_tiles) break;
+            tile = eng->tiles[tix];
+        }
+        if (lane == 0) {
+            if (nspk) atomicAdd(&s_ctr[3], nspk);
+            __threadfence_block();
+            if (atomicAdd(&s_ctr[2], 1u) == P - 1u) {  // the last tile warp: the block's spike count
+                __threadfence_block();
+                const uint32_t total = *(volatile uint32_t *)&s_ctr[3];
+                if (total) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
+            }
+        }
+        return;
+    }
+    // ---- delivery warps
+    constexpr int U = kDeliverUnroll<INT>;
+    uint32_t *__restrict__ ringw = (uint32_t *)s_nd.ring;
+    const uint32_t *__restrict__ tgt = s_nd.tgt;
+    const uint32_t *__restrict__ wbits = (const uint32_t *)s_nd.w;
+    const uint32_t n_pad = s_nd.n_pad, D = s_nd.D;
+    const bool d16 = s_nd.flags & kNetDelay16;
+    const bool xsyn_on = !PLAIN && (s_nd.flags & kNetXsyn);
+    const uint32_t e_total = s_nd.rowptr[s_nd.n];  // a queued row must lie inside the CSR
+    for (;;) {
+        uint32_t pos = 0;
+        if (lane == 0) pos = atomicAdd(&s_ctr[1], 1u);
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        const uint4 *c = s_cell + (pos & (kWsCells - 1u));
+        // lane 0 waits for the row at `pos` (1), or for the end: every tile
+        // warp finished and `pos` lies past the last claimed position (2),
+        // or gives up (3); the warp follows its decision
+        uint32_t st = 0;
+        if (lane == 0) {
+            unsigned long long t0 = 0;
+            for (uint32_t polls = 1; st == 0u; ++polls) {
+                if (ld_acquire_cta(&c->x) == pos + 1u) st = 1u;
+                else if (ld_acquire_cta(&s_ctr[2]) == P && pos >= *(volatile uint32_t *)&s_ctr[0]) st = 2u;
+                else if ((polls & 63u) == 0u) {
+                    const unsigned long long now = globaltimer_ns();
+                    if (t0 == 0) t0 = now;
+                    else if (now - t0 > kWsWaitLimitNs || *(volatile unsigned int *)eng->err != 0u) {
+                        atomicCAS(eng->err, 0u, kErrDeliveryQueue);
+                        st = 3u;
+                    }
+                }
+                if (st == 0u) __nanosleep(20);
+            }
+        }
+        st = __shfl_sync(0xffffffffu, st, 0);
+        if (st != 1u) break;
+        __syncwarp();  // orders lane 0's acquire before the other lanes' reads
+        const uint32_t rlo = c->y, rhi = c->z;
+        __syncwarp();  // every lane has read the cell before lane 0 hands it on
+        if (lane == 0) st_release_cta((uint32_t *)&c->x, pos + kWsCells);
+        if (rlo > rhi || rhi > e_total) {  // never expected: report it rather than read outside the CSR
+            if (lane == 0) atomicCAS(eng->err, 0u, kErrDeliveryQueue);
+            continue;
+        }
+        const uint32_t cnt = rhi - rlo;
+        for (uint32_t f = lane; f < cnt; f += 32u * U) {
+            // a lane past the row's end repeats its first synapse's loads and
+            // skips the add
+            uint32_t j[U], tg[U], sl_[U], wb[U];
+            j[0] = rlo + f;
+#pragma unroll
+            for (int q = 1; q < U; ++q) j[q] = f + 32u * q < cnt ? rlo + f + 32u * q : j[0];
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                tg[q] = tgt[j[q]];
+                const uint32_t d = d16 ? (uint32_t)((const uint16_t *)s_nd.delay)[j[q]]
+                                       : (uint32_t)((const uint8_t *)s_nd.delay)[j[q]];
+                const uint32_t slot = tmod + d;
+                sl_[q] = slot >= D ? slot - D : slot;
+                wb[q] = wbits[j[q]];
+            }
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                if (f + 32u * q >= cnt) continue;
+                if (xsyn_on) {
+                    const uint32_t k = s_nd.xmap[j[q]];
+                    if (k != kNoXsyn) {  // its own current: mark the arrival (cpu.rs:270-273)
+                        atomicOr(s_nd.xpend + (size_t)sl_[q] * s_nd.xwords + (k >> 5), 1u << (k & 31u));
+                        continue;
+                    }
+                }
+                const size_t idx = (size_t)sl_[q] * n_pad + tg[q];
+                if (INT) atomicAdd((int *)ringw + idx, (int)wb[q]);
+                else atomicAdd((float *)ringw + idx, __uint_as_float(wb[q]));
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------- resident kernel
 
 __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p) {
     unsigned int v;
@@ -598,7 +820,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int
                         break;
                     }
                     if (globaltimer_ns() - t0 > limit_ns) {
-                        atomicExch(err, 1u);
+                        atomicExch(err, kErrBarrier);
                         ok = 0u;
                         break;
                     }
@@ -691,6 +913,22 @@ static cudaError_t launch_pdl(void (*kernel)(Args...), uint32_t grid, uint32_t b
 
 template <bool INT, bool ADEX>
 int StepKind<INT, ADEX>::occupancy(uint32_t block, uint32_t npt, int variant) {
+    if (variant & kStepWS) {
+#define X(B, P)                                                                                                 \
+        if (block == B && npt == P) {                                                                           \
+            int b = 0;                                                                                          \
+            if ((variant & ~kStepWS) == kStepPlain)                                                             \
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel_ws<INT, B, P, ADEX, true>,        \
+                                                              B + 32 * ws_warps<B>(), 0);                       \
+            else                                                                                                \
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel_ws<INT, B, P, ADEX, false>,       \
+                                                              B + 32 * ws_warps<B>(), 0);                       \
+            return b;                                                                                           \
+        }
+        NE2B_WS_SHAPES(X)
+#undef X
+        return 0;
+    }
 #define X(B, P)                                                                                                 \
     if (block == B && npt == P) {                                                                               \
         int b = 0;                                                                                              \
@@ -712,6 +950,18 @@ int StepKind<INT, ADEX>::occupancy(uint32_t block, uint32_t npt, int variant) {
 template <bool INT, bool ADEX>
 cudaError_t StepKind<INT, ADEX>::launch(uint32_t block, uint32_t npt, int variant, const EngineDev *eng,
                                         uint32_t k_step, uint32_t grid, cudaStream_t st) {
+    if (variant & kStepWS) {
+#define X(B, P)                                                                                                    \
+        if (block == B && npt == P)                                                                                \
+            return (variant & ~kStepWS) == kStepPlain                                                              \
+                       ? launch_pdl(step_kernel_ws<INT, B, P, ADEX, true>, grid, B + 32 * ws_warps<B>(), st,       \
+                                    k_step > 0, eng, k_step)                                                       \
+                       : launch_pdl(step_kernel_ws<INT, B, P, ADEX, false>, grid, B + 32 * ws_warps<B>(), st,      \
+                                    k_step > 0, eng, k_step);
+        NE2B_WS_SHAPES(X)
+#undef X
+        return cudaErrorInvalidValue;
+    }
 #define X(B, P)                                                                                                   \
     if (block == B && npt == P)                                                                                   \
         return variant == kStepMulti                                                                              \

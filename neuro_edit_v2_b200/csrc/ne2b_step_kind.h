@@ -12,6 +12,10 @@
 #define NE2B_SHAPES(X) \
     X(64, 1) X(64, 2) X(64, 4) X(128, 1) X(128, 2) X(128, 4) X(128, 8) X(256, 1) X(256, 2) X(256, 4) X(256, 8) \
     X(512, 1) X(512, 2) X(512, 4)
+// Shapes with an instance of the warp-specialised single-net kernel
+// (step_kernel_ws: the tile warps plus separate delivery warps).
+#define NE2B_WS_SHAPES(X) \
+    X(128, 1) X(128, 2) X(128, 4) X(128, 8) X(256, 1) X(256, 2) X(256, 4) X(256, 8) X(512, 1) X(512, 2) X(512, 4)
 
 namespace ne2b {
 
@@ -35,6 +39,9 @@ __host__ __device__ constexpr uint32_t resident_head_bytes() {
 // synapses, f32 trace, watches), many nets (batches, the server), and many
 // nets without records, custom-tau synapses, f32 trace or watches.
 enum StepVariant : int { kStepSingle = 0, kStepMulti = 1, kStepPlain = 2, kStepMultiLean = 3 };
+// Added to kStepSingle or kStepPlain: the warp-specialised instance
+// (separate delivery warps; engines of one net, NE2B_WS_SHAPES only).
+constexpr int kStepWS = 0x10;
 
 template <bool INT, bool ADEX>
 struct StepKind {

@@ -302,11 +302,23 @@ class B200Sim:
     def set_tile_shape(self, block: int, neurons_per_thread: int, blocks_per_sm: int = 0) -> None:
         check(lib.ne2b_set_tile_shape(self._h, block, neurons_per_thread, blocks_per_sm))
 
+    def set_delivery_warps(self, on: bool) -> None:
+        """Separate delivery warps in the streaming step kernel (one-net sims;
+        tile blocks of 128, 256 or 512 threads); results are unchanged."""
+        check(lib.ne2b_set_delivery_warps(self._h, 1 if on else 0))
+
+    def delivery_warps(self) -> tuple[bool, bool]:
+        """(requested, used by the kernel that runs)."""
+        a, b = C.c_int32(), C.c_int32()
+        check(lib.ne2b_delivery_warps(self._h, C.byref(a), C.byref(b)))
+        return bool(a.value), bool(b.value)
+
     def tiling(self) -> dict:
         a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
         check(lib.ne2b_tile_shape(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return {"kernel": "resident" if self.kernel_mode()[1] else "stream", "block": int(a.value),
-                "neurons_per_thread": int(b.value), "blocks_per_sm": int(c.value)}
+                "neurons_per_thread": int(b.value), "blocks_per_sm": int(c.value),
+                "delivery_warps": self.delivery_warps()[1]}
 
     # --- instrumentation (new) ------------------------------------------
     def stream_handle(self) -> int:

@@ -92,7 +92,8 @@ def lockstep_many(onet: O.ONet, steps: int, variants, int_weights: bool = True, 
     """One oracle run against several GPU sims of the same net and config.
 
     `variants` is a list of dicts: {"mode": kernel mode or None, "records":
-    True/False}.  A sim with records off runs the step instance without the
+    True/False, "ws": (block, npt) to force the delivery-warp kernel in that
+    tile shape}.  A sim with records off runs the step instance without the
     optional features (when nothing else is switched on); its spike totals
     and every state bit are compared after each chunk.  A sim with records on
     has every raster row compared as well.  Stops at the first difference;
@@ -108,6 +109,10 @@ def lockstep_many(onet: O.ONet, steps: int, variants, int_weights: bool = True, 
         g = nb.B200Sim(flat, gc)
         if v.get("mode") is not None:
             g.set_kernel_mode(v["mode"])
+        if v.get("ws"):
+            g.set_tile_shape(*v["ws"])
+            g.set_delivery_warps(True)
+            assert g.delivery_warps() == (True, True)
         gs.append(g)
     if drive:
         drive(o)

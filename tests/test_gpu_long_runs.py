@@ -23,6 +23,8 @@ ADEX_TONIC = [281.0, 30.0, -70.6, -50.4, 2.0, 4.0, 144.0, 80.5, -70.6, 20.0]
 STREAM = {"mode": nb.KERNEL_STREAM}
 RESIDENT = {"mode": nb.KERNEL_RESIDENT}
 PLAIN = {"mode": nb.KERNEL_STREAM, "records": False}
+WS = {"mode": nb.KERNEL_STREAM, "ws": (256, 4)}                       # delivery warps, records on
+WS_PLAIN = {"mode": nb.KERNEL_STREAM, "records": False, "ws": (256, 4)}  # the instance the 1M bench picks
 
 
 def check(gs, o, firsts, variants, spikes=True):
@@ -67,7 +69,7 @@ def test_config_driven_full_1000_ms_bit_exact(n):
 def test_100k_active_regime_full_1000_ms_bit_exact():
     """The bench's active 100k regime: Gaussian noise sd 1 plus Poisson kicks
     100 Hz x 20 mV (~23 Hz firing, ~2e4 events per step), all 10,000 rows."""
-    variants = [STREAM, PLAIN]
+    variants = [STREAM, PLAIN, WS]
     gs, o, firsts = lockstep_many(O.ONet.random_kout(100_000, 100, 1), 10_000, variants, chunk=500, gauss_sd=1.0,
                                   synapse_tau_ms=5.0, noise_rate_hz=100.0, noise_kick_mv=20.0, seed=1)
     check(gs, o, firsts, variants)
@@ -79,8 +81,9 @@ def test_1m_active_regime_1000_steps_bit_exact():
     """1,000,000 neurons x K=100 (~1e8 synapses, a ~670 MB ring), Gaussian
     noise sd 1 plus Poisson kicks 100 Hz x 20 mV: ~2e5 synaptic events per
     step into the HBM-resident ring.  Records on (every raster row of 1000
-    steps) and off (the plain instance the bench times)."""
-    variants = [STREAM, PLAIN]
+    steps) and off (the plain instance the bench times), each with and
+    without delivery warps."""
+    variants = [STREAM, PLAIN, WS, WS_PLAIN]
     gs, o, firsts = lockstep_many(O.ONet.random_kout(1_000_000, 100, 1), 1000, variants, chunk=250, gauss_sd=1.0,
                                   synapse_tau_ms=5.0, noise_rate_hz=100.0, noise_kick_mv=20.0, seed=1)
     check(gs, o, firsts, variants)

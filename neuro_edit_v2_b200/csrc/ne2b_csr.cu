@@ -18,8 +18,9 @@
 //      always started; each wait is bounded by %globaltimer and a timeout is
 //      reported, never spun forever.  Finally each synapse is written to its
 //      place: target, Dale-signed weight (network.rs:668-672; quantised as
-//      kernels.rs:61 rt_put for the fixed-point ring), delay (u8 when the
-//      ring has at most 256 slots).
+//      kernels.rs:61 rt_put for the fixed-point ring) and delay, packed in
+//      one 8-byte record (target | delay << 24, weight bits), or the bare
+//      target and a separate u16 delay for a wide net (kNetDelayWide).
 //
 // The result equals the host build (ne2b_net_from_synapses, a stable
 // counting sort) bit for bit.
@@ -167,9 +168,9 @@ __global__ void __launch_bounds__(kThreads) csr_scatter_kernel(const uint32_t *_
                                                                const float *__restrict__ w,
                                                                const uint16_t *__restrict__ steps,
                                                                const uint8_t *__restrict__ kind, uint64_t E,
-                                                               uint32_t *cursor, uint32_t *__restrict__ tgt_out,
-                                                               void *__restrict__ w_out, void *__restrict__ delay_out,
-                                                               bool int_w, bool d16, uint32_t *ticket, uint32_t *done,
+                                                               uint32_t *cursor, SynRec *__restrict__ syn_out,
+                                                               uint16_t *__restrict__ delay16_out,
+                                                               bool int_w, bool wide, uint32_t *ticket, uint32_t *done,
                                                                CsrScalars *sc, unsigned long long limit_ns) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long *key = (unsigned long long *)smem;         // (source << 32) | position in the chunk
@@ -271,13 +272,12 @@ __global__ void __launch_bounds__(kThreads) csr_scatter_kernel(const uint32_t *_
         const uint32_t s = (uint32_t)(kv >> 32);
         const uint64_t j = j0 + (uint32_t)kv;
         const uint32_t pos = run_base[run_start[p]] + (p - run_start[p]);
-        tgt_out[pos] = tgt[j];
         const float m = fabsf(w[j]);
         const float ws = kind[s] == 1u ? -m : m;
-        if (int_w) ((int32_t *)w_out)[pos] = __float2int_rn(__fmul_rn(ws, 4096.0f));
-        else ((float *)w_out)[pos] = ws;
-        if (d16) ((uint16_t *)delay_out)[pos] = steps[j];
-        else ((uint8_t *)delay_out)[pos] = (uint8_t)steps[j];
+        const uint32_t wb = int_w ? (uint32_t)__float2int_rn(__fmul_rn(ws, 4096.0f)) : __float_as_uint(ws);
+        const uint32_t td = wide ? tgt[j] : tgt[j] | ((uint32_t)steps[j] << kSynTgtBits);
+        *reinterpret_cast<uint2 *>(syn_out + pos) = make_uint2(td, wb);
+        if (wide) delay16_out[pos] = steps[j];
     }
 }
 
@@ -305,8 +305,8 @@ cudaError_t csr_scan(const uint32_t *counts, uint32_t n, uint32_t e, uint32_t *r
 uint32_t csr_scan_blocks(uint32_t n) { return (n + kScan - 1) / kScan; }
 uint64_t csr_chunks(uint64_t n_syn) { return (n_syn + kChunk - 1) / kChunk; }
 
-cudaError_t csr_scatter(const DevSynapses &ds, const uint16_t *steps, uint32_t *cursor, uint32_t *tgt_out,
-                        void *w_out, void *delay_out, bool int_w, bool d16, uint32_t *ticket, uint32_t *done,
+cudaError_t csr_scatter(const DevSynapses &ds, const uint16_t *steps, uint32_t *cursor, SynRec *syn_out,
+                        uint16_t *delay16_out, bool int_w, bool wide, uint32_t *ticket, uint32_t *done,
                         CsrScalars *sc, unsigned long long limit_ns, cudaStream_t st) {
     const uint64_t chunks = csr_chunks(ds.n_syn);
     if (chunks == 0) return cudaSuccess;
@@ -314,7 +314,7 @@ cudaError_t csr_scatter(const DevSynapses &ds, const uint16_t *steps, uint32_t *
                                          (int)kScatterSmem);
     if (e != cudaSuccess) return e;
     csr_scatter_kernel<<<(unsigned)chunks, kThreads, kScatterSmem, st>>>(ds.src, ds.tgt, ds.w, steps, ds.kind, ds.n_syn, cursor,
-                                                              tgt_out, w_out, delay_out, int_w, d16, ticket, done, sc,
+                                                              syn_out, delay16_out, int_w, wide, ticket, done, sc,
                                                               limit_ns);
     return cudaGetLastError();
 }

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "ne2b_layout.h"
+
 namespace ne2b {
 
 // The synapse list and the per-neuron kinds, in device memory.
@@ -36,8 +38,8 @@ uint32_t csr_scan_blocks(uint32_t n);
 // Scatter blocks (8192 synapses each); `ticket` (one word) and `done`
 // (csr_chunks words) zeroed by the caller.
 uint64_t csr_chunks(uint64_t n_syn);
-cudaError_t csr_scatter(const DevSynapses &ds, const uint16_t *steps, uint32_t *cursor, uint32_t *tgt_out,
-                        void *w_out, void *delay_out, bool int_w, bool d16, uint32_t *ticket, uint32_t *done,
+cudaError_t csr_scatter(const DevSynapses &ds, const uint16_t *steps, uint32_t *cursor, SynRec *syn_out,
+                        uint16_t *delay16_out, bool int_w, bool wide, uint32_t *ticket, uint32_t *done,
                         CsrScalars *sc, unsigned long long limit_ns, cudaStream_t st);
 
 }  // namespace ne2b

@@ -513,10 +513,13 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
     NET_TRY(alloc(&p, sizeof(unsigned long long) * np)); d.pn_total = (unsigned long long *)p;
     NET_TRY(alloc(&p, sizeof(uint32_t) * (size_t)h->D * np)); d.ring = p;
     NET_TRY(alloc(&p, sizeof(uint32_t) * ((size_t)n + 1))); d.rowptr = (const uint32_t *)p;
-    NET_TRY(alloc(&p, sizeof(uint32_t) * h->e)); d.tgt = (const uint32_t *)p;
-    NET_TRY(alloc(&p, sizeof(uint32_t) * h->e)); d.w = p;
-    const bool d16 = h->D > 256;
-    NET_TRY(alloc(&p, (d16 ? 2 : 1) * h->e)); d.delay = p;
+    NET_TRY(alloc(&p, sizeof(SynRec) * h->e)); d.syn = (const SynRec *)p;
+    // delays past 8 bits, or targets past 24, do not fit the packed record
+    const bool wide = h->D > kSynMaxPackedDelay + 1u || n > kSynTgtMask + 1u;
+    if (wide) {
+        NET_TRY(alloc(&p, sizeof(uint16_t) * h->e));
+        d.delay16 = (const uint16_t *)p;
+    }
 
     tp[2] = now_ms();
     // host-side rows: params -> dictionary, x0
@@ -551,7 +554,7 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         // the list's CSR sorted into place on the device (csrc/ne2b_csr.cu)
         NET_TRY(cuda_error(csr_scan(dc->counts, n, (uint32_t)h->e, (uint32_t *)d.rowptr, dc->cursor, dc->sums, bst),
                            "device CSR: row pointers"));
-        NET_TRY(cuda_error(csr_scatter(dc->syn, dc->steps, dc->cursor, (uint32_t *)d.tgt, (void *)d.w, (void *)d.delay, int_ring_, d16,
+        NET_TRY(cuda_error(csr_scatter(dc->syn, dc->steps, dc->cursor, (SynRec *)d.syn, (uint16_t *)d.delay16, int_ring_, wide,
                                        dc->ticket, dc->done, dc->sc, 5000000000ull, bst),
                            "device CSR: scatter"));
         h->build_launches += (n ? 3 : 0) + (h->e ? 1 : 0);
@@ -559,56 +562,51 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         NET_TRY(up((void *)d.rowptr, net->src_ptr, sizeof(uint32_t) * ((size_t)n + 1)));
     }
     if (h->e && !dc) {
-        // one parallel pass over the synapses into pinned staging: targets
-        // copied, weights quantised (kernels.rs:61 rt_put: lrintf(w * 4096))
-        // for the fixed-point ring, delays narrowed to u8 when D <= 256;
+        // one parallel pass over the synapses into pinned staging: each
+        // record packs the target with its delay (u8) and the weight,
+        // quantised (kernels.rs:61 rt_put: lrintf(w * 4096)) for the
+        // fixed-point ring; a wide net's delays go to their own u16 array;
         // synapses [j0, j0 + m) into host buffers at their offset 0
         const bool iq = int_ring_;
-        const size_t db = d16 ? 2 : 1;
-        auto fill = [&](uint32_t *tg, void *wst, void *dst8, uint64_t j0, uint64_t m) {
+        auto fill = [&](SynRec *rec, uint16_t *d16, uint64_t j0, uint64_t m) {
             parallel_for(m, [&](uint64_t lo, uint64_t hi) {
-                if (tg) memcpy(tg + lo, net->tgt + j0 + lo, 4 * (hi - lo));
-                if (wst && iq) {
-                    int32_t *wq = (int32_t *)wst;
-                    for (uint64_t j = lo; j < hi; ++j) wq[j] = (int32_t)lrintf(net->w[j0 + j] * 4096.0f);
-                } else if (wst) {
-                    memcpy((float *)wst + lo, net->w + j0 + lo, 4 * (hi - lo));
-                }
-                if (dst8 && d16) {
-                    memcpy((uint16_t *)dst8 + lo, net->delay_steps + j0 + lo, 2 * (hi - lo));
-                } else if (dst8) {
-                    uint8_t *d8 = (uint8_t *)dst8;
-                    for (uint64_t j = lo; j < hi; ++j) d8[j] = (uint8_t)net->delay_steps[j0 + j];
-                }
+                if (rec)
+                    for (uint64_t j = lo; j < hi; ++j) {
+                        const uint64_t k = j0 + j;
+                        const float wf = net->w[k];
+                        uint32_t wb;
+                        if (iq) wb = (uint32_t)(int32_t)lrintf(wf * 4096.0f);
+                        else memcpy(&wb, &wf, 4);
+                        const uint32_t tg = net->tgt[k];
+                        rec[j].td = wide ? tg : tg | ((uint32_t)net->delay_steps[k] << kSynTgtBits);
+                        rec[j].w = wb;
+                    }
+                if (d16) memcpy(d16 + lo, net->delay_steps + j0 + lo, 2 * (hi - lo));
             });
         };
-        if (4 * h->e > 2 * Stager::kRingBytes) {
+        if (sizeof(SynRec) * h->e > 2 * Stager::kRingBytes) {
             // a large net streams through the stager's ring of pinned blocks
-            const uint64_t per = Stager::kRingBytes / 4;
+            const uint64_t per = Stager::kRingBytes / sizeof(SynRec);
             for (uint64_t j0 = 0; j0 < h->e; j0 += per) {
                 const uint64_t m = std::min<uint64_t>(per, h->e - j0);
                 void *hb = nullptr;
                 NET_TRY(sg.ring_next(&hb));
-                fill((uint32_t *)hb, nullptr, nullptr, j0, m);
-                NET_TRY(sg.ring_issue((uint32_t *)d.tgt + j0, 4 * m));
-                NET_TRY(sg.ring_next(&hb));
-                fill(nullptr, hb, nullptr, j0, m);
-                NET_TRY(sg.ring_issue((uint32_t *)d.w + j0, 4 * m));
-                NET_TRY(sg.ring_next(&hb));
-                fill(nullptr, nullptr, hb, j0, m);
-                NET_TRY(sg.ring_issue((uint8_t *)d.delay + db * j0, db * m));
+                fill((SynRec *)hb, nullptr, j0, m);
+                NET_TRY(sg.ring_issue((SynRec *)d.syn + j0, sizeof(SynRec) * m));
+                if (wide) {
+                    NET_TRY(sg.ring_next(&hb));
+                    fill(nullptr, (uint16_t *)hb, j0, m);
+                    NET_TRY(sg.ring_issue((uint16_t *)d.delay16 + j0, sizeof(uint16_t) * m));
+                }
             }
         } else {
-            uint32_t *tg = nullptr;
-            void *wst = nullptr;
-            void *dst8 = nullptr;
-            NET_TRY(sg.reserve(4 * h->e, (void **)&tg));
-            NET_TRY(sg.reserve(4 * h->e, &wst));
-            NET_TRY(sg.reserve(db * h->e, &dst8));
-            fill(tg, wst, dst8, 0, h->e);
-            NET_TRY(sg.issue((void *)d.tgt, tg, 4 * h->e));
-            NET_TRY(sg.issue((void *)d.w, wst, 4 * h->e));
-            NET_TRY(sg.issue((void *)d.delay, dst8, db * h->e));
+            SynRec *rec = nullptr;
+            uint16_t *d16 = nullptr;
+            NET_TRY(sg.reserve(sizeof(SynRec) * h->e, (void **)&rec));
+            if (wide) NET_TRY(sg.reserve(sizeof(uint16_t) * h->e, (void **)&d16));
+            fill(rec, d16, 0, h->e);
+            NET_TRY(sg.issue((void *)d.syn, rec, sizeof(SynRec) * h->e));
+            if (wide) NET_TRY(sg.issue((void *)d.delay16, d16, sizeof(uint16_t) * h->e));
         }
     }
     if (any_tau) {
@@ -726,7 +724,7 @@ ne2b_status Engine::build_net(const ne2b_net_desc *net, const ne2b_config *cfg, 
         d.trace_last = (uint32_t)tab.size() - 1;
     }
     fill_noise(d, *cfg);
-    d.flags = kNetActive | (d16 ? kNetDelay16 : 0u) | (rec_rows ? kNetRecord : 0u) |
+    d.flags = kNetActive | (wide ? kNetDelayWide : 0u) | (rec_rows ? kNetRecord : 0u) |
               (cfg->window_steps ? kNetWindows : 0u) | (any_adex ? kNetHasAdex : 0u) | (h->nx ? kNetXsyn : 0u) |
               (d.trace_f ? kNetTraceF32 : 0u);
     tp[5] = now_ms();
@@ -1165,18 +1163,18 @@ ne2b_status Engine::run_steps(uint64_t steps) {
 ne2b_status Engine::read_csr(NetHost &h, uint32_t *rowptr, uint32_t *tgt, uint32_t *w_bits, uint16_t *delay_steps) {
     const NetDev &d = h.dev;
     if (rowptr) NE2B_CUDA(cudaMemcpyAsync(rowptr, d.rowptr, sizeof(uint32_t) * ((size_t)h.n + 1), cudaMemcpyDeviceToHost, stream_));
-    if (h.e) {
-        if (tgt) NE2B_CUDA(cudaMemcpyAsync(tgt, d.tgt, sizeof(uint32_t) * h.e, cudaMemcpyDeviceToHost, stream_));
-        if (w_bits) NE2B_CUDA(cudaMemcpyAsync(w_bits, d.w, sizeof(uint32_t) * h.e, cudaMemcpyDeviceToHost, stream_));
-        if (delay_steps) {
-            if (d.flags & kNetDelay16) {
-                NE2B_CUDA(cudaMemcpyAsync(delay_steps, d.delay, sizeof(uint16_t) * h.e, cudaMemcpyDeviceToHost, stream_));
-            } else {
-                std::vector<uint8_t> d8(h.e);
-                NE2B_CUDA(cudaMemcpyAsync(d8.data(), d.delay, h.e, cudaMemcpyDeviceToHost, stream_));
-                NE2B_CUDA(cudaStreamSynchronize(stream_));
-                for (uint64_t j = 0; j < h.e; ++j) delay_steps[j] = d8[j];
-            }
+    const bool wide = d.flags & kNetDelayWide;
+    if (h.e && (tgt || w_bits || delay_steps)) {
+        // unpack the records (target | delay << 24, weight bits)
+        std::vector<SynRec> rec(h.e);
+        NE2B_CUDA(cudaMemcpyAsync(rec.data(), d.syn, sizeof(SynRec) * h.e, cudaMemcpyDeviceToHost, stream_));
+        if (delay_steps && wide)
+            NE2B_CUDA(cudaMemcpyAsync(delay_steps, d.delay16, sizeof(uint16_t) * h.e, cudaMemcpyDeviceToHost, stream_));
+        NE2B_CUDA(cudaStreamSynchronize(stream_));
+        for (uint64_t j = 0; j < h.e; ++j) {
+            if (tgt) tgt[j] = wide ? rec[j].td : rec[j].td & kSynTgtMask;
+            if (w_bits) w_bits[j] = rec[j].w;
+            if (delay_steps && !wide) delay_steps[j] = (uint16_t)(rec[j].td >> kSynTgtBits);
         }
     }
     NE2B_CUDA(cudaStreamSynchronize(stream_));

@@ -11,8 +11,11 @@
 //     pn_total (u64 lifetime spike counts), wcount (u32 current-window counts)
 //   delay ring: D x n_pad words (int32 fixed point or f32), slot-major, so the
 //     neuron pass reads one contiguous slot row per step
-//   CSR by source: rowptr[n+1] (u32, local), tgt[E] (u32, local), w[E]
-//     (int32 = lrintf(w*4096) or f32), delay[E] (u8 when D <= 256, else u16)
+//   CSR by source: rowptr[n+1] (u32, local) and one 8-byte record per
+//     synapse, syn[E] = {target | delay << 24, weight bits (int32 =
+//     lrintf(w*4096) or f32)}, read with one 64-bit load; a net whose delays
+//     exceed 255 steps or whose targets exceed 24 bits (kNetDelayWide) keeps
+//     the bare target in the record and its delays in delay16[E] (u16)
 //   stimulus: neuron-major (input, weight) rows and a [steps x n_inputs] f32
 //     value buffer; spike record: rows x n_pad/32 u32 words; window counts:
 //     max_windows x n_pad u16.
@@ -26,7 +29,7 @@ constexpr uint32_t kMaxParams = 12;
 
 enum NetFlags : uint32_t {
     kNetHasExt = 1u << 0,
-    kNetDelay16 = 1u << 1,
+    kNetDelayWide = 1u << 1,  // delays in delay16[], bare targets in the records
     kNetRecord = 1u << 2,
     kNetWindows = 1u << 3,
     kNetActive = 1u << 4,
@@ -56,6 +59,16 @@ struct alignas(16) Tile {
     uint32_t pad[3];
 };
 
+// One synapse of the CSR: td = target | delay_steps << 24 (or the bare
+// target with kNetDelayWide), w = weight bits.
+struct alignas(8) SynRec {
+    uint32_t td;
+    uint32_t w;
+};
+constexpr uint32_t kSynTgtBits = 24;
+constexpr uint32_t kSynTgtMask = (1u << kSynTgtBits) - 1u;
+constexpr uint32_t kSynMaxPackedDelay = 255u;
+
 constexpr uint16_t kTraceZero = 0xFFFFu;  // tk value of a zero trace
 constexpr uint32_t kNoXsyn = 0xFFFFFFFFu;  // xmap value of a synapse on the merged ring
 constexpr uint32_t kWatchCap = 4096;       // samples kept per watched neuron (cpu.rs:78 V_HIST_CAP)
@@ -80,9 +93,8 @@ struct alignas(16) NetDev {
     void *ring;
     // csr
     const uint32_t *rowptr;
-    const uint32_t *tgt;
-    const void *w;          // int32 or f32
-    const void *delay;      // u8 or u16
+    const SynRec *syn;        // [E]
+    const uint16_t *delay16;  // [E], kNetDelayWide only
     // stimulus
     const uint32_t *stim_ptr;
     const uint32_t *stim_in;

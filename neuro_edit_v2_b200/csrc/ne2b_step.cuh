@@ -431,11 +431,11 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     __syncthreads();
     if (threadIdx.x == 0) atomicAdd(&eng->counters[tile.net].spikes_total, (unsigned long long)total);
     // ---- delivery: the block strides the flat synapse range; a thread
-    // finds its row by binary search over off[], then adds the weight into
+    // finds its row by binary search over off[], loads the synapse's 8-byte
+    // record (target | delay << 24, weight bits), then adds the weight into
     // ring[(t + d) % D][tgt] with a no-return atomic
-    const uint32_t *__restrict__ tgt = nd.tgt;
-    const uint32_t *__restrict__ wbits = (const uint32_t *)nd.w;
-    const bool d16 = flags & kNetDelay16;
+    const SynRec *__restrict__ csr = nd.syn;
+    const bool wide = flags & kNetDelayWide;
     auto syn_at = [&](uint32_t f) {
         uint32_t lo = 0, hi = total;  // off[lo] <= f < off[hi]
         while (hi - lo > 1) {
@@ -445,10 +445,12 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         }
         return sl.lo[lo] + (f - sl.off[lo]);
     };
-    auto slot_of = [&](uint32_t j) {
-        const uint32_t d = d16 ? (uint32_t)((const uint16_t *)nd.delay)[j] : (uint32_t)((const uint8_t *)nd.delay)[j];
-        const uint32_t slot = tmod + d;
-        return slot >= D ? slot - D : slot;
+    // the record's target and arrival slot
+    auto unpack = [&](uint32_t j, const uint2 r, uint32_t &tg, uint32_t &slot) {
+        const uint32_t d = wide ? (uint32_t)nd.delay16[j] : r.x >> kSynTgtBits;
+        tg = wide ? r.x : r.x & kSynTgtMask;
+        slot = tmod + d;
+        if (slot >= D) slot -= D;
     };
     auto add = [&](uint32_t slot, uint32_t tg, uint32_t wb) {
         const size_t idx = (size_t)slot * n_pad + tg;
@@ -470,9 +472,9 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             for (int q = 1; q < U; ++q) j[q] = f + q * BLOCK < nsyn ? syn_at(f + q * BLOCK) : j[0];
 #pragma unroll
             for (int q = 0; q < U; ++q) {
-                tg[q] = tgt[j[q]];
-                sl_[q] = slot_of(j[q]);
-                wb[q] = wbits[j[q]];
+                const uint2 r = *reinterpret_cast<const uint2 *>(csr + j[q]);
+                unpack(j[q], r, tg[q], sl_[q]);
+                wb[q] = r.y;
             }
 #pragma unroll
             for (int q = 0; q < U; ++q)
@@ -483,8 +485,9 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     }
     for (uint32_t f = threadIdx.x; f < nsyn; f += BLOCK) {
         const uint32_t j = syn_at(f);
-        const uint32_t tg = tgt[j];
-        const uint32_t slot = slot_of(j);
+        const uint2 r = *reinterpret_cast<const uint2 *>(csr + j);
+        uint32_t tg, slot;
+        unpack(j, r, tg, slot);
         {
             const uint32_t k = nd.xmap[j];
             if (k != kNoXsyn) {  // its own current: mark the arrival (cpu.rs:270-273)
@@ -492,7 +495,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
                 continue;
             }
         }
-        add(slot, tg, wbits[j]);
+        add(slot, tg, r.y);
     }
     // the next tile reuses the shared lists
     __syncthreads();
@@ -703,10 +706,10 @@ __global__ void __launch_bounds__(BLOCK + 32 * ws_warps<BLOCK>()) step_kernel_ws
     // ---- delivery warps
     constexpr int U = kDeliverUnroll<INT>;
     uint32_t *__restrict__ ringw = (uint32_t *)s_nd.ring;
-    const uint32_t *__restrict__ tgt = s_nd.tgt;
-    const uint32_t *__restrict__ wbits = (const uint32_t *)s_nd.w;
+    const SynRec *__restrict__ syn = s_nd.syn;
+    const uint16_t *__restrict__ delay16 = s_nd.delay16;
     const uint32_t n_pad = s_nd.n_pad, D = s_nd.D;
-    const bool d16 = s_nd.flags & kNetDelay16;
+    const bool wide = s_nd.flags & kNetDelayWide;
     const bool xsyn_on = !PLAIN && (s_nd.flags & kNetXsyn);
     const uint32_t e_total = s_nd.rowptr[s_nd.n];  // a queued row must lie inside the CSR
     for (;;) {
@@ -754,12 +757,12 @@ __global__ void __launch_bounds__(BLOCK + 32 * ws_warps<BLOCK>()) step_kernel_ws
             for (int q = 1; q < U; ++q) j[q] = f + 32u * q < cnt ? rlo + f + 32u * q : j[0];
 #pragma unroll
             for (int q = 0; q < U; ++q) {
-                tg[q] = tgt[j[q]];
-                const uint32_t d = d16 ? (uint32_t)((const uint16_t *)s_nd.delay)[j[q]]
-                                       : (uint32_t)((const uint8_t *)s_nd.delay)[j[q]];
+                const uint2 r = *reinterpret_cast<const uint2 *>(syn + j[q]);  // target | delay << 24, weight
+                const uint32_t d = wide ? (uint32_t)delay16[j[q]] : r.x >> kSynTgtBits;
+                tg[q] = wide ? r.x : r.x & kSynTgtMask;
                 const uint32_t slot = tmod + d;
                 sl_[q] = slot >= D ? slot - D : slot;
-                wb[q] = wbits[j[q]];
+                wb[q] = r.y;
             }
 #pragma unroll
             for (int q = 0; q < U; ++q) {

@@ -557,7 +557,7 @@ constexpr uint32_t kStageTiles = 16;
 // PLAIN: the lean instance; single-net, it also drops the input features
 // (LEAN and NOIO), many-net only the others (LEAN).
 template <bool INT, int BLOCK, int NPT, bool ADEX, bool MULTI, bool PLAIN>
-__global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
+__device__ __forceinline__ void step_body(const EngineDev *__restrict__ eng, uint32_t k_step) {
     pdl_trigger();
     constexpr uint32_t kNetWords = sizeof(NetDev) / 16;
     __shared__ uint32_t s_lists[smem_lists_words<BLOCK, NPT>()];
@@ -637,6 +637,23 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict
                                                             s_nd.pidx + tile.start, sl);
         }
     }
+}
+
+template <bool INT, int BLOCK, int NPT, bool ADEX, bool MULTI, bool PLAIN>
+__global__ void __launch_bounds__(BLOCK) step_kernel(const EngineDev *__restrict__ eng, uint32_t k_step) {
+    step_body<INT, BLOCK, NPT, ADEX, MULTI, PLAIN>(eng, k_step);
+}
+
+// The plain single-net instance at one neuron per thread, held to 64
+// registers (1,024 resident threads per SM), which its code fits without
+// spilling.  Left to its own heuristic the compiler chose 56 registers and
+// a spill on the critical path of the 100k step (128 x 1: 2.28 against
+// 1.94 us per step, one box).  The other instances keep the compiler's
+// choice: the same cap made them spill or run slower.
+template <bool INT, int BLOCK, bool ADEX>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) step_kernel_r64(const EngineDev *__restrict__ eng,
+                                                                       uint32_t k_step) {
+    step_body<INT, BLOCK, 1, ADEX, false, true>(eng, k_step);
 }
 
 // ------------------------------------------- warp-specialised streaming kernel
@@ -939,6 +956,8 @@ int StepKind<INT, ADEX>::occupancy(uint32_t block, uint32_t npt, int variant) {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX, true, false>, B, 0);  \
         else if (variant == kStepMultiLean)                                                                     \
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX, true, true>, B, 0);   \
+        else if (variant == kStepPlain && P == 1)                                                               \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel_r64<INT, B, ADEX>, B, 0);              \
         else if (variant == kStepPlain)                                                                         \
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, step_kernel<INT, B, P, ADEX, false, true>, B, 0);  \
         else                                                                                                    \
@@ -971,6 +990,8 @@ cudaError_t StepKind<INT, ADEX>::launch(uint32_t block, uint32_t npt, int varian
                    ? launch_pdl(step_kernel<INT, B, P, ADEX, true, false>, grid, B, st, k_step > 0, eng, k_step)  \
                : variant == kStepMultiLean                                                                        \
                    ? launch_pdl(step_kernel<INT, B, P, ADEX, true, true>, grid, B, st, k_step > 0, eng, k_step)   \
+               : variant == kStepPlain && P == 1                                                                  \
+                   ? launch_pdl(step_kernel_r64<INT, B, ADEX>, grid, B, st, k_step > 0, eng, k_step)              \
                : variant == kStepPlain                                                                            \
                    ? launch_pdl(step_kernel<INT, B, P, ADEX, false, true>, grid, B, st, k_step > 0, eng, k_step)  \
                    : launch_pdl(step_kernel<INT, B, P, ADEX, false, false>, grid, B, st, k_step > 0, eng, k_step);

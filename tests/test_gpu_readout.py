@@ -121,3 +121,23 @@ def test_arguments_the_reference_rejects():
         nb.fit_ridge_multi(x, np.full(10, 3), 3, 1.0)
     with pytest.raises(nb.Ne2bError, match="T >= 2"):
         nb.fit_ridge_multi(x[:1], np.zeros(1), 2, 1.0)
+
+
+def test_reference_readout_cases_on_the_device():
+    """The reference's own readout tests (sim/src/readout.rs:310-376) through
+    the device solvers: the weights equal the oracle's bit for bit and meet
+    the reference's bars (weights 2, -1, bias 0.5 within 1e-3; dual and
+    primal scores within 1e-4)."""
+    from test_oracle_kats import reference_ridge_dual_case, reference_ridge_linear_case, ridge_output
+
+    x, y = reference_ridge_linear_case()
+    w = nb.fit_ridge(x, y, 1e-9)
+    assert np.array_equal(w.view(np.uint64), O.fit_ridge(x, y, 1e-9).view(np.uint64))
+    assert abs(w[0] - 2.0) < 1e-3 and abs(w[1] + 1.0) < 1e-3 and abs(w[2] - 0.5) < 1e-3, w
+    x, lab, k = reference_ridge_dual_case()
+    ws = nb.fit_ridge_multi(x, lab, k, 0.7)
+    assert np.array_equal(ws.view(np.uint64), O.fit_ridge_multi(x, lab, k, 0.7).view(np.uint64))
+    for c in range(k):
+        wp = nb.fit_ridge(x, (lab == c).astype(np.float32), 0.7)
+        for r in range(x.shape[0]):
+            assert abs(ridge_output(wp, x[r]) - ridge_output(ws[c], x[r])) < 1e-4, (c, r)

@@ -497,3 +497,47 @@ def test_ridge_oracle_equals_the_normal_equations():
     a[f, f] -= lam
     ref = np.linalg.solve(a, x1.T @ y.astype(np.float64))
     assert np.abs(w - ref).max() < 1e-11 * max(1.0, np.abs(ref).max())
+
+
+def reference_ridge_linear_case():
+    """The design of sim/src/readout.rs:311-321 (ridge_fits_linear): six
+    samples of two features, y = 2 x0 - x1 + 0.5 computed in f32."""
+    x = np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0], [1.0, 1.0], [2.0, 1.0], [-1.0, 2.0]], np.float32)
+    y = (np.float32(2.0) * x[:, 0] - x[:, 1] + np.float32(0.5)).astype(np.float32)
+    return x, y
+
+
+def reference_ridge_dual_case():
+    """The design of sim/src/readout.rs:355-360 (ridge_multi_dual_matches_primal):
+    Rng(3), 40 x 7 features uniform in [-1, 1) as f32, labels row % 3."""
+    r = O.rng(3)
+    t, f, k = 40, 7, 3
+    x = np.array([np.float32(-1.0 + 2.0 * O.lib().ne2o_rng_f64(O.C.byref(r))) for _ in range(t * f)],
+                 np.float32).reshape(t, f)
+    return x, np.arange(t) % k, k
+
+
+def ridge_output(w, row):
+    """sim/src/readout.rs:254-262: bias first, then the features in order, in f64."""
+    s = float(w[-1])
+    for i in range(len(row)):
+        s += float(w[i]) * float(row[i])
+    return s
+
+
+def test_ridge_fits_linear_reference_case():
+    """readout.rs:310-326: weights 2, -1 and bias 0.5 within 1e-3 at lambda 1e-9."""
+    x, y = reference_ridge_linear_case()
+    w = O.fit_ridge(x, y, 1e-9)
+    assert abs(w[0] - 2.0) < 1e-3 and abs(w[1] + 1.0) < 1e-3 and abs(w[2] - 0.5) < 1e-3, w
+
+
+def test_ridge_multi_dual_matches_primal_reference_case():
+    """readout.rs:354-375: each class's dual (multi) readout scores every row
+    within 1e-4 of the primal binary readout trained on that class."""
+    x, lab, k = reference_ridge_dual_case()
+    ws = O.fit_ridge_multi(x, lab, k, 0.7)
+    for c in range(k):
+        wp = O.fit_ridge(x, (lab == c).astype(np.float32), 0.7)
+        for r in range(x.shape[0]):
+            assert abs(ridge_output(wp, x[r]) - ridge_output(ws[c], x[r])) < 1e-4, (c, r)

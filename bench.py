@@ -526,6 +526,10 @@ def bench_1m(nb, torch, scrub, model: int, steps: int, warmup: int, peak: float)
 
     def measure(kick_hz):
         sim.set_noise(kick_hz, 20.0 if kick_hz else 0.0)
+        # tune on a state inside the regime (half a trial from reset), not on
+        # the state the previous regime left
+        sim.reset_state()
+        sim.run_steps(trial // 2)
         tiling = sim.autotune(128)
         ms, spikes, launches = timed_trials(sim, steps, warmup, trial, 1, torch, scrub)
         per_launch_s = ms / 1000.0 / (trial * steps)

@@ -125,6 +125,21 @@ __device__ __forceinline__ bool ws_wait_turn(const uint32_t *turn, uint32_t want
 // trace or watches; NOIO: nor an external current, a stimulus or windows.
 // Their code is compiled out (the engine launches such an instance only
 // then).
+// A ring arrival: a no-return add whose L2 line is marked evict-first, so
+// the random ring lines of a large net do not push the neuron state (read
+// and written every step) out of L2.
+__device__ __forceinline__ uint64_t ring_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+template <bool INT>
+__device__ __forceinline__ void ring_add(uint32_t *word, uint32_t wb, uint64_t pol) {
+    if (INT) asm volatile("red.global.add.L2::cache_hint.s32 [%0], %1, %2;" ::"l"(word), "r"(wb), "l"(pol) : "memory");
+    else asm volatile("red.global.add.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(word), "f"(__uint_as_float(wb)), "l"(pol)
+                      : "memory");
+}
+
 // WSQ (step_kernel_ws): the tile's threads are the producer warps of a
 // delivery queue; they push their spiking neurons' rows into `wq` and count
 // their spikes into *nspk (per warp) instead of compacting and delivering.
@@ -452,10 +467,10 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
         slot = tmod + d;
         if (slot >= D) slot -= D;
     };
+    const uint64_t pol = ring_policy();
     auto add = [&](uint32_t slot, uint32_t tg, uint32_t wb) {
         const size_t idx = (size_t)slot * n_pad + tg;
-        if (INT) atomicAdd((int *)ringw + idx, (int)wb);
-        else atomicAdd((float *)ringw + idx, __uint_as_float(wb));
+        ring_add<INT>(ringw + idx, wb, pol);
     };
     if (!xsyn_on) {
         // U synapses per thread and pass, all their loads issued before any
@@ -729,6 +744,7 @@ __global__ void __launch_bounds__(BLOCK + 32 * ws_warps<BLOCK>()) step_kernel_ws
     const bool wide = s_nd.flags & kNetDelayWide;
     const bool xsyn_on = !PLAIN && (s_nd.flags & kNetXsyn);
     const uint32_t e_total = s_nd.rowptr[s_nd.n];  // a queued row must lie inside the CSR
+    const uint64_t pol = ring_policy();
     for (;;) {
         uint32_t pos = 0;
         if (lane == 0) pos = atomicAdd(&s_ctr[1], 1u);
@@ -792,8 +808,7 @@ __global__ void __launch_bounds__(BLOCK + 32 * ws_warps<BLOCK>()) step_kernel_ws
                     }
                 }
                 const size_t idx = (size_t)sl_[q] * n_pad + tg[q];
-                if (INT) atomicAdd((int *)ringw + idx, (int)wb[q]);
-                else atomicAdd((float *)ringw + idx, __uint_as_float(wb[q]));
+                ring_add<INT>(ringw + idx, wb[q], pol);
             }
         }
     }

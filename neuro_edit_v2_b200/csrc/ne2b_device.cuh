@@ -48,15 +48,27 @@ __device__ __forceinline__ bool noise_fires(uint64_t base, float p) {
     return __fmul_rn(__uint2float_rn(h), 2.3283064e-10f) < p;
 }
 
-// Gaussian current numerator: the four 16-bit fields of one splitmix64 hash
-// of base + G (G = 0xD1B54A32D192ED03) summed (Irwin-Hall, 4 terms) minus the
-// mean 131070.  Multiplied by sd*sqrt(3)/65536 it has mean 0 and variance
-// 1 - 2^-32.  Integer-exact, so CPU and GPU agree bit-for-bit.
-__device__ __forceinline__ int32_t gauss_numer(uint64_t base) {
-    uint64_t h = mix64(base + 0xD1B54A32D192ED03ull);
-    uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
-    int32_t s = (int32_t)((lo & 0xffffu) + (lo >> 16) + (hi & 0xffffu) + (hi >> 16));
-    return s - 131070;
+// Gaussian current numerator for neuron i at the step whose noise step part
+// (noise_base_step) is `step`: one 32-bit hash, x = i XOR the step part's
+// low half through the lowbias32 mixer (C. Wellons' hash-prospector), then
+// its high half folded in by one multiply-xorshift round; the four bytes of
+// x summed (Irwin-Hall, 4 uniforms on [0, 255]) minus the mean 510.
+// Multiplied by sd*sqrt(3)/256 it has mean 0 and variance 1 - 2^-16; tails
+// end at +-3.45 sd.  32-bit integer operations only (the 64-bit splitmix64
+// draw it replaces cost the 1M step 15% of its time), integer-exact, so CPU
+// and GPU agree bit for bit.
+__device__ __forceinline__ int32_t gauss_numer(uint32_t i, uint64_t step) {
+    uint32_t x = i ^ (uint32_t)step;
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    x ^= (uint32_t)(step >> 32);
+    x *= 0x9e3779b1u;
+    x ^= x >> 16;
+    const uint32_t pairs = (x & 0x00ff00ffu) + ((x >> 8) & 0x00ff00ffu);  // two 16-bit byte-pair sums
+    return (int32_t)((pairs & 0xffffu) + (pairs >> 16)) - 510;
 }
 
 // Deterministic exp(x) for the AdEx step: Cody-Waite reduction x = k*ln2 + r

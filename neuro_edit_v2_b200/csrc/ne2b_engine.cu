@@ -238,7 +238,7 @@ static float host_decay(float dt, float tau) {
 static void fill_noise(NetDev &d, const ne2b_config &c) {
     d.pkick = c.noise_rate_hz * c.dt_ms / 1000.0f;                 // cpu.rs:197
     d.kick = c.noise_kick_mv != 0.0f ? c.noise_kick_mv / c.dt_ms : 0.0f;  // cpu.rs:198-202
-    d.gauss_k = c.gauss_sd != 0.0f ? (float)((double)c.gauss_sd * 1.7320508075688772 / 65536.0) : 0.0f;
+    d.gauss_k = c.gauss_sd != 0.0f ? (float)((double)c.gauss_sd * 1.7320508075688772 / 256.0) : 0.0f;
 }
 
 Stager::~Stager() {

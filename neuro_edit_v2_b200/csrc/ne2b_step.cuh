@@ -280,12 +280,9 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
             p[8] = p2.x; p[9] = p2.y;
         }
         const float gain = (ADEX && adex) ? p[0] : 1.0f;  // model/mod.rs:104-106, adex.rs:189-191
-        if (pkick > 0.0f || gauss_k != 0.0f) {
-            const uint64_t base = noise_base_at(i, nbase);
-            if (pkick > 0.0f && noise_fires(base, pkick)) I = __fadd_rn(I, __fmul_rn(kick, gain));
-            if (gauss_k != 0.0f)
-                I = __fadd_rn(I, __fmul_rn(__int2float_rn(gauss_numer(base)), __fmul_rn(gauss_k, gain)));
-        }
+        if (pkick > 0.0f && noise_fires(noise_base_at(i, nbase), pkick)) I = __fadd_rn(I, __fmul_rn(kick, gain));
+        if (gauss_k != 0.0f)
+            I = __fadd_rn(I, __fmul_rn(__int2float_rn(gauss_numer(i, nbase)), __fmul_rn(gauss_k, gain)));
         bool sp;
         if (ADEX && adex) sp = adex_step(p, v[q], u[q], I, dt);
         else sp = izh_step(p, v[q], u[q], I, dt);

@@ -494,20 +494,32 @@ int ne2o_noise_fires(uint32_t i, uint64_t t, uint64_t seed, float p) {
     return (float)ne2o_noise_hash(i, t, seed) * 2.3283064e-10f < p;
 }
 /* Gaussian current noise (project definition, not in the reference): the
- * (i, t, seed) base of noise_hash offset by G = 0xD1B54A32D192ED03 goes
- * through the splitmix64 finaliser once; its four 16-bit fields are
- * uniforms on [0, 65535] and their sum S is Irwin-Hall(4) with mean 131070
- * and variance 4*(65536^2-1)/12, so (S - 131070) * sqrt(3)/65536 has mean 0
- * and variance 1 - 2^-32.  Integer-exact on CPU and GPU; tails end at
- * +-2*sqrt(3) sd. */
+ * step part of the noise base, st = t*0xBF58476D1CE4E5B9 + seed*0x94D049BB133111EB
+ * (noise_base without the neuron term), and the neuron index give one 32-bit
+ * hash: x = i ^ lo32(st) through the lowbias32 mixer (x ^= x>>16;
+ * x *= 0x7feb352d; x ^= x>>15; x *= 0x846ca68b; x ^= x>>16; C. Wellons'
+ * hash-prospector), then x ^= hi32(st); x *= 0x9e3779b1; x ^= x>>16.  Its
+ * four bytes are uniforms on [0, 255]; their sum S is Irwin-Hall(4) with
+ * mean 510 and variance 4*(256^2-1)/12, so (S - 510) * sqrt(3)/256 has mean 0
+ * and variance 1 - 2^-16.  Integer-exact on CPU and GPU; tails end at
+ * +-510*sqrt(3)/256 = 3.45 sd. */
 int64_t ne2o_gauss_numer(uint32_t i, uint64_t t, uint64_t seed) {
-    uint64_t h = mix64(noise_base(i, t, seed) + 0xD1B54A32D192ED03ull);
-    int64_t s = (int64_t)(h & 0xffff) + (int64_t)((h >> 16) & 0xffff) + (int64_t)((h >> 32) & 0xffff) +
-                (int64_t)(h >> 48);
-    return s - 131070;
+    const uint64_t st = t * 0xBF58476D1CE4E5B9ull + seed * 0x94D049BB133111EBull;
+    uint32_t x = i ^ (uint32_t)st;
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    x ^= (uint32_t)(st >> 32);
+    x *= 0x9e3779b1u;
+    x ^= x >> 16;
+    const int64_t s = (int64_t)(x & 0xff) + (int64_t)((x >> 8) & 0xff) + (int64_t)((x >> 16) & 0xff) +
+                      (int64_t)(x >> 24);
+    return s - 510;
 }
 float ne2o_gauss_scale(float sd) {
-    return (float)((double)sd * 1.7320508075688772 / 65536.0);
+    return (float)((double)sd * 1.7320508075688772 / 256.0);
 }
 
 /* ===================================================== deterministic exp */

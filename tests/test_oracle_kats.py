@@ -363,12 +363,38 @@ def test_det_expf_against_libm():
 
 
 def test_gauss_noise_moments():
-    """Project noise definition: mean 0, variance 1 - 2^-32 on a seeded sample."""
-    z = np.array([O.gauss_numer(i, t, 5) for i in range(200) for t in range(200)], dtype=np.float64)
-    z *= math.sqrt(3.0) / 65536.0
-    assert abs(z.mean()) < 0.02
-    assert abs(z.var() - 1.0) < 0.03
-    assert np.abs(z).max() <= 2 * math.sqrt(3.0)
+    """Project noise definition: mean 0, variance 1 - 2^-16, the kurtosis of
+    a sum of four uniforms (3 - 6/20 = 2.7) on a seeded sample, and no
+    correlation between neighbouring neurons or steps."""
+    z = np.array([[O.gauss_numer(i, t, 5) for t in range(300)] for i in range(300)], dtype=np.float64)
+    assert z.min() >= -510 and z.max() <= 510
+    z *= math.sqrt(3.0) / 256.0
+    assert abs(z.mean()) < 0.01
+    assert abs(z.var() - 1.0) < 0.02
+    kurt = ((z - z.mean()) ** 4).mean() / z.var() ** 2
+    assert abs(kurt - 2.7) < 0.05, kurt
+    for a, b in ((z[1:, :], z[:-1, :]), (z[:, 1:], z[:, :-1])):
+        assert abs(np.corrcoef(a.ravel(), b.ravel())[0, 1]) < 0.02
+
+
+def test_gauss_noise_known_answers():
+    """The definition written out in Python integers on a few (i, t, seed)."""
+    def ref(i, t, seed):
+        m = (1 << 64) - 1
+        st = (t * 0xBF58476D1CE4E5B9 + seed * 0x94D049BB133111EB) & m
+        x = i ^ (st & 0xFFFFFFFF)
+        x ^= x >> 16
+        x = (x * 0x7FEB352D) & 0xFFFFFFFF
+        x ^= x >> 15
+        x = (x * 0x846CA68B) & 0xFFFFFFFF
+        x ^= x >> 16
+        x ^= st >> 32
+        x = (x * 0x9E3779B1) & 0xFFFFFFFF
+        x ^= x >> 16
+        return sum((x >> s) & 0xFF for s in (0, 8, 16, 24)) - 510
+
+    for i, t, seed in ((0, 0, 0), (1, 0, 0), (0, 1, 0), (12345, 678, 9), (2**32 - 1, 2**40 + 3, 2**63 + 5)):
+        assert O.gauss_numer(i, t, seed) == ref(i, t, seed), (i, t, seed)
 
 
 # --- editor watches (sim/tests/v_watch.rs, sim/tests/grid_trace.rs) ---------

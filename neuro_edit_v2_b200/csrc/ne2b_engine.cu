@@ -1164,17 +1164,22 @@ ne2b_status Engine::read_csr(NetHost &h, uint32_t *rowptr, uint32_t *tgt, uint32
     const NetDev &d = h.dev;
     if (rowptr) NE2B_CUDA(cudaMemcpyAsync(rowptr, d.rowptr, sizeof(uint32_t) * ((size_t)h.n + 1), cudaMemcpyDeviceToHost, stream_));
     const bool wide = d.flags & kNetDelayWide;
+    if (delay_steps && wide && h.e)
+        NE2B_CUDA(cudaMemcpyAsync(delay_steps, d.delay16, sizeof(uint16_t) * h.e, cudaMemcpyDeviceToHost, stream_));
     if (h.e && (tgt || w_bits || delay_steps)) {
-        // unpack the records (target | delay << 24, weight bits)
-        std::vector<SynRec> rec(h.e);
-        NE2B_CUDA(cudaMemcpyAsync(rec.data(), d.syn, sizeof(SynRec) * h.e, cudaMemcpyDeviceToHost, stream_));
-        if (delay_steps && wide)
-            NE2B_CUDA(cudaMemcpyAsync(delay_steps, d.delay16, sizeof(uint16_t) * h.e, cudaMemcpyDeviceToHost, stream_));
-        NE2B_CUDA(cudaStreamSynchronize(stream_));
-        for (uint64_t j = 0; j < h.e; ++j) {
-            if (tgt) tgt[j] = wide ? rec[j].td : rec[j].td & kSynTgtMask;
-            if (w_bits) w_bits[j] = rec[j].w;
-            if (delay_steps && !wide) delay_steps[j] = (uint16_t)(rec[j].td >> kSynTgtBits);
+        // unpack the records (target | delay << 24, weight bits) through a
+        // bounded host buffer, a chunk at a time
+        const uint64_t chunk = std::min<uint64_t>(h.e, 1ull << 22);
+        std::vector<SynRec> rec(chunk);
+        for (uint64_t j0 = 0; j0 < h.e; j0 += chunk) {
+            const uint64_t m = std::min<uint64_t>(chunk, h.e - j0);
+            NE2B_CUDA(cudaMemcpyAsync(rec.data(), d.syn + j0, sizeof(SynRec) * m, cudaMemcpyDeviceToHost, stream_));
+            NE2B_CUDA(cudaStreamSynchronize(stream_));
+            for (uint64_t j = 0; j < m; ++j) {
+                if (tgt) tgt[j0 + j] = wide ? rec[j].td : rec[j].td & kSynTgtMask;
+                if (w_bits) w_bits[j0 + j] = rec[j].w;
+                if (delay_steps && !wide) delay_steps[j0 + j] = (uint16_t)(rec[j].td >> kSynTgtBits);
+            }
         }
     }
     NE2B_CUDA(cudaStreamSynchronize(stream_));

@@ -71,37 +71,33 @@ __device__ __forceinline__ int32_t gauss_numer(uint32_t i, uint64_t step) {
     return (int32_t)((pairs & 0xffffu) + (pairs >> 16)) - 510;
 }
 
-// Deterministic exp(x) for the AdEx step: Cody-Waite reduction x = k*ln2 + r
-// with ln2 split into a 32-significant-bit head and a double tail, the
-// degree-13 Taylor polynomial of e^r (coefficients 1/i! rounded to double)
-// evaluated by Horner with fused multiply-adds, scaled by 2^k, rounded once to
-// float.  Only IEEE double operations, so the host copy (ne2b_expf) and the
-// parity oracle reproduce it bit-for-bit.
+// Deterministic exp(x) for the AdEx step, in single precision: Cody-Waite
+// reduction x = k*ln2 + r with fdlibm's split of ln2 (a 15-bit head, so
+// k*head is exact for every k reached here, and a tail), the degree-7
+// Taylor polynomial of e^r (coefficients 1/i! rounded to float) by Horner
+// with fused multiply-adds, and the scale 2^k applied as two exact powers
+// of two (so neither factor underflows before the last rounding).  Only
+// rounded IEEE single operations, so the host copy (ne2b_expf) and the
+// parity oracle reproduce it bit for bit; within 2 ulp of the correctly
+// rounded exp on [-104, 88.8].
 __device__ __forceinline__ float det_expf(float x) {
     if (x != x) return x;
     if (x > 88.8f) return __int_as_float(0x7f800000);
     if (x < -104.0f) return 0.0f;
-    const double xd = (double)x;
-    const double k = rint(__dmul_rn(xd, 0x1.71547652b82fep+0));
-    double r = __fma_rn(-k, 0x1.62e42fee00000p-1, xd);
-    r = __fma_rn(-k, 0x1.a39ef35793c76p-33, r);
-    double p = 0x1.6124613a86d09p-33;
-    p = __fma_rn(p, r, 0x1.1eed8eff8d898p-29);
-    p = __fma_rn(p, r, 0x1.ae64567f544e4p-26);
-    p = __fma_rn(p, r, 0x1.27e4fb7789f5cp-22);
-    p = __fma_rn(p, r, 0x1.71de3a556c734p-19);
-    p = __fma_rn(p, r, 0x1.a01a01a01a01ap-16);
-    p = __fma_rn(p, r, 0x1.a01a01a01a01ap-13);
-    p = __fma_rn(p, r, 0x1.6c16c16c16c17p-10);
-    p = __fma_rn(p, r, 0x1.1111111111111p-7);
-    p = __fma_rn(p, r, 0x1.5555555555555p-5);
-    p = __fma_rn(p, r, 0x1.5555555555555p-3);
-    p = __fma_rn(p, r, 0x1.0000000000000p-1);
-    p = __fma_rn(p, r, 1.0);
-    p = __fma_rn(p, r, 1.0);
-    const long long ki = (long long)k;
-    const double scale = __longlong_as_double((ki + 1023ll) << 52);
-    return __double2float_rn(__dmul_rn(p, scale));
+    const float k = rintf(__fmul_rn(x, 0x1.715476p+0f));
+    float r = __fmaf_rn(-k, 0x1.62e4p-1f, x);
+    r = __fmaf_rn(-k, 0x1.7f7d1cp-20f, r);
+    float p = 0x1.a01a02p-13f;
+    p = __fmaf_rn(p, r, 0x1.6c16c2p-10f);
+    p = __fmaf_rn(p, r, 0x1.111112p-7f);
+    p = __fmaf_rn(p, r, 0x1.555556p-5f);
+    p = __fmaf_rn(p, r, 0x1.555556p-3f);
+    p = __fmaf_rn(p, r, 0.5f);
+    p = __fmaf_rn(p, r, 1.0f);
+    p = __fmaf_rn(p, r, 1.0f);
+    const int ki = (int)k, k1 = ki / 2, k2 = ki - k1;  // both in [-75, 64]
+    p = __fmul_rn(p, __int_as_float((k1 + 127) << 23));
+    return __fmul_rn(p, __int_as_float((k2 + 127) << 23));
 }
 
 // Izhikevich step, sim/src/model/izh.rs:184-192 (CUDA text izh.rs:194-199):

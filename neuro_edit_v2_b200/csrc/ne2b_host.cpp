@@ -439,27 +439,34 @@ ne2b_status ne2b_net_free(ne2b_net *net) {
     return NE2B_OK;
 }
 
-// Host copy of the device det_expf (ne2b_device.cuh): same IEEE double
-// sequence, so host and device agree bit-for-bit.
+// Host copy of the device det_expf (ne2b_device.cuh): the same rounded IEEE
+// single operations (fmaf is the fused multiply-add, rounded once), so host
+// and device agree bit for bit.
+static float pow2f(int e) {
+    const uint32_t bits = (uint32_t)(e + 127) << 23;
+    float f;
+    memcpy(&f, &bits, sizeof f);
+    return f;
+}
 float ne2b_expf(float x) {
     if (x != x) return x;
     if (x > 88.8f) return INFINITY;
     if (x < -104.0f) return 0.0f;
-    static const double c[14] = {
-        1.0, 1.0, 0x1.0000000000000p-1, 0x1.5555555555555p-3, 0x1.5555555555555p-5, 0x1.1111111111111p-7,
-        0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-16, 0x1.71de3a556c734p-19,
-        0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26, 0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33};
-    const double xd = (double)x;
-    const double k = nearbyint(xd * 0x1.71547652b82fep+0);
-    double r = fma(-k, 0x1.62e42fee00000p-1, xd);
-    r = fma(-k, 0x1.a39ef35793c76p-33, r);
-    double p = c[13];
-    for (int i = 12; i >= 0; --i) p = fma(p, r, c[i]);
-    const long long ki = (long long)k;
-    const unsigned long long bits = (unsigned long long)(ki + 1023) << 52;
-    double scale;
-    memcpy(&scale, &bits, sizeof scale);
-    return (float)(p * scale);
+    const float xl = x * 0x1.715476p+0f;
+    const float k = rintf(xl);
+    float r = fmaf(-k, 0x1.62e4p-1f, x);
+    r = fmaf(-k, 0x1.7f7d1cp-20f, r);
+    float p = 0x1.a01a02p-13f;
+    p = fmaf(p, r, 0x1.6c16c2p-10f);
+    p = fmaf(p, r, 0x1.111112p-7f);
+    p = fmaf(p, r, 0x1.555556p-5f);
+    p = fmaf(p, r, 0x1.555556p-3f);
+    p = fmaf(p, r, 0.5f);
+    p = fmaf(p, r, 1.0f);
+    p = fmaf(p, r, 1.0f);
+    const int ki = (int)k, k1 = ki / 2, k2 = ki - k1;
+    p = p * pow2f(k1);
+    return p * pow2f(k2);
 }
 
 }  // extern "C"

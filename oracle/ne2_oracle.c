@@ -523,43 +523,49 @@ float ne2o_gauss_scale(float sd) {
 }
 
 /* ===================================================== deterministic exp */
-/* exp(x) in double by Cody-Waite reduction x = k*ln2 + r (ln2 split into a
- * 32-significant-bit head and a tail) and the degree-13 Taylor polynomial
- * of e^r (coefficients 1/i! rounded to double) evaluated by Horner with
- * fused multiply-adds, scaled by 2^k and rounded once to float.  Every
- * step is an IEEE-754 double operation, so the device kernels reproduce it
- * bit-for-bit. */
-static const double DX_INV_LN2 = 0x1.71547652b82fep+0;
-static const double DX_LN2_HI = 0x1.62e42fee00000p-1;
-static const double DX_LN2_LO = 0x1.a39ef35793c76p-33;
-static const double DX_C[14] = {
-    0x1.0000000000000p+0, 0x1.0000000000000p+0, 0x1.0000000000000p-1, 0x1.5555555555555p-3,
-    0x1.5555555555555p-5, 0x1.1111111111111p-7, 0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13,
-    0x1.a01a01a01a01ap-16, 0x1.71de3a556c734p-19, 0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26,
-    0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33};
+/* exp(x) in single precision by Cody-Waite reduction x = k*ln2 + r (fdlibm's
+ * split of ln2: a 15-bit head 0x1.62e4p-1, so k*head is exact for |k| <= 150,
+ * and a tail 0x1.7f7d1cp-20), the degree-7 Taylor polynomial of e^r
+ * (coefficients 1/i! rounded to float) evaluated by Horner with fmaf, and
+ * the scale 2^k applied as two exact powers of two, k = k1 + k2 with
+ * k1 = k/2, so that neither factor underflows before the last rounding.
+ * Every step is a rounded IEEE-754 single operation, so the device kernels
+ * reproduce it bit-for-bit; it is within 2 ulp of the correctly rounded exp
+ * on [-104, 88.8]. */
+static float det_pow2f(int e) {
+    const uint32_t bits = (uint32_t)(e + 127) << 23;
+    float f;
+    memcpy(&f, &bits, sizeof f);
+    return f;
+}
 
 float ne2o_det_expf(float x) {
     if (x != x) return x;
     if (x > 88.8f) return INFINITY;
     if (x < -104.0f) return 0.0f;
-    double xd = (double)x;
-    double k = nearbyint(xd * DX_INV_LN2);
-    double r = fma(-k, DX_LN2_HI, xd);
-    r = fma(-k, DX_LN2_LO, r);
-    double p = DX_C[13];
-    for (int i = 12; i >= 0; --i) p = fma(p, r, DX_C[i]);
-    int64_t ki = (int64_t)k;
-    uint64_t bits = (uint64_t)(ki + 1023) << 52;
-    double scale;
-    memcpy(&scale, &bits, sizeof scale);
-    return (float)(p * scale);
+    const float xl = x * 0x1.715476p+0f;
+    const float k = rintf(xl);
+    float r = fmaf(-k, 0x1.62e4p-1f, x);
+    r = fmaf(-k, 0x1.7f7d1cp-20f, r);
+    float p = 0x1.a01a02p-13f;
+    p = fmaf(p, r, 0x1.6c16c2p-10f);
+    p = fmaf(p, r, 0x1.111112p-7f);
+    p = fmaf(p, r, 0x1.555556p-5f);
+    p = fmaf(p, r, 0x1.555556p-3f);
+    p = fmaf(p, r, 0.5f);
+    p = fmaf(p, r, 1.0f);
+    p = fmaf(p, r, 1.0f);
+    const int ki = (int)k, k1 = ki / 2, k2 = ki - k1;
+    p = p * det_pow2f(k1);
+    return p * det_pow2f(k2);
 }
 
 struct expf_job {
     float (*f)(float);
     uint32_t lo_bits, hi_bits; /* ordered float keys, see expf_key */
     uint32_t stride, first, step;
-    uint64_t bad, checked;
+    uint64_t bad, checked;     /* bad: mismatches, or the largest ulp distance in ulp_mode */
+    int ulp_mode;
 };
 /* total order of float bit patterns as unsigned keys: -x < -0 < +0 < x */
 static uint32_t expf_key(float x) {
@@ -580,29 +586,50 @@ static void *expf_worker(void *arg) {
         const float x = expf_unkey((uint32_t)k);
         const float a = j->f(x), b = ne2o_det_expf(x);
         j->checked++;
-        if (memcmp(&a, &b, sizeof a) != 0) j->bad++;
+        if (j->ulp_mode) {
+            /* distance in representable floats (both results are >= 0) */
+            const uint32_t ka = expf_key(a), kb = expf_key(b);
+            const uint64_t d = ka > kb ? ka - kb : kb - ka;
+            if (d > j->bad) j->bad = d;
+        } else if (memcmp(&a, &b, sizeof a) != 0) {
+            j->bad++;
+        }
     }
     return NULL;
 }
-uint64_t ne2o_expf_mismatches(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
-                              uint64_t *checked) {
+static uint64_t expf_scan(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
+                          uint64_t *checked, int ulp_mode) {
     if (threads < 1) threads = 1;
     if (threads > 64) threads = 64;
     if (stride < 1) stride = 1;
     struct expf_job jobs[64];
     pthread_t th[64];
     for (uint32_t i = 0; i < threads; ++i) {
-        jobs[i] = (struct expf_job){f, expf_key(lo), expf_key(hi), stride, i, threads, 0, 0};
+        jobs[i] = (struct expf_job){f, expf_key(lo), expf_key(hi), stride, i, threads, 0, 0, ulp_mode};
         pthread_create(&th[i], NULL, expf_worker, &jobs[i]);
     }
     uint64_t bad = 0, n = 0;
     for (uint32_t i = 0; i < threads; ++i) {
         pthread_join(th[i], NULL);
-        bad += jobs[i].bad;
+        if (ulp_mode) bad = jobs[i].bad > bad ? jobs[i].bad : bad;
+        else bad += jobs[i].bad;
         n += jobs[i].checked;
     }
     if (checked) *checked = n;
     return bad;
+}
+uint64_t ne2o_expf_mismatches(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
+                              uint64_t *checked) {
+    return expf_scan(f, lo, hi, stride, threads, checked, 0);
+}
+uint64_t ne2o_expf_max_ulp(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
+                           uint64_t *checked) {
+    return expf_scan(f, lo, hi, stride, threads, checked, 1);
+}
+/* exp in double, rounded once to float: the correctly rounded exp except
+ * where exp(x) falls within a double ulp of a float midpoint */
+float ne2o_expf_ref(float x) {
+    return (float)exp((double)x);
 }
 
 /* ============================================================ readout */

@@ -139,6 +139,11 @@ void ne2o_fit_ridge(const float *x, uint32_t t, uint32_t f, const float *y, floa
 int ne2o_cholesky_solve(const double *a, const double *b, uint32_t n, double *w);
 uint64_t ne2o_expf_mismatches(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
                               uint64_t *checked);
+/* test support: the largest distance, in representable floats, between f
+ * and ne2o_det_expf on the same inputs as ne2o_expf_mismatches */
+uint64_t ne2o_expf_max_ulp(float (*f)(float), float lo, float hi, uint32_t stride, uint32_t threads,
+                           uint64_t *checked);
+float    ne2o_expf_ref(float x);  /* (float)exp((double)x) */
 
 /* --------------------------------------------------------------- sim */
 typedef struct {

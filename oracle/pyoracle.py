@@ -81,6 +81,8 @@ def lib() -> C.CDLL:
             "ne2o_gauss_scale": (f32, [f32]),
             "ne2o_det_expf": (f32, [f32]),
             "ne2o_expf_mismatches": (u64, [vp, f32, f32, u32, u32, vp]),
+            "ne2o_expf_max_ulp": (u64, [vp, f32, f32, u32, u32, vp]),
+            "ne2o_expf_ref": (f32, [f32]),
             "ne2o_fit_ridge_multi": (None, [vp, u32, u32, vp, u32, f64, vp]),
             "ne2o_fit_ridge": (None, [vp, u32, u32, vp, f32, vp]),
             "ne2o_cholesky_solve": (i32, [vp, vp, u32, vp]),

@@ -126,9 +126,9 @@ def test_host_expf_matches_oracle_det_expf():
 
 
 def test_host_expf_equals_oracle_on_a_stride_of_all_floats():
-    """The library's host copy of the device exp equals the oracle's, which
-    is the correctly rounded exp, on every 64th float of [-104, 88.8] (every
-    float with NE2B_EXHAUSTIVE_EXP=1: 2,239,863,196 values)."""
+    """The library's host copy of the device exp equals the oracle's on every
+    64th float of [-104, 88.8] (every float with NE2B_EXHAUSTIVE_EXP=1:
+    2,239,863,196 values)."""
     key = lambda x: (lambda b: (~b & 0xFFFFFFFF) if b >> 31 else b | 0x80000000)(
         struct.unpack("<I", struct.pack("<f", x))[0])
     n = key(88.8) - key(-104.0) + 1
@@ -197,3 +197,16 @@ def test_parallel_csr_build_is_the_stable_order():
     q = (d[order] / np.float32(0.1)).astype(np.float64)  # f32 quotient; roundf rounds half away from zero
     steps = np.maximum(1, np.floor(q + 0.5)).astype(np.uint16)
     assert np.array_equal(a.delay_steps, steps)
+
+
+def test_deterministic_exp_within_two_ulp():
+    """The deterministic exp (single precision, shared by kernel, library and
+    oracle) lies within 2 ulp of exp computed in double and rounded to float,
+    on every 64th float of [-104, 88.8] (every float with
+    NE2B_EXHAUSTIVE_EXP=1), subnormal results included."""
+    stride = 1 if os.environ.get("NE2B_EXHAUSTIVE_EXP") == "1" else 64
+    fn = ctypes.cast(O.lib().ne2o_expf_ref, ctypes.c_void_p)
+    checked = ctypes.c_uint64()
+    worst = O.lib().ne2o_expf_max_ulp(fn, -104.0, 88.8, stride, os.cpu_count() or 1, ctypes.byref(checked))
+    assert checked.value == (2_239_863_196 + stride - 1) // stride
+    assert worst <= 2, worst

@@ -442,7 +442,8 @@ def run_ours(args):
     extra = {}
     if not args.no_extras and ws == 1:
         peak_v, _ = load_peaks()
-        jobs = (("c1m_izh", lambda: bench_1m(nb, torch, scrub, nb.MODEL_IZH, 2, 3, peak_v)),
+        jobs = (("c10k", lambda: bench_10k(nb, torch, scrub, args.steps, peak_v)),
+                ("c1m_izh", lambda: bench_1m(nb, torch, scrub, nb.MODEL_IZH, 2, 3, peak_v)),
                 ("c1m_adex", lambda: bench_1m(nb, torch, scrub, nb.MODEL_ADEX, 2, 3, peak_v)),
                 ("fp32_ring_100k", lambda: bench_fp32_ring(nb, torch, scrub, net, args.steps, peak_v)),
                 ("batched_256", lambda: bench_batched(nb, torch, scrub, 2, 3)),
@@ -550,6 +551,33 @@ def bench_1m(nb, torch, scrub, model: int, steps: int, warmup: int, peak: float)
     out["quiet"] = measure(0.0)
     out["active"] = measure(ADEX_ACTIVE_KICK_HZ if adex else ACTIVE_KICK_HZ)
     sim.close()
+    return out
+
+
+def bench_10k(nb, torch, scrub, steps: int, peak: float):
+    """The 10,000-neuron configuration (same generator, K=100, 1000 ms trials
+    from reset, Gaussian noise sd 1, tau_syn 5 ms) in both ring modes, as
+    configured (silent) and with Poisson kicks 100 Hz x 20 mV; the
+    autotuner picks the kernel (the resident one fits at this size)."""
+    n = 10_000
+    net = nb.random_kout(n, K_OUT, SEED)
+    out = {"neurons": n, "synapses": n * K_OUT, "trial_steps": TRIAL_STEPS}
+    for ring, iw in (("int32", 1), ("f32", 0)):
+        for name, kick in (("quiet", 0.0), ("active", ACTIVE_KICK_HZ)):
+            sim = nb.B200Sim(net, nb.default_config(int_weights=iw, gauss_sd=1.0, synapse_tau_ms=5.0,
+                                                    noise_rate_hz=kick, noise_kick_mv=20.0, seed=SEED))
+            tiling = sim.autotune(256)
+            ms, spikes, launches = timed_trials(sim, steps, 3, TRIAL_STEPS, 1, torch, scrub)
+            events = spikes * K_OUT
+            step_s = ms / 1000.0 / (TRIAL_STEPS * steps)
+            alg = B_NEURON * n + (B_SPIKE * spikes + B_EVENT * events) / (TRIAL_STEPS * steps)
+            out[f"{ring}_{name}"] = {"kick_hz": kick, "neuron_updates_per_s": n * TRIAL_STEPS * steps / (ms / 1000.0),
+                                     "synaptic_events_per_s": events / (ms / 1000.0),
+                                     "firing_rate_hz": spikes / (n * steps * TRIAL_STEPS * 1e-4),
+                                     "ms_per_trial": ms / steps, "step_us": step_s * 1e6,
+                                     "roofline_frac": alg / step_s / 1e9 / peak, "gpu_launches": launches,
+                                     "tiling": tiling}
+            sim.close()
     return out
 
 
@@ -877,7 +905,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the 1M, batched and serving measurements")
     ap.add_argument("--extras", default="",
-                    help="comma-separated subset of the extras (c1m_izh, c1m_adex, fp32_ring_100k, batched_256, "
+                    help="comma-separated subset of the extras (c10k, c1m_izh, c1m_adex, fp32_ring_100k, batched_256, "
                          "batched_256_active, serving)")
     ap.add_argument("--serving-requests", type=int, default=200)
     ap.add_argument("--admission-threads", type=int, default=4,

@@ -168,11 +168,11 @@ ne2b_status ne2b_external(ne2b_sim *sim, float *out);
 ne2b_status ne2b_set_noise(ne2b_sim *sim, float rate_hz, float kick_mv);
 ne2b_status ne2b_set_gauss_noise(ne2b_sim *sim, float sd);                 /* new */
 
-/* Step kernel selection (new): NE2B_KERNEL_AUTO picks the resident
- * persistent kernel when every net's state fits in shared memory, else the
- * streaming kernel; the other two force one (RESIDENT fails with
- * NE2B_UNSUPPORTED when the nets do not fit).  *resident reports which
- * kernel runs.  The environment variable NE2B_KERNEL=stream|resident sets
+/* Step kernel selection (new): NE2B_KERNEL_AUTO runs the streaming kernel
+ * (one launch per step), which ne2b_autotune may replace by the resident
+ * persistent kernel where that measures faster; the other two force one
+ * (RESIDENT fails with NE2B_UNSUPPORTED when the nets' state does not fit
+ * in shared memory).  *resident reports which kernel runs.  The environment variable NE2B_KERNEL=stream|resident sets
  * the initial mode of every handle. */
 enum { NE2B_KERNEL_AUTO = 0, NE2B_KERNEL_STREAM = 1, NE2B_KERNEL_RESIDENT = 2 };
 ne2b_status ne2b_set_kernel_mode(ne2b_sim *sim, int32_t mode);

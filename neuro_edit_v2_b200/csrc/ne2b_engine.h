@@ -78,8 +78,6 @@ struct NetHost {
 
 enum KernelMode { kModeAuto = 0, kModeStream = 1, kModeResident = 2 };
 
-constexpr uint64_t kResidentAutoMax = 150000;  // neurons
-
 struct EngineSnapshot {
     struct Item {
         void *live, *backup;

@@ -199,10 +199,13 @@ def test_100k_workload_int_ring_bit_exact_first_1000_steps(mode):
     assert_state_bits_equal(g, o)
 
 
-def test_auto_mode_picks_resident_when_state_fits_and_stream_when_not():
+def test_auto_mode_streams_and_resident_runs_only_where_state_fits():
     small = nb.random_kout(20_000, 10, 1)
     g = nb.B200Sim(small)
-    assert g.kernel_mode() == (nb.KERNEL_AUTO, True)
+    assert g.kernel_mode() == (nb.KERNEL_AUTO, False)
+    g.set_kernel_mode(nb.KERNEL_RESIDENT)
+    assert g.kernel_mode() == (nb.KERNEL_RESIDENT, True)
+    g.run_steps(10)
     n = 3_000_000  # 16 B of on-chip state per neuron exceeds 148 SMs x 227 KB
     big = nb.FlatNet(model=np.zeros(n, np.uint8), params=np.tile(np.float32([0.02, 0.2, -65, 8]), (n, 1)),
                      src_ptr=np.zeros(n + 1, np.uint32), tgt=np.zeros(0, np.uint32), w=np.zeros(0, np.float32),

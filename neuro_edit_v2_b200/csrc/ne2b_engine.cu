@@ -834,6 +834,8 @@ bool Engine::plan_resident(std::vector<Tile> &tiles, std::vector<uint32_t> &bloc
     // (10k neurons: 2.9 against 1.4 us per step; 100k: 3.1 against 1.9).
     // It runs when forced, or when ne2b_autotune finds it faster.
     if (tiles.empty() || mode_ != kModeResident) return false;
+    uint64_t total = 0;
+    for (const Tile &t : tiles) total += t.count;
     const uint32_t head = resident_head(shape_.block, shape_.npt);
     const uint32_t max_bps = std::max<uint32_t>(1, 2048 / shape_.block);
     for (uint32_t bps = shape_.blocks_per_sm ? shape_.blocks_per_sm : max_bps; bps >= 1; --bps) {

@@ -660,14 +660,15 @@ def bench_batched(nb, torch, scrub, steps: int, warmup: int, serial_sample: int 
             events += int((c * deg).sum())
     launches = b.kernel_launches()
     b.close()
-    # the same kernels, one network at a time, on a sample of the set: every
-    # 8th net, so the sample spans the size range (the nets are in a seeded
-    # random size order); its trials/s is scaled to the whole set by neurons
+    # the same kernels, one network at a time (each autotuned, as the batch
+    # is), on a sample of the set: every 8th net, so the sample spans the size
+    # range (the nets are in a seeded random size order)
     sample = list(range(0, len(nets), max(1, len(nets) // serial_sample)))[:serial_sample]
     ser_ms = 0.0
     for k in sample:
         one = nb.Batch([nets[k]], [cfgs[k]])
         one.set_input_matrix(0, inputs[k])
+        one.autotune(128)  # each net on its own best kernel and tiles, as the batch is
         ser_ms += batch_trials(one, torch, scrub, 1, 1, trial)
         one.close()
     batched_tps = len(nets) * steps / (total_ms / 1000.0)

@@ -778,6 +778,26 @@ def bench_serving(nb, count: int, threads: int = 4):
         srv.take(rid)
     srv.close()
     one_tps = sample / (time.perf_counter() - t0)
+    # one at a time, each request on its own engine with the kernel and tiles
+    # the autotuner picks for it alone (the tuning itself untimed): building
+    # it, running it from reset and reading its counts back
+    tuned_sample = min(12, count)
+    tuned_s = 0.0
+    for r in range(tuned_sample):
+        t1 = time.perf_counter()
+        one = nb.Batch([reqs[r].net], [W.request_config(reqs[r], 11 + r)])
+        one.set_input_matrix(0, reqs[r].inputs)
+        t2 = time.perf_counter()
+        one.autotune(128)
+        one.reset_state()
+        one.synchronize()
+        t3 = time.perf_counter()
+        one.run_steps(reqs[r].steps)
+        one.window_counts(0, 0)
+        one.synchronize()
+        tuned_s += (t2 - t1) + (time.perf_counter() - t3)
+        one.close()
+    tuned_tps = tuned_sample / tuned_s
     q = np.quantile(np.array(lat), [0.5, 0.99])
     sq = np.quantile(np.array(sat_lat), [0.5, 0.99])
     neuron_steps = sum(q_.n * q_.steps for q_ in reqs)
@@ -792,6 +812,9 @@ def bench_serving(nb, count: int, threads: int = 4):
             "one_at_a_time_trials_per_s": one_tps, "one_at_a_time_sample": sample,
             "served_vs_one_at_a_time": (count / span) / one_tps,
             "saturated_vs_one_at_a_time": (count / sat_span) / one_tps,
+            "one_at_a_time_tuned": {"trials_per_s": tuned_tps, "sample": tuned_sample,
+                                    "served_vs": (count / span) / tuned_tps,
+                                    "saturated_vs": (count / sat_span) / tuned_tps},
             "mean_neurons": float(np.mean([q_.n for q_ in reqs])),
             "mean_steps": float(np.mean([q_.steps for q_ in reqs]))}
 

@@ -123,6 +123,7 @@ struct alignas(16) NetDev {
     unsigned long long t_end;   // steps at or beyond this are skipped (serving)
     long long stim_t0;          // step of stim_buf row 0
     unsigned long long seed;
+    unsigned long long noise_step;  // step part of the noise base at t (set_step)
     uint32_t n, n_pad, D, tmod;  // tmod = t % D
     uint32_t n_inputs, stim_len;
     uint32_t rec_rows, win_steps, max_windows, flags;
@@ -140,9 +141,17 @@ struct alignas(16) NetDev {
 #else
 #define NE2B_HD
 #endif
-// Sets t and every phase derived from it (tmod, rphase, wphase, widx0).
+// The noise counter hash's multipliers of the step and the seed
+// (sim/src/state.rs:285-288).
+constexpr unsigned long long kNoiseStepMul = 0xBF58476D1CE4E5B9ull;
+constexpr unsigned long long kNoiseSeedMul = 0x94D049BB133111EBull;
+
+// Sets t and every phase derived from it (tmod, rphase, wphase, widx0, and
+// the noise base's step part t * kNoiseStepMul + seed * kNoiseSeedMul, from
+// which a kernel reaches step t + k with one multiply-add).
 NE2B_HD inline void set_step(NetDev &d, unsigned long long t) {
     d.t = t;
+    d.noise_step = t * kNoiseStepMul + d.seed * kNoiseSeedMul;
     d.tmod = (uint32_t)(t % d.D);
     d.rphase = d.rec_rows ? (uint32_t)(t % d.rec_rows) : 0u;
     if (d.win_steps) {

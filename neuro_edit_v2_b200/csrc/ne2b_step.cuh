@@ -160,7 +160,7 @@ __device__ __forceinline__ void process_tile(const EngineDev *__restrict__ eng, 
     const size_t slot_off = (size_t)tmod * n_pad;
     const float dt = nd.dt, decay_s = nd.decay_s;
     const float pkick = nd.pkick, kick = nd.kick, gauss_k = nd.gauss_k;
-    const uint64_t nbase = noise_base_step(t, nd.seed);
+    const uint64_t nbase = nd.noise_step + (uint64_t)k * kNoiseStepMul;  // = noise_base_step(t, seed)
     const uint32_t tlast = nd.trace_last;
     uint32_t *__restrict__ ringw = (uint32_t *)nd.ring;
     const bool has_ext = !NOIO && (flags & kNetHasExt);
